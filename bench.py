@@ -1,0 +1,366 @@
+#!/usr/bin/env python
+"""Benchmark of the multi-bounce trace loop: ray-bounces/s on one B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (default): the tetrahedron scene — four unit spheres on a regular
+tetrahedron of edge 2.5, 6 x 8 x 8 patches each on 7 x 7 Chebyshev-Lobatto
+nodes, coarse grid 17 x 17 — lit by 1,048,576 seeded rays from z = 5 over
+[-3,3]^2 in a 10-degree cone about -z, at most 200 bounces, Newton tolerance
+1e-12.  One step = one bbrt_trace call over all rays.
+
+value     bounces of all rays / device time of the trace kernel (inputs already
+          in HBM; CUDA events on the launching stream; L2 flushed before each
+          step outside the timed events).
+e2e       the same metric through bbrt_trace with pinned host buffers: the
+          host->device copy of the rays and the device->host copy of the
+          per-ray results are inside the timed region.
+roofline  the trace kernel's dominant pipe (FP64: the path keeps every decision
+          in exact FP64) against the pipe peak measured in this process.
+cpu_baseline  the reference's own OpenMP trace loop (oracle/_ref), or the
+          oracle port when the reference was not built, on a bounded sample
+          of the same rays on all host cores (rank 0, N = 1 only).
+
+With --impl reference the reference's CPU implementation is timed instead
+(rank 0 only; other ranks exit 0), on a bounded slice of the same workload
+per step.  Multi-GPU: replicas — every rank traces its own seeded 1M rays
+(weak scaling, no collective in the data path); value is the sum of all
+ranks' bounces over the maximum rank time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "ray-bounces/sec on 1 B200, learned vs plain Newton guess, at hit err ≤1e-10"
+UNIT = "ray-bounces/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="tetra_spheres")
+    ap.add_argument("--rays", type=int, default=None)
+    ap.add_argument("--cull", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=8.0, help="target wall time of the CPU sample")
+    return ap.parse_args()
+
+
+def workload_config(name, n_rays, maxb, cn, tol, extra=None):
+    desc = {
+        "tetra_spheres": "4 unit spheres on a tetrahedron (edge 2.5), 6x8x8 patches each, 7x7 nodes (degree 6), "
+                         "coarse 17x17 (16x16x2 triangles); rays from z=5 over [-3,3]^2 in a 10-degree cone about -z",
+        "two_spheres": "2 unit spheres at (+-1.5,0,0), 6x4x4 patches each, 5x5 nodes, coarse 9x9; "
+                       "128x128 plane grid on z=4 over [-3,3]^2, direction (0.3,0,-1)",
+        "ellipsoids": "16 random ellipsoids (semi-axes U[0.2,1.2]) in [-6,6]^3, 6x8x8 patches each, 7x7 nodes, "
+                      "coarse 17x17; rays from z=8 over [-6,6]^2 in a 20-degree cone",
+    }[name]
+    c = {"workload": f"{name}: {desc}", "rays": int(n_rays), "max_bounces": int(maxb), "coarse_n": int(cn),
+         "newton_tol": tol, "precision": "fp64 (exact, reference operation order)", "guess": "triangle"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+class ClockSampler:
+    """nvidia-smi sampled every 200 ms in the background during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(prefix="bbrt_clocks_", suffix=".csv")
+            os.close(fd)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.gpu), "-lms", "200"], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def fp64_flop_model(st, nodes_per_axis):
+    """Executed FP64 work of one trace launch from its counters (the model is
+    stated in DESIGN.md): node slab tests 12, Moller-Trumbore up to the
+    u pre-test 28 (+23 past it, bounded by counting all tests at 51 below),
+    corner offsets 72 per tested cell, Newton 18N^2+24N+70 per iteration,
+    reflection and nudge 18 per bounce."""
+    N = nodes_per_axis
+    tested_cells = st["tri_tests"] / 6.0
+    lo = (12 * st["node_tests"] + 28 * st["tri_tests"] + 72 * tested_cells +
+          (18 * N * N + 24 * N + 70) * st["newton_iters"] + 18 * st["bounces"])
+    hi = lo + 23 * st["tri_tests"]
+    return lo, hi
+
+
+def cpu_baseline(patches, o, d, maxb, cn, tol, target_s):
+    """The reference's trace loop (or the oracle port) on a bounded sample."""
+    import oracle
+    threads = os.cpu_count() or 1
+    if oracle.reference_available():
+        tmp = tempfile.mkdtemp(prefix="bbrt_bench_ref_")
+        runner = oracle.Reference.from_patches(patches, tmpdir=tmp, coarse_n=cn, newton_tol=tol)
+        kind = "reference"
+    else:
+        from billardballraytracing3d_b200 import _capi as C
+        runner = oracle.Oracle(patches, config=C.default_config(coarse_grid_n=cn, newton_tol=tol))
+        kind = "port"
+    probe = min(8192, o.shape[0])
+    r = runner.trace(o[:probe], d[:probe], maxb, K=0, nthreads=threads)
+    rate = probe / max(r["seconds"], 1e-6)
+    n = int(min(o.shape[0], max(probe, rate * target_s)))
+    r = runner.trace(o[:n], d[:n], maxb, K=0, nthreads=threads)
+    bounces = int(r["bounce_count"].sum())
+    return {"value": bounces / r["seconds"], "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"first {n} of the workload's rays ({bounces} bounces, {r['seconds']:.2f} s wall, "
+                      f"OpenMP schedule(dynamic) over trace_ray)"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from billardballraytracing3d_b200 import scenes
+    import oracle
+    patches, o, d, maxb, cn, tol = scenes.workload(args.workload, args.rays)
+    threads = os.cpu_count() or 1
+    if oracle.reference_available():
+        runner = oracle.Reference.from_patches(patches, tmpdir=tempfile.mkdtemp(prefix="bbrt_ref_"),
+                                               coarse_n=cn, newton_tol=tol)
+        kind = "reference"
+    else:
+        from billardballraytracing3d_b200 import _capi as C
+        runner = oracle.Oracle(patches, config=C.default_config(coarse_grid_n=cn, newton_tol=tol))
+        kind = "port"
+    # size one step's slice for ~1.5 s of wall time on this host
+    probe = min(8192, o.shape[0])
+    pr = runner.trace(o[:probe], d[:probe], maxb, K=0, nthreads=threads)
+    per = int(min(o.shape[0], max(1024, probe / max(pr["seconds"], 1e-6) * 1.5)))
+    slices = [(k * per) % max(1, o.shape[0] - per + 1) for k in range(args.warmup + args.steps)]
+    for k in range(args.warmup):
+        s = slices[k]
+        runner.trace(o[s:s + per], d[s:s + per], maxb, K=0, nthreads=threads)
+    tot_s, tot_b = 0.0, 0
+    for k in range(args.warmup, args.warmup + args.steps):
+        s = slices[k]
+        r = runner.trace(o[s:s + per], d[s:s + per], maxb, K=0, nthreads=threads)
+        tot_s += r["seconds"]
+        tot_b += int(r["bounce_count"].sum())
+    value = tot_b / tot_s
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_s / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(args.workload, o.shape[0], maxb, cn, tol,
+                                      {"parallelism": f"OpenMP x{threads} host threads",
+                                       "step": f"{per} rays per step (bounded slice of the workload)"}),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                             "sample": f"{args.steps} slices of {per} rays of the workload"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from billardballraytracing3d_b200 import _capi as C
+    from billardballraytracing3d_b200 import api, scenes
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    patches, o, d, maxb, cn, tol = scenes.workload(args.workload, args.rays)
+    if rank > 0 and args.workload != "two_spheres":   # replicas: every rank its own seeded rays
+        o, d = scenes.cone_rays(o.shape[0], 1234 + rank, 5.0, 3.0, 10.0)
+    n = o.shape[0]
+    cfg = C.default_config(coarse_grid_n=cn, newton_tol=tol, cull=args.cull)
+    scene = api.Scene(patches, config=cfg)
+    scene.upload()
+    lib = C.load_library()
+    import ctypes
+    peak = ctypes.c_double()
+    C.check(lib, lib.bbrt_measure_pipe_peak(C.PIPE_FP64, ctypes.byref(peak)), "bbrt_measure_pipe_peak")
+    fp64_peak = peak.value
+    C.check(lib, lib.bbrt_measure_pipe_peak(C.PIPE_FP32, ctypes.byref(peak)), "bbrt_measure_pipe_peak")
+    fp32_peak = peak.value
+
+    to = torch.from_numpy(np.ascontiguousarray(o)).to(dev)
+    td = torch.from_numpy(np.ascontiguousarray(d)).to(dev)
+    st_ = torch.empty(n, dtype=torch.int32, device=dev)
+    bc = torch.empty(n, dtype=torch.int32, device=dev)
+    ed = torch.empty((n, 3), dtype=torch.float64, device=dev)
+    outs = dict(status=st_.data_ptr(), bounce_count=bc.data_ptr(), exit_dir=ed.data_ptr())
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)   # > 126 MB L2
+    # a real stream handle: torch's legacy default stream is handle 0, which the
+    # C ABI reads as "the scene's own stream"
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+
+    stats = None
+    for _ in range(args.warmup):
+        stats = scene.trace_device(to.data_ptr(), td.data_ptr(), n, maxb, outs, stream=stream.cuda_stream,
+                                   want_stats=True)
+    torch.cuda.synchronize(dev)
+    bounces_per_step = int(bc.sum().item())
+    assert stats is None or stats["bounces"] == bounces_per_step
+
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    torch.cuda.synchronize(dev)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    wall0 = time.perf_counter()
+    for k in range(args.steps):
+        flush.zero_()
+        evs[k][0].record(stream)
+        scene.trace_device(to.data_ptr(), td.data_ptr(), n, maxb, outs, stream=stream.cuda_stream)
+        evs[k][1].record(stream)
+    torch.cuda.synchronize(dev)
+    wall = time.perf_counter() - wall0
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    kern_s = sum(step_ms) / 1e3
+    total_b = bounces_per_step * args.steps
+    if world > 1:
+        t = torch.tensor([kern_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        b = torch.tensor([total_b], dtype=torch.int64, device=dev)
+        dist.all_reduce(b, op=dist.ReduceOp.SUM)
+        kern_s, total_b = float(t.item()), int(b.item())
+    value = total_b / kern_s
+
+    # e2e: host (pinned) buffers through the same C ABI call, copies inside the timed region
+    ho = torch.from_numpy(np.ascontiguousarray(o)).pin_memory()
+    hd = torch.from_numpy(np.ascontiguousarray(d)).pin_memory()
+    hs = torch.empty(n, dtype=torch.int32).pin_memory()
+    hb = torch.empty(n, dtype=torch.int32).pin_memory()
+    he = torch.empty((n, 3), dtype=torch.float64).pin_memory()
+    out = C.TraceOut()
+    out.status = ctypes.cast(ctypes.c_void_p(hs.data_ptr()), C.c_int_p)
+    out.bounce_count = ctypes.cast(ctypes.c_void_p(hb.data_ptr()), C.c_int_p)
+    out.exit_dir = ctypes.cast(ctypes.c_void_p(he.data_ptr()), C.c_double_p)
+    e2e_steps = max(1, min(args.steps, 5))
+    e2e_s = 0.0
+    for k in range(e2e_steps + 1):
+        flush.zero_()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        C.check(lib, lib.bbrt_trace(scene.h, ctypes.c_void_p(ho.data_ptr()), ctypes.c_void_p(hd.data_ptr()), n, maxb,
+                                    0, ctypes.byref(out), None, ctypes.c_void_p(stream.cuda_stream)), "bbrt_trace")
+        if k > 0:
+            e2e_s += time.perf_counter() - t0
+    e2e_b = int(hb.numpy().sum()) * e2e_steps
+    if world > 1:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        b = torch.tensor([e2e_b], dtype=torch.int64, device=dev)
+        dist.all_reduce(b, op=dist.ReduceOp.SUM)
+        e2e_s, e2e_b = float(t.item()), int(b.item())
+    e2e = {"value": e2e_b / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(ho.numel() * 8 + hd.numel() * 8),
+           "d2h_bytes_per_step": int(hs.numel() * 4 + hb.numel() * 4 + he.numel() * 8),
+           "note": "host wall clock around bbrt_trace with pinned host arrays (copies + kernel + sync)"}
+
+    if rank != 0:
+        return
+    per_launch_s = kern_s / args.steps
+    flop_lo, flop_hi = fp64_flop_model(stats, patches[0].imax) if stats else (0.0, 0.0)
+    achieved = flop_lo / per_launch_s / 1e12
+    roofline = {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                "frac": achieved / fp64_peak, "traffic": None,
+                "kernel": "k_trace",
+                "note": "executed FP64 work from device counters (lower bound of the model; upper bound "
+                        f"{flop_hi / per_launch_s / 1e12:.3f} TFLOP/s) over the mean CUDA-event launch time; peak = "
+                        "FP64 FMA throughput measured in this process (bbrt_measure_pipe_peak), of measured; "
+                        "the exact path runs with -fmad=false so unfused mul/add cap it at half that peak",
+                "fp32_peak_tflops": fp32_peak}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * per_launch_s, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(args.workload, n, maxb, cn, tol,
+                                      {"parallelism": "replicas" if world > 1 else "single GPU",
+                                       "cull": args.cull,
+                                       "l2": "flushed before each step (256 MiB write), flush outside the timed events",
+                                       "bounces_per_step": bounces_per_step}),
+            "e2e": e2e, "gpu_launches": args.steps, "roofline": roofline, "clocks": clk,
+            "wall_s_timed_region": wall,
+            "counters_per_step": {k: v for k, v in (stats or {}).items() if k not in ("kernel_ms", "total_ms")}}
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(patches, o, d, maxb, cn, tol, args.cpu_seconds)
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,198 @@
+"""Python face of the C ABI (include/bbrt.h) for tests, benchmarks and scripts.
+
+Every method is one C-ABI call into libbbrt_cuda.so; nothing here computes a
+trace result itself.  The C++ classes under include/bbrt/ are the drop-in
+mirror of the reference's RayTracingDriver / BVH / PlaneSourceDriver /
+BounceMapDriver API; this module is the same boundary seen from Python.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Dict, Optional, Sequence
+
+import numpy as np
+
+from . import _capi as C
+
+P = lambda a: None if a is None else ctypes.c_void_p(a.ctypes.data)  # noqa: E731
+
+
+class TraceResult(dict):
+    """Per-ray arrays keyed like bbrt_trace_out, plus 'stats'."""
+
+
+class Scene:
+    """One bbrt scene (device arrays + stream).  Build from patches
+    (scenes.Patch), triangles (9 floats each), or a patch directory."""
+
+    def __init__(self, patches: Sequence = (), triangles: Sequence = (), config: C.Config = None,
+                 directory: str = None, _handle=None):
+        self.lib = C.load_library()
+        self.config = config if config is not None else C.default_config()
+        h = ctypes.c_void_p()
+        if _handle is not None:
+            h = _handle
+        elif directory is not None:
+            C.check(self.lib, self.lib.bbrt_scene_create_from_dir(directory.encode(), ctypes.byref(self.config),
+                                                                   ctypes.byref(h)), "bbrt_scene_create_from_dir")
+        else:
+            self.table = C.ObjectTable(patches, triangles)
+            C.check(self.lib, self.lib.bbrt_scene_create(self.table.descs, self.table.n, ctypes.byref(self.config),
+                                                         ctypes.byref(h)), "bbrt_scene_create")
+        self.h = h
+        inf = self.info()
+        self.n_objects = inf["n_objects"]
+
+    @classmethod
+    def from_range(cls, directory: str, prefix: str, first: int, last: int, config: C.Config = None):
+        lib = C.load_library()
+        cfg = config if config is not None else C.default_config()
+        h = ctypes.c_void_p()
+        C.check(lib, lib.bbrt_scene_create_from_range(directory.encode(), prefix.encode(), first, last,
+                                                      ctypes.byref(cfg), ctypes.byref(h)), "bbrt_scene_create_from_range")
+        return cls(config=cfg, _handle=h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.bbrt_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- host-side queries (no GPU needed) ---------------------------------
+    def info(self) -> Dict:
+        s = C.SceneInfo()
+        C.check(self.lib, self.lib.bbrt_scene_info_get(self.h, ctypes.byref(s)), "bbrt_scene_info_get")
+        return {k: getattr(s, k) for k, _ in s._fields_}
+
+    def object_info(self, k: int) -> Dict:
+        o = C.ObjectInfo()
+        C.check(self.lib, self.lib.bbrt_object_info_get(self.h, k, ctypes.byref(o)), "bbrt_object_info_get")
+        return dict(kind=o.kind, zone_id=o.zone_id, box=np.array(list(o.box_min) + list(o.box_max)),
+                    centroid=np.array(list(o.centroid)), padding=o.padding)
+
+    def coarse_grid(self, k: int) -> Dict:
+        n = ctypes.c_int()
+        C.check(self.lib, self.lib.bbrt_patch_coarse_grid(self.h, k, ctypes.byref(n), None, None, None, None, None),
+                "bbrt_patch_coarse_grid")
+        g = n.value
+        u = np.zeros(g); v = np.zeros(g); xyz = np.zeros((g * g, 3))
+        sag = np.zeros((g - 1) ** 2); nrm = np.zeros(((g - 1) ** 2, 3))
+        C.check(self.lib, self.lib.bbrt_patch_coarse_grid(self.h, k, ctypes.byref(n), C.ptr(u), C.ptr(v), C.ptr(xyz),
+                                                          C.ptr(sag), C.ptr(nrm)), "bbrt_patch_coarse_grid")
+        return dict(n=g, u=u, v=v, coarse_xyz=xyz, sagitta=sag, cell_normal=nrm)
+
+    def self_intersect_epsilon(self, k: int = -1) -> float:
+        e = ctypes.c_double()
+        C.check(self.lib, self.lib.bbrt_self_intersect_epsilon(self.h, k, ctypes.byref(e)), "bbrt_self_intersect_epsilon")
+        return e.value
+
+    # ---- GPU calls ------------------------------------------------------------
+    def upload(self):
+        C.check(self.lib, self.lib.bbrt_scene_upload(self.h), "bbrt_scene_upload")
+
+    def intersect(self, origins, dirs, mode: int = C.QUERY_BVH, obj: int = 0) -> np.ndarray:
+        o = np.ascontiguousarray(origins, dtype=np.float64).reshape(-1, 3)
+        d = np.ascontiguousarray(dirs, dtype=np.float64).reshape(-1, 3)
+        out = np.zeros(o.shape[0], dtype=C.HIT_DTYPE)
+        C.check(self.lib, self.lib.bbrt_intersect(self.h, P(o), P(d), o.shape[0], mode, obj, 0, P(out), None),
+                "bbrt_intersect")
+        return out
+
+    def trace(self, origins, dirs, max_bounces: int, record: int = 8, want_stats: bool = True,
+              outputs: Sequence[str] = ("status", "bounce_count", "exit_dir", "end_point", "hit_object",
+                                        "hit_point", "hit_uv", "err_object", "err_value")) -> TraceResult:
+        o = np.ascontiguousarray(origins, dtype=np.float64).reshape(-1, 3)
+        d = np.ascontiguousarray(dirs, dtype=np.float64).reshape(-1, 3)
+        n = o.shape[0]
+        K = record
+        shapes = dict(status=((n,), np.int32), bounce_count=((n,), np.int32), exit_dir=((n, 3), np.float64),
+                      end_point=((n, 3), np.float64), hit_object=((n, K), np.int32),
+                      hit_point=((n, K, 3), np.float64), hit_uv=((n, K, 2), np.float64),
+                      err_object=((n,), np.int32), err_value=((n, 2), np.float64))
+        r = TraceResult()
+        for k in outputs:
+            shp, dt = shapes[k]
+            r[k] = np.zeros(shp, dt)
+        out = C.TraceOut()
+        out.record_bounces = K
+        for k in shapes:
+            ct = ctypes.c_int if shapes[k][1] == np.int32 else ctypes.c_double
+            setattr(out, k, C.ptr(r.get(k), ct))
+        st = C.TraceStats()
+        C.check(self.lib, self.lib.bbrt_trace(self.h, P(o), P(d), n, max_bounces, 0, ctypes.byref(out),
+                                              ctypes.byref(st) if want_stats else None, None), "bbrt_trace")
+        if want_stats:
+            r["stats"] = st.as_dict()
+        return r
+
+    def trace_device(self, origins_ptr: int, dirs_ptr: int, n: int, max_bounces: int, out_ptrs: Dict[str, int],
+                     record: int = 0, stream: int = 0, want_stats: bool = False) -> Optional[Dict]:
+        """bbrt_trace on device pointers (e.g. torch tensors' data_ptr())."""
+        out = C.TraceOut()
+        out.record_bounces = record
+        for k, v in out_ptrs.items():
+            ct = ctypes.c_int if k in ("status", "bounce_count", "hit_object", "err_object") else ctypes.c_double
+            setattr(out, k, ctypes.cast(ctypes.c_void_p(v), ctypes.POINTER(ct)))
+        st = C.TraceStats()
+        C.check(self.lib, self.lib.bbrt_trace(self.h, ctypes.c_void_p(origins_ptr), ctypes.c_void_p(dirs_ptr), n,
+                                              max_bounces, C.DEVICE_PTRS, ctypes.byref(out),
+                                              ctypes.byref(st) if want_stats else None,
+                                              ctypes.c_void_p(stream) if stream else None), "bbrt_trace")
+        return st.as_dict() if want_stats else None
+
+    def plane_source(self, corner0, corner1, direction, nx: int, ny: int, max_bounces: int,
+                     count_direct_hit: bool = False, want_stats: bool = False):
+        c0 = np.ascontiguousarray(corner0, dtype=np.float64)
+        c1 = np.ascontiguousarray(corner1, dtype=np.float64)
+        dd = np.ascontiguousarray(direction, dtype=np.float64)
+        counts = np.zeros(self.n_objects, np.int64)
+        st = C.TraceStats()
+        C.check(self.lib, self.lib.bbrt_plane_source(self.h, C.ptr(c0), C.ptr(c1), C.ptr(dd), nx, ny, max_bounces,
+                                                     int(count_direct_hit), C.ptr(counts, ctypes.c_longlong),
+                                                     ctypes.byref(st) if want_stats else None, None),
+                "bbrt_plane_source")
+        return (counts, st.as_dict()) if want_stats else counts
+
+    def bounce_map(self, sample_patches: Sequence, grid_n: int, theta_n: int, phi_n: int,
+                   cone_angle_deg: float = 180.0, max_bounces: int = 50):
+        t = C.ObjectTable(sample_patches)
+        m = len(sample_patches) * grid_n * grid_n
+        mb = np.zeros(m, np.int32); er = np.zeros(m, np.int32); bd = np.zeros(m, np.int32)
+        C.check(self.lib, self.lib.bbrt_bounce_map(self.h, t.pdescs, len(sample_patches), grid_n, theta_n, phi_n,
+                                                   float(cone_angle_deg), max_bounces, C.ptr(mb, ctypes.c_int),
+                                                   C.ptr(er, ctypes.c_int), C.ptr(bd, ctypes.c_int), None, None),
+                "bbrt_bounce_map")
+        return mb, er, bd
+
+
+def sample_grid(patch, n: int):
+    """SurfacePatch::sample_grid(n) through the C ABI: (xyz, normal, dX/du)."""
+    lib = C.load_library()
+    t = C.ObjectTable([patch])
+    xyz = np.zeros((n * n, 3)); nrm = np.zeros((n * n, 3)); du = np.zeros((n * n, 3))
+    C.check(lib, lib.bbrt_patch_sample_grid(t.pdescs, n, C.ptr(xyz), C.ptr(nrm), C.ptr(du)), "bbrt_patch_sample_grid")
+    return xyz, nrm, du
+
+
+def read_patch_file(path: str) -> Dict:
+    """SurfacePatch::load_patch_file through the C ABI; returns numpy copies."""
+    lib = C.load_library()
+    f = C.PatchFile()
+    C.check(lib, lib.bbrt_patch_file_read(path.encode(), ctypes.byref(f)), "bbrt_patch_file_read")
+    try:
+        d = f.desc
+        n = d.imax * d.jmax * d.kmax
+        arr = lambda p, m: np.ctypeslib.as_array(p, shape=(m,)).copy()  # noqa: E731
+        out = dict(imax=d.imax, jmax=d.jmax, kmax=d.kmax, zone_id=d.zone_id,
+                   u_nodes=arr(d.u_nodes, d.imax), v_nodes=arr(d.v_nodes, d.jmax),
+                   mask=arr(f.mask, n), dS=arr(f.dS, n), edge_flags=list(f.edge_flags))
+        for k in ("x", "y", "z", "dxdu", "dydu", "dzdu", "dxdv", "dydv", "dzdv", "nu_x", "nu_y", "nu_z"):
+            out[k] = arr(getattr(d, k), n)
+        return out
+    finally:
+        lib.bbrt_patch_file_free(ctypes.byref(f))

@@ -1,0 +1,722 @@
+// C ABI of libbbrt_cuda.so (include/bbrt.h): scene lifetime, device upload,
+// and the batch entry points that launch the trace kernels.
+//
+// Reference call sites replaced (manuelarturosantana/BillardBallRayTracing3D):
+//   RayTracingDriver(dir) / (dir, prefix, first, last)   RayTracingDriver.hpp:91-114, 346-424
+//   RayTracingDriver::trace_ray / run                     :172-242, :143-150
+//   BVH::intersect, brute_force_intersect                 BVH.hpp:75-128, BruteForce.hpp:7-16
+//   PlaneSourceDriver::run                                PlaneSourceDriver.hpp:79-109
+//   BounceMapDriver::run                                  BounceMapDriver.hpp:103-259
+//   SurfacePatch::load_patch_file / sample_grid           SurfacePatch.hpp:313-371, :199-242
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <filesystem>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "../../include/bbrt.h"
+#include "dscene.h"
+#include "scene_host.hpp"
+
+namespace bbrt {
+cudaError_t launch_trace(const DScene& S, const TraceArgs& A, cudaStream_t stream, int sm_count);
+cudaError_t launch_query(const DScene& S, const QueryArgs& Q, cudaStream_t stream);
+}  // namespace bbrt
+
+namespace {
+
+thread_local std::string g_error;
+
+int fail(int code, const std::string& msg) {
+    g_error = msg;
+    return code;
+}
+
+#define BBRT_CUDA(call)                                                                   \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return fail(BBRT_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// A grow-only device buffer.
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    cudaError_t ensure(size_t n) {
+        if (n <= bytes) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaMalloc(&p, n);
+        if (e == cudaSuccess) bytes = n;
+        return e;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+};
+
+}  // namespace
+
+struct bbrt_scene {
+    bbrt::HostScene host;
+    bbrt::CullTables cull;
+    bbrt::DScene dev;
+    bool uploaded = false;
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[4] = { nullptr, nullptr, nullptr, nullptr };
+    std::vector<void*> allocs;
+    long long device_bytes = 0;
+    DevBuf stats, work, in_o, in_d, o_status, o_bounce, o_dir, o_end, o_hobj, o_hpt, o_huv, o_eobj, o_eval,
+        counts, hits;
+    std::mutex mu;
+
+    ~bbrt_scene() {
+        for (void* p : allocs) cudaFree(p);
+        for (DevBuf* b : { &stats, &work, &in_o, &in_d, &o_status, &o_bounce, &o_dir, &o_end, &o_hobj, &o_hpt,
+                           &o_huv, &o_eobj, &o_eval, &counts, &hits })
+            b->release();
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    template <class T>
+    int upload(const std::vector<T>& v, const T*& dst) {
+        if (v.empty()) { dst = nullptr; return BBRT_OK; }
+        void* p = nullptr;
+        BBRT_CUDA(cudaMalloc(&p, v.size() * sizeof(T)));
+        allocs.push_back(p);
+        device_bytes += static_cast<long long>(v.size() * sizeof(T));
+        BBRT_CUDA(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+        dst = static_cast<const T*>(p);
+        return BBRT_OK;
+    }
+};
+
+namespace {
+
+int ensure_uploaded(bbrt_scene* s) {
+    if (s->uploaded) return BBRT_OK;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0)
+        return fail(BBRT_ERR_CUDA, "bbrt: no CUDA device available (the trace path has no CPU fallback)");
+    BBRT_CUDA(cudaGetDevice(&s->device));
+    BBRT_CUDA(cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, s->device));
+    BBRT_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    for (auto& e : s->ev) BBRT_CUDA(cudaEventCreate(&e));
+    const bbrt::HostScene& H = s->host;
+    bbrt::DScene& D = s->dev;
+    D = bbrt::DScene();
+    D.n_objects = H.n_objects;
+    D.n_nodes = static_cast<int>(H.nodes.size());
+    D.coarse_n = H.coarse_n;
+    D.newton_max_iters = H.cfg.newton_max_iters;
+    D.newton_tol = H.cfg.newton_tol;
+    D.scene_diagonal = H.scene_diagonal;
+    D.max_patch_sagitta = H.max_patch_sagitta;
+    D.eps_factor = H.cfg.self_intersect_eps_factor;
+    D.sag_factor = H.cfg.sagitta_clearance_factor;
+    D.backface_tol = H.cfg.backface_tol;
+    std::vector<double> nbox(6 * H.nodes.size());
+    std::vector<int> nlink(4 * H.nodes.size());
+    for (size_t k = 0; k < H.nodes.size(); ++k) {
+        std::memcpy(&nbox[6 * k], H.nodes[k].box, sizeof(double) * 6);
+        nlink[4 * k] = H.nodes[k].right;
+        nlink[4 * k + 1] = H.nodes[k].start;
+        nlink[4 * k + 2] = H.nodes[k].count;
+        nlink[4 * k + 3] = H.nodes[k].axis;
+    }
+    std::vector<int> dims(2 * static_cast<size_t>(H.n_patches));
+    for (int q = 0; q < H.n_patches; ++q) { dims[2 * q] = H.p_imax[q]; dims[2 * q + 1] = H.p_jmax[q]; }
+    int rc;
+    if ((rc = s->upload(nbox, D.node_box))) return rc;
+    if ((rc = s->upload(nlink, D.node_link))) return rc;
+    if ((rc = s->upload(H.leaf_objects, D.leaf_objects))) return rc;
+    if ((rc = s->upload(H.kind, D.obj_kind))) return rc;
+    if ((rc = s->upload(H.sub, D.obj_sub))) return rc;
+    if ((rc = s->upload(H.padding, D.obj_pad))) return rc;
+    if ((rc = s->upload(dims, D.p_dims))) return rc;
+    if ((rc = s->upload(H.p_node_off, D.p_node_off))) return rc;
+    if ((rc = s->upload(H.p_field_off, D.p_field_off))) return rc;
+    if ((rc = s->upload(H.p_nodes, D.p_nodes))) return rc;
+    if ((rc = s->upload(H.p_fields, D.p_fields))) return rc;
+    if ((rc = s->upload(H.coarse_uv, D.coarse_uv))) return rc;
+    if ((rc = s->upload(H.c_xyz, D.c_xyz))) return rc;
+    if ((rc = s->upload(H.c_cell, D.c_cell))) return rc;
+    if ((rc = s->upload(H.tri, D.tri))) return rc;
+    if (s->cull.enabled) {
+        if ((rc = s->upload(s->cull.cell_box, D.c_cell_box))) return rc;
+        if ((rc = s->upload(s->cull.block_box, D.c_block_box))) return rc;
+        D.block_cells = s->cull.block_cells;
+        D.n_blocks_side = s->cull.n_blocks_side;
+        D.cull_enabled = 1;
+        D.cull_a = s->cull.a;
+        D.cull_h = s->cull.h;
+        D.cull_b = s->cull.b;
+        D.cull_coord = s->cull.coord;
+        D.cull_radius = s->cull.radius;
+        for (int a = 0; a < 3; ++a) D.cull_center[a] = s->cull.center[a];
+    }
+    BBRT_CUDA(s->stats.ensure(sizeof(long long) * bbrt::ST_COUNT));
+    BBRT_CUDA(s->work.ensure(sizeof(unsigned long long)));
+    s->uploaded = true;
+    return BBRT_OK;
+}
+
+int create_scene(const bbrt_object_desc* objects, int n, const bbrt_config* cfg, bbrt_scene_t* out) {
+    if (!out) return fail(BBRT_ERR_ARG, "bbrt_scene_create: out is NULL");
+    *out = nullptr;
+    bbrt_config c;
+    bbrt_config_init(&c);
+    if (cfg) c = *cfg;
+    std::unique_ptr<bbrt_scene> s(new bbrt_scene());
+    try {
+        bbrt::build_host_scene(objects, n, c, s->host);
+        bbrt::build_cull_tables(s->host, s->cull);
+    } catch (const std::invalid_argument& e) {
+        return fail(BBRT_ERR_ARG, e.what());
+    } catch (const std::runtime_error& e) {
+        return fail(BBRT_ERR_FORMAT, e.what());
+    } catch (const std::bad_alloc&) {
+        return fail(BBRT_ERR_NOMEM, "bbrt_scene_create: out of host memory");
+    }
+    *out = s.release();
+    return BBRT_OK;
+}
+
+// Reads a list of patch files and builds the scene from them.
+int create_from_files(const std::vector<std::string>& paths, const bbrt_config* cfg, bbrt_scene_t* out) {
+    std::vector<bbrt::PatchFileData> files(paths.size());
+    try {
+        for (size_t k = 0; k < paths.size(); ++k) bbrt::read_patch_file(paths[k], files[k]);
+    } catch (const std::runtime_error& e) {
+        const std::string m = e.what();
+        return fail(m.find("cannot open") != std::string::npos ? BBRT_ERR_IO : BBRT_ERR_FORMAT, m);
+    }
+    std::vector<bbrt_patch_desc> pd(files.size());
+    std::vector<bbrt_object_desc> od(files.size());
+    for (size_t k = 0; k < files.size(); ++k) {
+        pd[k] = bbrt::patch_desc_of(files[k]);
+        od[k] = bbrt_object_desc{};
+        od[k].kind = BBRT_OBJ_PATCH;
+        od[k].patch = &pd[k];
+    }
+    return create_scene(od.data(), static_cast<int>(od.size()), cfg, out);
+}
+
+cudaStream_t pick_stream(bbrt_scene* s, void* stream) {
+    return stream ? static_cast<cudaStream_t>(stream) : s->stream;
+}
+
+void fill_stats(bbrt_scene* s, const long long* st, long long n, float kernel_ms, float total_ms,
+                bbrt_trace_stats* out) {
+    std::memset(out, 0, sizeof *out);
+    out->rays = n;
+    out->bounces = st[bbrt::ST_BOUNCES];
+    out->queries = st[bbrt::ST_QUERIES];
+    out->node_tests = st[bbrt::ST_NODE_TESTS];
+    out->patch_tests = st[bbrt::ST_PATCH_TESTS];
+    out->cell_tests = st[bbrt::ST_CELL_TESTS];
+    out->tri_tests = st[bbrt::ST_TRI_TESTS];
+    out->newton_iters = st[bbrt::ST_NEWTON_ITERS];
+    out->newton_iters_fp32 = st[bbrt::ST_NEWTON_ITERS_FP32];
+    for (int k = 0; k < BBRT_RAY_STATUS_COUNT; ++k) out->status_hist[k] = st[bbrt::ST_HIST0 + k];
+    out->kernel_ms = kernel_ms;
+    out->total_ms = total_ms;
+    (void)s;
+}
+
+// Launches the trace kernel on device arrays.  hit_counts (device, may be
+// null) receives per-object counts for bounces with index >= count_from.
+int run_trace_device(bbrt_scene* s, const double* d_o, const double* d_d, long long n, int max_bounces,
+                     const bbrt_trace_out* out_dev, unsigned long long* hit_counts, int count_from,
+                     cudaStream_t st, bool want_stats, long long* host_stats, float* kernel_ms) {
+    bbrt::TraceArgs A;
+    A.origins = d_o;
+    A.dirs = d_d;
+    A.n = n;
+    A.max_bounces = max_bounces;
+    A.cull = s->host.cfg.cull;
+    if (out_dev) {
+        A.record = out_dev->record_bounces;
+        A.status = out_dev->status;
+        A.bounce_count = out_dev->bounce_count;
+        A.exit_dir = out_dev->exit_dir;
+        A.end_point = out_dev->end_point;
+        A.hit_object = out_dev->hit_object;
+        A.hit_point = out_dev->hit_point;
+        A.hit_uv = out_dev->hit_uv;
+        A.err_object = out_dev->err_object;
+        A.err_value = out_dev->err_value;
+    }
+    if (A.record < 0) return fail(BBRT_ERR_ARG, "bbrt_trace: record_bounces < 0");
+    A.hit_counts = hit_counts;
+    A.count_from = count_from;
+    A.stats = want_stats ? static_cast<long long*>(s->stats.p) : nullptr;
+    A.work_counter = static_cast<unsigned long long*>(s->work.p);
+    if (want_stats) BBRT_CUDA(cudaMemsetAsync(s->stats.p, 0, sizeof(long long) * bbrt::ST_COUNT, st));
+    BBRT_CUDA(cudaMemsetAsync(s->work.p, 0, sizeof(unsigned long long), st));
+    BBRT_CUDA(cudaEventRecord(s->ev[0], st));
+    BBRT_CUDA(bbrt::launch_trace(s->dev, A, st, s->sm_count));
+    BBRT_CUDA(cudaEventRecord(s->ev[1], st));
+    if (want_stats) {
+        BBRT_CUDA(cudaMemcpyAsync(host_stats, s->stats.p, sizeof(long long) * bbrt::ST_COUNT,
+                                  cudaMemcpyDeviceToHost, st));
+    }
+    if (kernel_ms) {
+        BBRT_CUDA(cudaEventSynchronize(s->ev[1]));
+        BBRT_CUDA(cudaEventElapsedTime(kernel_ms, s->ev[0], s->ev[1]));
+    }
+    return BBRT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+BBRT_API const char* bbrt_version(void) { return "bbrt-b200 0.1 (sm_100a)"; }
+
+BBRT_API const char* bbrt_last_error(void) { return g_error.c_str(); }
+
+BBRT_API void bbrt_config_init(bbrt_config* c) {
+    if (!c) return;
+    c->coarse_grid_n = 100;
+    c->newton_max_iters = 20;
+    c->newton_tol = 1e-3;
+    c->leaf_threshold = 4;
+    c->self_intersect_eps_factor = 1e-9;
+    c->sagitta_clearance_factor = 5.0;
+    c->backface_tol = 1e-9;
+    c->precision = BBRT_PREC_FP64;
+    c->guess = BBRT_GUESS_TRIANGLE;
+    c->cull = 1;
+}
+
+BBRT_API int bbrt_device_count(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+    return n;
+}
+
+BBRT_API int bbrt_patch_file_read(const char* path, bbrt_patch_file* out) {
+    if (!path || !out) return fail(BBRT_ERR_ARG, "bbrt_patch_file_read: NULL argument");
+    std::memset(out, 0, sizeof *out);
+    auto* d = new (std::nothrow) bbrt::PatchFileData();
+    if (!d) return fail(BBRT_ERR_NOMEM, "bbrt_patch_file_read: out of memory");
+    try {
+        bbrt::read_patch_file(path, *d);
+    } catch (const std::runtime_error& e) {
+        delete d;
+        const std::string m = e.what();
+        return fail(m.find("cannot open") != std::string::npos ? BBRT_ERR_IO : BBRT_ERR_FORMAT, m);
+    }
+    out->desc = bbrt::patch_desc_of(*d);
+    out->mask = d->mask.data();
+    out->dS = d->f[9].data();
+    for (int k = 0; k < 4; ++k) out->edge_flags[k] = d->edge_flags[k];
+    out->storage_ = d;
+    return BBRT_OK;
+}
+
+BBRT_API void bbrt_patch_file_free(bbrt_patch_file* f) {
+    if (!f) return;
+    delete static_cast<bbrt::PatchFileData*>(f->storage_);
+    std::memset(f, 0, sizeof *f);
+}
+
+BBRT_API int bbrt_scene_create(const bbrt_object_desc* objects, int n_objects, const bbrt_config* cfg,
+                               bbrt_scene_t* out) {
+    return create_scene(objects, n_objects, cfg, out);
+}
+
+BBRT_API int bbrt_scene_create_from_dir(const char* directory, const bbrt_config* cfg, bbrt_scene_t* out) {
+    namespace fs = std::filesystem;
+    if (!directory || !out) return fail(BBRT_ERR_ARG, "bbrt_scene_create_from_dir: NULL argument");
+    std::vector<fs::path> files;
+    try {
+        if (!fs::exists(directory) || !fs::is_directory(directory))
+            return fail(BBRT_ERR_IO, std::string("RayTracingDriver: not a directory: ") + directory);
+        for (const auto& entry : fs::directory_iterator(directory))
+            if (entry.is_regular_file() && entry.path().extension() == ".txt") files.push_back(entry.path());
+    } catch (const fs::filesystem_error& e) {
+        return fail(BBRT_ERR_IO, e.what());
+    }
+    std::sort(files.begin(), files.end());
+    if (files.empty())
+        return fail(BBRT_ERR_IO, std::string("RayTracingDriver: no *.txt patch files found in: ") + directory);
+    std::vector<std::string> paths;
+    for (const auto& f : files) paths.push_back(f.string());
+    return create_from_files(paths, cfg, out);
+}
+
+BBRT_API int bbrt_scene_create_from_range(const char* directory, const char* file_prefix, int first, int last,
+                                          const bbrt_config* cfg, bbrt_scene_t* out) {
+    if (!directory || !file_prefix || !out) return fail(BBRT_ERR_ARG, "bbrt_scene_create_from_range: NULL argument");
+    if (last < first)
+        return fail(BBRT_ERR_ARG, "RayTracingDriver: empty patch index range [" + std::to_string(first) + ", " +
+                                      std::to_string(last) + "]");
+    std::vector<std::string> paths;
+    for (int i = first; i <= last; ++i) paths.push_back(std::string(directory) + file_prefix + std::to_string(i) + ".txt");
+    return create_from_files(paths, cfg, out);
+}
+
+BBRT_API void bbrt_scene_destroy(bbrt_scene_t s) { delete s; }
+
+BBRT_API int bbrt_scene_upload(bbrt_scene_t s) {
+    if (!s) return fail(BBRT_ERR_ARG, "bbrt_scene_upload: NULL scene");
+    std::lock_guard<std::mutex> g(s->mu);
+    return ensure_uploaded(s);
+}
+
+BBRT_API int bbrt_scene_info_get(bbrt_scene_t s, bbrt_scene_info* out) {
+    if (!s || !out) return fail(BBRT_ERR_ARG, "bbrt_scene_info_get: NULL argument");
+    out->n_objects = s->host.n_objects;
+    out->n_nodes = static_cast<int>(s->host.nodes.size());
+    out->max_depth = s->host.max_depth;
+    out->scene_diagonal = s->host.scene_diagonal;
+    out->max_patch_sagitta = s->host.max_patch_sagitta;
+    out->device_bytes = s->device_bytes;
+    return BBRT_OK;
+}
+
+BBRT_API int bbrt_object_info_get(bbrt_scene_t s, int k, bbrt_object_info* out) {
+    if (!s || !out) return fail(BBRT_ERR_ARG, "bbrt_object_info_get: NULL argument");
+    if (k < 0 || k >= s->host.n_objects) return fail(BBRT_ERR_ARG, "bbrt_object_info_get: object out of range");
+    const bbrt::HostScene& H = s->host;
+    out->kind = H.kind[k];
+    out->zone_id = H.zone[k];
+    for (int a = 0; a < 3; ++a) {
+        out->box_min[a] = H.box[6 * k + a];
+        out->box_max[a] = H.box[6 * k + 3 + a];
+        out->centroid[a] = H.centroid[3 * k + a];
+    }
+    out->padding = H.padding[k];
+    return BBRT_OK;
+}
+
+BBRT_API int bbrt_patch_coarse_grid(bbrt_scene_t s, int k, int* n, double* u, double* v, double* xyz,
+                                    double* sag, double* nrm) {
+    if (!s) return fail(BBRT_ERR_ARG, "bbrt_patch_coarse_grid: NULL scene");
+    const bbrt::HostScene& H = s->host;
+    if (k < 0 || k >= H.n_objects || H.kind[k] != BBRT_OBJ_PATCH)
+        return fail(BBRT_ERR_ARG, "bbrt_patch_coarse_grid: not a patch object");
+    const int q = H.sub[k], cn = H.coarse_n, nc = cn - 1;
+    if (n) *n = cn;
+    if (u) std::memcpy(u, H.coarse_uv.data(), sizeof(double) * cn);
+    if (v) std::memcpy(v, H.coarse_uv.data(), sizeof(double) * cn);
+    if (xyz) std::memcpy(xyz, &H.c_xyz[3 * static_cast<size_t>(cn) * cn * q], sizeof(double) * 3 * cn * cn);
+    const double* cc = &H.c_cell[4 * static_cast<size_t>(nc) * nc * q];
+    for (int c = 0; c < nc * nc; ++c) {
+        if (sag) sag[c] = cc[4 * c + 3];
+        if (nrm) for (int a = 0; a < 3; ++a) nrm[3 * c + a] = cc[4 * c + a];
+    }
+    return BBRT_OK;
+}
+
+BBRT_API int bbrt_self_intersect_epsilon(bbrt_scene_t s, int k, double* eps) {
+    if (!s || !eps) return fail(BBRT_ERR_ARG, "bbrt_self_intersect_epsilon: NULL argument");
+    const bbrt::HostScene& H = s->host;
+    if (k >= H.n_objects) return fail(BBRT_ERR_ARG, "bbrt_self_intersect_epsilon: object out of range");
+    const double pad = (k >= 0) ? H.padding[k] : H.max_patch_sagitta;
+    const double a = H.cfg.self_intersect_eps_factor * H.scene_diagonal, b = H.cfg.sagitta_clearance_factor * pad;
+    *eps = (a < b) ? b : a;
+    return BBRT_OK;
+}
+
+BBRT_API int bbrt_intersect(bbrt_scene_t s, const double* origins, const double* dirs, long long n, int mode,
+                            int object, int flags, bbrt_hit* out, void* stream) {
+    if (!s || (n > 0 && (!origins || !dirs || !out))) return fail(BBRT_ERR_ARG, "bbrt_intersect: NULL argument");
+    if (n < 0) return fail(BBRT_ERR_ARG, "bbrt_intersect: n < 0");
+    if (mode < BBRT_QUERY_BVH || mode > BBRT_QUERY_OBJECT) return fail(BBRT_ERR_ARG, "bbrt_intersect: bad mode");
+    if (mode == BBRT_QUERY_OBJECT && (object < 0 || object >= s->host.n_objects))
+        return fail(BBRT_ERR_ARG, "bbrt_intersect: object out of range");
+    std::lock_guard<std::mutex> g(s->mu);
+    int rc = ensure_uploaded(s);
+    if (rc) return rc;
+    if (n == 0) return BBRT_OK;
+    cudaStream_t st = pick_stream(s, stream);
+    bbrt::QueryArgs Q;
+    Q.n = n;
+    Q.mode = mode;
+    Q.object = object;
+    Q.cull = s->host.cfg.cull;
+    if (flags & BBRT_DEVICE_PTRS) {
+        Q.origins = origins;
+        Q.dirs = dirs;
+        Q.out = out;
+        BBRT_CUDA(bbrt::launch_query(s->dev, Q, st));
+        return BBRT_OK;
+    }
+    const size_t vb = sizeof(double) * 3 * static_cast<size_t>(n);
+    BBRT_CUDA(s->in_o.ensure(vb));
+    BBRT_CUDA(s->in_d.ensure(vb));
+    BBRT_CUDA(s->hits.ensure(sizeof(bbrt_hit) * static_cast<size_t>(n)));
+    BBRT_CUDA(cudaMemcpyAsync(s->in_o.p, origins, vb, cudaMemcpyHostToDevice, st));
+    BBRT_CUDA(cudaMemcpyAsync(s->in_d.p, dirs, vb, cudaMemcpyHostToDevice, st));
+    Q.origins = static_cast<const double*>(s->in_o.p);
+    Q.dirs = static_cast<const double*>(s->in_d.p);
+    Q.out = s->hits.p;
+    BBRT_CUDA(bbrt::launch_query(s->dev, Q, st));
+    BBRT_CUDA(cudaMemcpyAsync(out, s->hits.p, sizeof(bbrt_hit) * static_cast<size_t>(n), cudaMemcpyDeviceToHost, st));
+    BBRT_CUDA(cudaStreamSynchronize(st));
+    return BBRT_OK;
+}
+
+BBRT_API int bbrt_trace(bbrt_scene_t s, const double* origins, const double* dirs, long long n, int max_bounces,
+                        int flags, const bbrt_trace_out* out, bbrt_trace_stats* stats, void* stream) {
+    if (!s) return fail(BBRT_ERR_ARG, "bbrt_trace: NULL scene");
+    if (n < 0) return fail(BBRT_ERR_ARG, "bbrt_trace: n < 0");
+    if (n > 0 && (!origins || !dirs)) return fail(BBRT_ERR_ARG, "bbrt_trace: NULL rays");
+    if (max_bounces < 0) return fail(BBRT_ERR_ARG, "bbrt_trace: max_bounces < 0");
+    if (out && out->record_bounces < 0) return fail(BBRT_ERR_ARG, "bbrt_trace: record_bounces < 0");
+    std::lock_guard<std::mutex> g(s->mu);
+    int rc = ensure_uploaded(s);
+    if (rc) return rc;
+    cudaStream_t st = pick_stream(s, stream);
+    long long hs[bbrt::ST_COUNT] = { 0 };
+    float kms = 0.0f;
+    if (n == 0) {
+        if (stats) fill_stats(s, hs, 0, 0.0f, 0.0f, stats);
+        return BBRT_OK;
+    }
+    if (flags & BBRT_DEVICE_PTRS) {
+        rc = run_trace_device(s, origins, dirs, n, max_bounces, out, nullptr, 1, st, stats != nullptr, hs,
+                              stats ? &kms : nullptr);
+        if (rc) return rc;
+        if (stats) {
+            BBRT_CUDA(cudaStreamSynchronize(st));
+            fill_stats(s, hs, n, kms, kms, stats);
+        }
+        return BBRT_OK;
+    }
+    // host arrays: stage through the scene's device buffers
+    const size_t N = static_cast<size_t>(n), K = out ? static_cast<size_t>(out->record_bounces) : 0;
+    BBRT_CUDA(cudaEventRecord(s->ev[2], st));
+    BBRT_CUDA(s->in_o.ensure(sizeof(double) * 3 * N));
+    BBRT_CUDA(s->in_d.ensure(sizeof(double) * 3 * N));
+    BBRT_CUDA(cudaMemcpyAsync(s->in_o.p, origins, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, st));
+    BBRT_CUDA(cudaMemcpyAsync(s->in_d.p, dirs, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, st));
+    bbrt_trace_out dev{};
+    struct Map { void* host; DevBuf* buf; size_t bytes; };
+    std::vector<Map> maps;
+    auto bind = [&](auto* host_ptr, DevBuf& b, size_t bytes, auto*& dev_field) -> int {
+        using T = std::remove_pointer_t<std::remove_reference_t<decltype(dev_field)>>;
+        if (!host_ptr || bytes == 0) { dev_field = nullptr; return BBRT_OK; }
+        BBRT_CUDA(b.ensure(bytes));
+        dev_field = static_cast<T*>(b.p);
+        maps.push_back({ static_cast<void*>(host_ptr), &b, bytes });
+        return BBRT_OK;
+    };
+    if (out) {
+        dev.record_bounces = out->record_bounces;
+        if ((rc = bind(out->status, s->o_status, sizeof(int) * N, dev.status))) return rc;
+        if ((rc = bind(out->bounce_count, s->o_bounce, sizeof(int) * N, dev.bounce_count))) return rc;
+        if ((rc = bind(out->exit_dir, s->o_dir, sizeof(double) * 3 * N, dev.exit_dir))) return rc;
+        if ((rc = bind(out->end_point, s->o_end, sizeof(double) * 3 * N, dev.end_point))) return rc;
+        if ((rc = bind(out->hit_object, s->o_hobj, sizeof(int) * N * K, dev.hit_object))) return rc;
+        if ((rc = bind(out->hit_point, s->o_hpt, sizeof(double) * 3 * N * K, dev.hit_point))) return rc;
+        if ((rc = bind(out->hit_uv, s->o_huv, sizeof(double) * 2 * N * K, dev.hit_uv))) return rc;
+        if ((rc = bind(out->err_object, s->o_eobj, sizeof(int) * N, dev.err_object))) return rc;
+        if ((rc = bind(out->err_value, s->o_eval, sizeof(double) * 2 * N, dev.err_value))) return rc;
+    }
+    rc = run_trace_device(s, static_cast<const double*>(s->in_o.p), static_cast<const double*>(s->in_d.p), n,
+                          max_bounces, out ? &dev : nullptr, nullptr, 1, st, stats != nullptr, hs, nullptr);
+    if (rc) return rc;
+    for (const Map& m : maps)
+        BBRT_CUDA(cudaMemcpyAsync(m.host, m.buf->p, m.bytes, cudaMemcpyDeviceToHost, st));
+    BBRT_CUDA(cudaEventRecord(s->ev[3], st));
+    BBRT_CUDA(cudaStreamSynchronize(st));
+    if (stats) {
+        float tot = 0.0f;
+        BBRT_CUDA(cudaEventElapsedTime(&kms, s->ev[0], s->ev[1]));
+        BBRT_CUDA(cudaEventElapsedTime(&tot, s->ev[2], s->ev[3]));
+        fill_stats(s, hs, n, kms, tot, stats);
+    }
+    return BBRT_OK;
+}
+
+BBRT_API int bbrt_plane_source(bbrt_scene_t s, const double c0[3], const double c1[3], const double dir[3], int nx,
+                               int ny, int max_bounces, int count_direct_hit, long long* hit_counts,
+                               bbrt_trace_stats* stats, void* stream) {
+    if (!s || !c0 || !c1 || !dir || !hit_counts) return fail(BBRT_ERR_ARG, "bbrt_plane_source: NULL argument");
+    if (nx < 1 || ny < 1) return fail(BBRT_ERR_ARG, "PlaneSourceDriver::run: nx and ny must both be >= 1");
+    const double dl2 = dir[0] * dir[0] + dir[1] * dir[1] + dir[2] * dir[2];
+    if (dl2 < 1e-300) return fail(BBRT_ERR_ARG, "PlaneSourceDriver::run: direction has zero length");
+    if (max_bounces < 0) return fail(BBRT_ERR_ARG, "bbrt_plane_source: max_bounces < 0");
+    // build_plane_grid (PlaneSourceDriver.hpp:190-243)
+    const double scale = std::max({ 1.0, std::fabs(c0[0]), std::fabs(c0[1]), std::fabs(c0[2]), std::fabs(c1[0]),
+                                    std::fabs(c1[1]), std::fabs(c1[2]) });
+    const double tol = 1e-9 * scale;
+    int constant_axis = -1, matches = 0;
+    for (int a = 0; a < 3; ++a)
+        if (std::fabs(c0[a] - c1[a]) < tol) { constant_axis = a; ++matches; }
+    if (matches != 1)
+        return fail(BBRT_ERR_ARG,
+                    "PlaneSourceDriver: corner0 and corner1 must agree in exactly one coordinate to define an "
+                    "axis-aligned plane (got " + std::to_string(matches) + " matching coordinates)");
+    int aa = -1, ab = -1;
+    for (int a = 0; a < 3; ++a) {
+        if (a == constant_axis) continue;
+        if (aa < 0) aa = a; else ab = a;
+    }
+    const size_t N = static_cast<size_t>(nx) * ny;
+    std::vector<double> src(3 * N), dirs(3 * N);
+    std::vector<double> ga(nx), gb(ny);
+    for (int i = 0; i < nx; ++i) ga[i] = (nx == 1) ? c0[aa] : c0[aa] + (c1[aa] - c0[aa]) * static_cast<double>(i) / (nx - 1);
+    for (int j = 0; j < ny; ++j) gb[j] = (ny == 1) ? c0[ab] : c0[ab] + (c1[ab] - c0[ab]) * static_cast<double>(j) / (ny - 1);
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j) {
+            double* p = &src[3 * (static_cast<size_t>(i) * ny + j)];
+            p[constant_axis] = c0[constant_axis];
+            p[aa] = ga[i];
+            p[ab] = gb[j];
+        }
+    for (size_t k = 0; k < N; ++k) { dirs[3 * k] = dir[0]; dirs[3 * k + 1] = dir[1]; dirs[3 * k + 2] = dir[2]; }
+    std::lock_guard<std::mutex> g(s->mu);
+    int rc = ensure_uploaded(s);
+    if (rc) return rc;
+    cudaStream_t st = pick_stream(s, stream);
+    BBRT_CUDA(s->in_o.ensure(sizeof(double) * 3 * N));
+    BBRT_CUDA(s->in_d.ensure(sizeof(double) * 3 * N));
+    BBRT_CUDA(s->counts.ensure(sizeof(unsigned long long) * s->host.n_objects));
+    BBRT_CUDA(cudaMemcpyAsync(s->in_o.p, src.data(), sizeof(double) * 3 * N, cudaMemcpyHostToDevice, st));
+    BBRT_CUDA(cudaMemcpyAsync(s->in_d.p, dirs.data(), sizeof(double) * 3 * N, cudaMemcpyHostToDevice, st));
+    BBRT_CUDA(cudaMemsetAsync(s->counts.p, 0, sizeof(unsigned long long) * s->host.n_objects, st));
+    long long hs[bbrt::ST_COUNT] = { 0 };
+    float kms = 0.0f;
+    rc = run_trace_device(s, static_cast<const double*>(s->in_o.p), static_cast<const double*>(s->in_d.p),
+                          static_cast<long long>(N), max_bounces, nullptr,
+                          static_cast<unsigned long long*>(s->counts.p), count_direct_hit ? 0 : 1, st,
+                          stats != nullptr, hs, stats ? &kms : nullptr);
+    if (rc) return rc;
+    std::vector<unsigned long long> c(s->host.n_objects);
+    BBRT_CUDA(cudaMemcpyAsync(c.data(), s->counts.p, sizeof(unsigned long long) * c.size(), cudaMemcpyDeviceToHost, st));
+    BBRT_CUDA(cudaStreamSynchronize(st));
+    for (size_t k = 0; k < c.size(); ++k) hit_counts[k] = static_cast<long long>(c[k]);
+    if (stats) fill_stats(s, hs, static_cast<long long>(N), kms, kms, stats);
+    return BBRT_OK;
+}
+
+BBRT_API int bbrt_patch_sample_grid(const bbrt_patch_desc* p, int n, double* xyz, double* normal, double* dxdu) {
+    if (!p || !xyz || !normal || !dxdu) return fail(BBRT_ERR_ARG, "bbrt_patch_sample_grid: NULL argument");
+    if (n < 1) return fail(BBRT_ERR_ARG, "bbrt_patch_sample_grid: n must be >= 1");
+    if (p->imax < 1 || p->jmax < 1) return fail(BBRT_ERR_ARG, "bbrt_patch_sample_grid: empty patch");
+    bbrt::sample_grid(*p, n, xyz, normal, dxdu);
+    return BBRT_OK;
+}
+
+BBRT_API int bbrt_bounce_map(bbrt_scene_t s, const bbrt_patch_desc* samples, int n_sample, int grid_n, int theta_n,
+                             int phi_n, double cone_angle_deg, int max_bounces, int* max_out, int* err_out,
+                             int* best_out, bbrt_trace_stats* stats, void* stream) {
+    if (!s || !samples || !max_out || !err_out) return fail(BBRT_ERR_ARG, "bbrt_bounce_map: NULL argument");
+    if (grid_n < 2) return fail(BBRT_ERR_ARG, "BounceMapDriver::run: position_grid_n must be >= 2");
+    if (theta_n < 1 || phi_n < 1) return fail(BBRT_ERR_ARG, "BounceMapDriver::run: theta_n and phi_n must both be >= 1");
+    if (!(cone_angle_deg > 0.0) || cone_angle_deg > 180.0)
+        return fail(BBRT_ERR_ARG, "BounceMapDriver::run: cone_angle_deg must be in (0, 180]");
+    if (n_sample < 1) return fail(BBRT_ERR_ARG, "bbrt_bounce_map: no sample patches");
+    // Ray generation on the host, in the reference's arithmetic
+    // (BounceMapDriver.hpp:119-237, build_tangent_frame :499-519).
+    const double kTwoPi = 6.283185307179586476925286766559;
+    const double cos_max = std::cos(cone_angle_deg / 2.0 * kTwoPi / 360.0);
+    const long long per = static_cast<long long>(grid_n) * grid_n, dirs_per = static_cast<long long>(theta_n) * phi_n;
+    const long long N = static_cast<long long>(n_sample) * per * dirs_per;
+    std::vector<double> org(3 * N), dir(3 * N);
+    std::vector<double> cphi(phi_n), sphi(phi_n), mu(theta_n), sth(theta_n);
+    for (int ti = 0; ti < theta_n; ++ti) {
+        mu[ti] = cos_max + (static_cast<double>(ti) + 0.5) / static_cast<double>(theta_n) * (1.0 - cos_max);
+        sth[ti] = std::sqrt(std::max(0.0, 1.0 - mu[ti] * mu[ti]));
+    }
+    for (int pj = 0; pj < phi_n; ++pj) {
+        const double phi = (static_cast<double>(pj) + 0.5) * kTwoPi / static_cast<double>(phi_n);
+        cphi[pj] = std::cos(phi);
+        sphi[pj] = std::sin(phi);
+    }
+    try {
+        for (int p = 0; p < n_sample; ++p) {
+            bbrt::HostScene one;
+            bbrt_object_desc od{};
+            od.kind = BBRT_OBJ_PATCH;
+            od.patch = &samples[p];
+            bbrt::build_host_scene(&od, 1, s->host.cfg, one);
+            const double a = s->host.cfg.self_intersect_eps_factor * s->host.scene_diagonal;
+            const double b = s->host.cfg.sagitta_clearance_factor * one.padding[0];
+            const double eps = (a < b) ? b : a;
+            std::vector<double> xyz(3 * per), nrm(3 * per), du(3 * per);
+            bbrt::sample_grid(samples[p], grid_n, xyz.data(), nrm.data(), du.data());
+            for (long long k = 0; k < per; ++k) {
+                const double* P = &xyz[3 * k];
+                double n0 = nrm[3 * k], n1 = nrm[3 * k + 1], n2 = nrm[3 * k + 2];
+                const double nl = std::sqrt(n0 * n0 + n1 * n1 + n2 * n2);
+                n0 /= nl; n1 /= nl; n2 /= nl;
+                const double d0 = du[3 * k], d1 = du[3 * k + 1], d2 = du[3 * k + 2];
+                const double du2 = d0 * d0 + d1 * d1 + d2 * d2, dn = d0 * n0 + d1 * n1 + d2 * n2;
+                const double q0 = d0 - dn * n0, q1 = d1 - dn * n1, q2 = d2 - dn * n2;
+                const double qq = q0 * q0 + q1 * q1 + q2 * q2;
+                double t1[3], t2[3];
+                if (qq > 1e-6 * 1e-6 * du2) {
+                    const double l = std::sqrt(q0 * q0 + q1 * q1 + q2 * q2);
+                    t1[0] = q0 / l; t1[1] = q1 / l; t1[2] = q2 / l;
+                } else {
+                    double ax[3] = { 0, 0, 0 };
+                    if (std::fabs(n0) <= std::fabs(n1) && std::fabs(n0) <= std::fabs(n2)) ax[0] = 1.0;
+                    else if (std::fabs(n1) <= std::fabs(n2)) ax[1] = 1.0;
+                    else ax[2] = 1.0;
+                    const double c0v = n1 * ax[2] - n2 * ax[1], c1v = n2 * ax[0] - n0 * ax[2], c2v = n0 * ax[1] - n1 * ax[0];
+                    const double l = std::sqrt(c0v * c0v + c1v * c1v + c2v * c2v);
+                    t1[0] = c0v / l; t1[1] = c1v / l; t1[2] = c2v / l;
+                }
+                t2[0] = n1 * t1[2] - n2 * t1[1];
+                t2[1] = n2 * t1[0] - n0 * t1[2];
+                t2[2] = n0 * t1[1] - n1 * t1[0];
+                const double o0 = P[0] + n0 * eps, o1 = P[1] + n1 * eps, o2 = P[2] + n2 * eps;
+                for (int ti = 0; ti < theta_n; ++ti)
+                    for (int pj = 0; pj < phi_n; ++pj) {
+                        const long long r = ((static_cast<long long>(p) * per + k) * dirs_per) + ti * phi_n + pj;
+                        org[3 * r] = o0; org[3 * r + 1] = o1; org[3 * r + 2] = o2;
+                        const double st_ = sth[ti], m = mu[ti], cp = cphi[pj], sp = sphi[pj];
+                        dir[3 * r] = t1[0] * st_ * cp + t2[0] * st_ * sp + n0 * m;
+                        dir[3 * r + 1] = t1[1] * st_ * cp + t2[1] * st_ * sp + n1 * m;
+                        dir[3 * r + 2] = t1[2] * st_ * cp + t2[2] * st_ * sp + n2 * m;
+                    }
+            }
+        }
+    } catch (const std::exception& e) {
+        return fail(BBRT_ERR_ARG, e.what());
+    }
+    std::vector<int> status(N), bounces(N);
+    bbrt_trace_out o{};
+    o.status = status.data();
+    o.bounce_count = bounces.data();
+    const int rc = bbrt_trace(s, org.data(), dir.data(), N, max_bounces, 0, &o, stats, stream);
+    if (rc) return rc;
+    // per point: max over non-Error directions, Error count, first maximum
+    for (long long q = 0; q < static_cast<long long>(n_sample) * per; ++q) {
+        int best = 0, nerr = 0, bdir = -1;
+        for (long long k = 0; k < dirs_per; ++k) {
+            const long long r = q * dirs_per + k;
+            const int stt = status[r];
+            if (stt != BBRT_RAY_ESCAPED && stt != BBRT_RAY_MAX_BOUNCES) { ++nerr; continue; }
+            if (bdir < 0 || bounces[r] > best) bdir = static_cast<int>(k);
+            best = std::max(best, bounces[r]);
+        }
+        max_out[q] = best;
+        err_out[q] = nerr;
+        if (best_out) best_out[q] = bdir;
+    }
+    return BBRT_OK;
+}
+
+}  // extern "C"

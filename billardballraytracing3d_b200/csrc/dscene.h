@@ -1,0 +1,97 @@
+// Device-side scene view and launch descriptors shared by the host C ABI
+// (capi.cpp) and the kernels (*.cu).  Plain pointers into one scene's device
+// allocation; passed to kernels by value.
+#pragma once
+
+#include <cstdint>
+
+namespace bbrt {
+
+struct DScene {
+    int n_objects = 0;
+    int n_nodes = 0;
+    int coarse_n = 0;               // coarse grid is coarse_n x coarse_n for every patch
+    int newton_max_iters = 20;
+    double newton_tol = 1e-3;
+    double scene_diagonal = 0.0;
+    double max_patch_sagitta = 0.0;
+    double eps_factor = 1e-9;       // kSelfIntersectEpsilonFactor
+    double sag_factor = 5.0;        // kSagittaClearanceFactor
+    double backface_tol = 1e-9;     // kBackfaceHitTol
+
+    // BVH (depth-first, left child = parent + 1)
+    const double* node_box = nullptr;      // [n_nodes][6]  min xyz, max xyz
+    const int* node_link = nullptr;        // [n_nodes][4]  right (-1 leaf), start, count, axis
+    const int* leaf_objects = nullptr;
+
+    // objects
+    const int* obj_kind = nullptr;         // BBRT_OBJ_*
+    const int* obj_sub = nullptr;          // patch or triangle index
+    const double* obj_pad = nullptr;       // self_intersect_padding
+
+    // patches
+    const int* p_dims = nullptr;           // [n_patches][2] imax, jmax
+    const long long* p_node_off = nullptr; // un[imax] vn[jmax] uw[imax] vw[jmax]
+    const long long* p_field_off = nullptr;// node-major, 12 doubles per node
+    const double* p_nodes = nullptr;
+    const double* p_fields = nullptr;
+    const double* coarse_uv = nullptr;     // [coarse_n]
+    const double* c_xyz = nullptr;         // [n_patches][coarse_n^2][3]
+    const double* c_cell = nullptr;        // [n_patches][(coarse_n-1)^2][4] normal xyz, sagitta
+    const float* c_cell_box = nullptr;     // [n_patches][(coarse_n-1)^2][6] cell AABB (cull)
+    const float* c_block_box = nullptr;    // [n_patches][n_blocks][6] block AABB (cull)
+    int block_cells = 4;                   // a block is block_cells x block_cells cells
+    int n_blocks_side = 0;                 // blocks per side
+    // Conservative inflation of the cull boxes for a ray with origin o:
+    //   L     = |o - cull_center| + cull_radius   (bounds |o - v| for every vertex v)
+    //   delta = cull_a * (L + cull_h) + cull_b * (L + |o| + cull_coord)
+    // cull_a covers the FP64 Moller-Trumbore rounding (hits accepted up to that
+    // far outside a triangle), cull_b the FP32 slab test's own rounding.
+    int cull_enabled = 0;
+    double cull_a = 0.0, cull_h = 0.0, cull_b = 0.0, cull_coord = 0.0;
+    double cull_center[3] = { 0.0, 0.0, 0.0 };
+    double cull_radius = 0.0;
+
+    // triangles
+    const double* tri = nullptr;           // [n_tri][9]
+};
+
+// Counter slots of the per-launch statistics buffer (long long each).
+enum StatSlot {
+    ST_BOUNCES = 0, ST_QUERIES, ST_NODE_TESTS, ST_PATCH_TESTS, ST_CELL_TESTS, ST_TRI_TESTS,
+    ST_NEWTON_ITERS, ST_NEWTON_ITERS_FP32, ST_HIST0, ST_COUNT = ST_HIST0 + 8
+};
+
+struct TraceArgs {
+    const double* origins = nullptr;   // [n][3]
+    const double* dirs = nullptr;      // [n][3]
+    long long n = 0;
+    int max_bounces = 0;
+    int record = 0;                    // K
+    int cull = 1;
+    int* status = nullptr;
+    int* bounce_count = nullptr;
+    double* exit_dir = nullptr;
+    double* end_point = nullptr;
+    int* hit_object = nullptr;         // [n][K]
+    double* hit_point = nullptr;       // [n][K][3]
+    double* hit_uv = nullptr;          // [n][K][2]
+    int* err_object = nullptr;
+    double* err_value = nullptr;       // [n][2]
+    unsigned long long* hit_counts = nullptr;  // per object (plane source), may be null
+    int count_from = 1;                // first bounce index that is counted
+    long long* stats = nullptr;        // [ST_COUNT], may be null
+    unsigned long long* work_counter = nullptr;  // persistent-launch ray counter (zeroed by host)
+};
+
+struct QueryArgs {
+    const double* origins = nullptr;
+    const double* dirs = nullptr;
+    long long n = 0;
+    int mode = 0;          // BBRT_QUERY_*
+    int object = 0;
+    int cull = 1;
+    void* out = nullptr;   // bbrt_hit[n]
+};
+
+}  // namespace bbrt

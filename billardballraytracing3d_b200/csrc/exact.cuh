@@ -1,0 +1,223 @@
+// Exact FP64 device primitives of the trace path.
+//
+// Each function reproduces one reference routine operation by operation:
+// the same association of every sum and product, the same comparisons, and
+// std::min/std::max's NaN behaviour written out as ternaries.  The
+// translation unit that includes this header is compiled with -fmad=false,
+// so no product is fused into an add: with IEEE division and sqrt the
+// results are bit-identical to the reference's x86-64 (SSE2) build.
+//
+// Reference (manuelarturosantana/BillardBallRayTracing3D):
+//   vec helpers, moller_trumbore     include/Utils/MollerTrumbore.hpp:13-64
+//   ray_box                          include/BVH.hpp:14-37
+//   lagrange_basis_1d                include/ScatObjects/SurfacePatch.hpp:518-538
+//   eval_scalar_field                SurfacePatch.hpp:542-555
+//   solve3x3                         SurfacePatch.hpp:559-579
+//   newton_refine                    SurfacePatch.hpp:593-660
+//   SurfacePatch::intersect stage 1  SurfacePatch.hpp:253-303, triangle_uv_centroid :499-510
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math_constants.h>
+
+#include "dscene.h"
+
+namespace bbrt {
+
+struct V3 { double x, y, z; };
+
+__device__ __forceinline__ V3 v3(double x, double y, double z) { V3 r; r.x = x; r.y = y; r.z = z; return r; }
+__device__ __forceinline__ V3 vsub(const V3& a, const V3& b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ V3 vcross(const V3& a, const V3& b) {
+    return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ double vdot(const V3& a, const V3& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ V3 vnormalize(const V3& v) {
+    const double len = sqrt(vdot(v, v));
+    return v3(v.x / len, v.y / len, v.z / len);
+}
+// std::max(a, b) / std::min(a, b)
+__device__ __forceinline__ double smax(double a, double b) { return (a < b) ? b : a; }
+__device__ __forceinline__ double smin(double a, double b) { return (b < a) ? b : a; }
+
+__device__ __forceinline__ V3 load3(const double* p) { return v3(p[0], p[1], p[2]); }
+
+// Moller-Trumbore with eps = 1e-9; returns the hit t.  Before the one FP64
+// division it rejects, from the signs and magnitudes of a = tvec.pvec and
+// det alone, every triangle whose u = fl(a * fl(1/det)) is certain to fall
+// outside [0, 1]: opposite signs with |a| > 1e-290 |det| give u < 0 (no
+// underflow to -0 possible), equal signs with |a| > |det| (1 + 1e-14) give
+// u > 1 (the rounding of 1/det and of the product is at most 2^-52
+// relative).  NaN or infinite operands fail both tests and take the exact
+// path, so the outcome is always the reference's.
+__device__ __forceinline__ bool mt_exact(const V3& o, const V3& d, const V3& v0, const V3& v1, const V3& v2,
+                                         double& t_out) {
+    const V3 e1 = vsub(v1, v0);
+    const V3 e2 = vsub(v2, v0);
+    const V3 pvec = vcross(d, e2);
+    const double det = vdot(e1, pvec);
+    if (fabs(det) < 1e-9) return false;
+    const V3 tvec = vsub(o, v0);
+    const double a = vdot(tvec, pvec);
+    const double fa = fabs(a), fd = fabs(det);
+    if ((a < 0.0) != (det < 0.0)) {
+        if (fa > fd * 1e-290) return false;
+    } else if (fa > fd * (1.0 + 1e-14)) {
+        return false;
+    }
+    const double inv_det = 1.0 / det;
+    const double u = a * inv_det;
+    if (u < 0.0 || u > 1.0) return false;
+    const V3 qvec = vcross(tvec, e1);
+    const double v = vdot(d, qvec) * inv_det;
+    if (v < 0.0 || u + v > 1.0) return false;
+    const double t = vdot(e2, qvec) * inv_det;
+    if (t < 1e-9) return false;
+    t_out = t;
+    return true;
+}
+
+// Plain Moller-Trumbore returning u, v too (Triangle objects).
+__device__ __forceinline__ bool mt_full(const V3& o, const V3& d, const V3& v0, const V3& v1, const V3& v2,
+                                        double& t_out, double& u_out, double& v_out) {
+    const V3 e1 = vsub(v1, v0);
+    const V3 e2 = vsub(v2, v0);
+    const V3 pvec = vcross(d, e2);
+    const double det = vdot(e1, pvec);
+    if (fabs(det) < 1e-9) return false;
+    const double inv_det = 1.0 / det;
+    const V3 tvec = vsub(o, v0);
+    const double u = vdot(tvec, pvec) * inv_det;
+    if (u < 0.0 || u > 1.0) return false;
+    const V3 qvec = vcross(tvec, e1);
+    const double v = vdot(d, qvec) * inv_det;
+    if (v < 0.0 || u + v > 1.0) return false;
+    const double t = vdot(e2, qvec) * inv_det;
+    if (t < 1e-9) return false;
+    t_out = t; u_out = u; v_out = v;
+    return true;
+}
+
+// Slab test of BVH.hpp:14-37 (tmin_out is never used by the caller there).
+__device__ __forceinline__ bool ray_box_exact(const V3& o, const double inv[3], const double* box, double best_t) {
+    double tmin = -CUDART_INF, tmax = CUDART_INF;
+    const double oo[3] = { o.x, o.y, o.z };
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        double t1 = (box[a] - oo[a]) * inv[a];
+        double t2 = (box[3 + a] - oo[a]) * inv[a];
+        if (inv[a] < 0.0) { const double s = t1; t1 = t2; t2 = s; }
+        tmin = smax(tmin, t1);
+        tmax = smin(tmax, t2);
+        if (tmax < tmin) return false;
+    }
+    if (tmin > best_t) return false;
+    return tmax >= smax(tmin, 0.0);
+}
+
+// Largest node count per axis the device Newton solve handles.
+constexpr int kDevMaxNodes = 16;
+
+// Second-form barycentric basis at x over N nodes (one-hot within 1e-12 of a node).
+__device__ __forceinline__ void basis_1d(const double* nodes, const double* w, int N, double x, double* b) {
+    for (int i = 0; i < N; ++i) b[i] = 0.0;
+    for (int i = 0; i < N; ++i)
+        if (fabs(x - nodes[i]) < 1.0e-12) { b[i] = 1.0; return; }
+    double denom = 0.0;
+    for (int i = 0; i < N; ++i) {
+        const double li = w[i] / (x - nodes[i]);
+        b[i] = li;
+        denom += li;
+    }
+    for (int i = 0; i < N; ++i) b[i] /= denom;
+}
+
+// Evaluates NF node-major fields (stride 12, starting at field `first`) at
+// basis (bu, bv) in the reference's order: per row i a left-to-right sum
+// over j, then the rows summed in i order, skipping rows whose bu_i is 0.
+template <int NF>
+__device__ __forceinline__ void eval_fields(const double* __restrict__ F, int I, int J, const double* bu,
+                                            const double* bv, int first, double* out) {
+#pragma unroll
+    for (int f = 0; f < NF; ++f) out[f] = 0.0;
+    for (int i = 0; i < I; ++i) {
+        const double li = bu[i];
+        if (li == 0.0) continue;
+        double rs[NF];
+#pragma unroll
+        for (int f = 0; f < NF; ++f) rs[f] = 0.0;
+        const double* row = F + static_cast<long long>(i) * J * 12 + first;
+        for (int j = 0; j < J; ++j) {
+            const double lj = bv[j];
+#pragma unroll
+            for (int f = 0; f < NF; ++f) rs[f] += lj * row[j * 12 + f];
+        }
+#pragma unroll
+        for (int f = 0; f < NF; ++f) out[f] += li * rs[f];
+    }
+}
+
+// Per-ray outcome of one object intersect: hit, miss, or a Newton failure.
+struct QHit {
+    double t;
+    V3 p, n;
+    double u, v;
+    int obj;
+    int err;          // 0 or BBRT_RAY_NEWTON_*
+    double ev0, ev1;  // values the reference's error message quotes
+};
+
+// Newton on F(u,v,t) = X(u,v) - (o + t d) from (u0, v0, t0).  Returns
+// 1 hit, or 0 with h.err set (singular / no convergence / out of domain).
+__device__ __forceinline__ int newton_exact(const DScene& S, int pidx, const V3 o, const V3 d, double u, double v,
+                                         double t, QHit& h, long long& iters) {
+    const int I = S.p_dims[2 * pidx], J = S.p_dims[2 * pidx + 1];
+    const double* un = S.p_nodes + S.p_node_off[pidx];
+    const double* vn = un + I;
+    const double* uw = vn + J;
+    const double* vw = uw + I;
+    const double* F = S.p_fields + S.p_field_off[pidx];
+    double bu[kDevMaxNodes], bv[kDevMaxNodes];
+    double step = CUDART_INF;
+    for (int it = 0; it < S.newton_max_iters; ++it) {
+        ++iters;
+        basis_1d(un, uw, I, u, bu);
+        basis_1d(vn, vw, J, v, bv);
+        double e[9];
+        eval_fields<9>(F, I, J, bu, bv, 0, e);
+        const V3 R = v3(o.x + t * d.x, o.y + t * d.y, o.z + t * d.z);
+        const double Fx = e[0] - R.x, Fy = e[1] - R.y, Fz = e[2] - R.z;
+        const double a11 = e[3], a12 = e[6], a13 = -d.x;
+        const double a21 = e[4], a22 = e[7], a23 = -d.y;
+        const double a31 = e[5], a32 = e[8], a33 = -d.z;
+        const double det = a11 * (a22 * a33 - a23 * a32) - a12 * (a21 * a33 - a23 * a31) + a13 * (a21 * a32 - a22 * a31);
+        if (fabs(det) < 1e-14) { h.err = 2; return 0; }   // BBRT_RAY_NEWTON_SINGULAR
+        const double bx = Fx, by = Fy, bz = Fz;
+        const double d0 = bx * (a22 * a33 - a23 * a32) - a12 * (by * a33 - a23 * bz) + a13 * (by * a32 - a22 * bz);
+        const double d1 = a11 * (by * a33 - a23 * bz) - bx * (a21 * a33 - a23 * a31) + a13 * (a21 * bz - by * a31);
+        const double d2 = a11 * (a22 * bz - by * a32) - a12 * (a21 * bz - by * a31) + bx * (a21 * a32 - a22 * a31);
+        const double x0 = d0 / det, x1 = d1 / det, x2 = d2 / det;
+        u -= x0;
+        v -= x1;
+        t -= x2;
+        step = sqrt(x0 * x0 + x1 * x1 + x2 * x2);
+        if (step < S.newton_tol) break;
+    }
+    if (step >= S.newton_tol) { h.err = 3; h.ev0 = step; return 0; }     // BBRT_RAY_NEWTON_NOCONV
+    if (u < -1.0 - 1e-6 || u > 1.0 + 1e-6 || v < -1.0 - 1e-6 || v > 1.0 + 1e-6) {
+        h.err = 4; h.ev0 = u; h.ev1 = v; return 0;                       // BBRT_RAY_NEWTON_DOMAIN
+    }
+    basis_1d(un, uw, I, u, bu);
+    basis_1d(vn, vw, J, v, bv);
+    double e[3], nn[3];
+    eval_fields<3>(F, I, J, bu, bv, 0, e);
+    eval_fields<3>(F, I, J, bu, bv, 9, nn);
+    h.t = t;
+    h.p = v3(e[0], e[1], e[2]);
+    h.n = vnormalize(v3(nn[0], nn[1], nn[2]));
+    h.u = u;
+    h.v = v;
+    return 1;
+}
+
+}  // namespace bbrt

@@ -1,0 +1,198 @@
+"""GPU parity: the CUDA trace path (through the C ABI) against the oracle and
+against the reference's own outputs (tests/golden/).
+
+The FP64 path is bit-identical to the reference by construction, so status,
+bounce counts and hit objects are compared exactly and hit points, end
+points and exit directions are compared for exact equality as well (the
+contract's bar is 1e-10 absolute; exact equality is stronger).
+"""
+import numpy as np
+import pytest
+
+import oracle
+from billardballraytracing3d_b200 import _capi as C
+from billardballraytracing3d_b200 import api, scenes
+from conftest import golden
+from test_oracle import TRACE_FIXTURES, _workload, bounce_map_scene_order, check_against_fixture
+
+pytestmark = pytest.mark.gpu
+POINT_TOL = 1e-10
+
+
+def assert_same_trace(g, r, exact=True):
+    for k in ("status", "bounce_count", "hit_object", "err_object"):
+        assert np.array_equal(g[k], r[k]), k
+    for k in ("hit_point", "end_point", "exit_dir", "hit_uv"):
+        if exact:
+            assert np.array_equal(g[k], r[k]), (k, np.max(np.abs(g[k] - r[k])))
+        else:
+            assert np.max(np.abs(g[k] - r[k])) <= POINT_TOL, k
+
+
+@pytest.mark.parametrize("cull", [0, 1])
+@pytest.mark.parametrize("name,n", [("two_spheres", None), ("tetra_spheres", 65536), ("ellipsoids", 32768)])
+def test_trace_matches_oracle(built, workloads, name, n, cull):
+    patches, o, d, maxb, cn, tol = workloads(name, n)
+    cfg = C.default_config(coarse_grid_n=cn, newton_tol=tol, cull=cull)
+    g = api.Scene(patches, config=cfg).trace(o, d, maxb, record=6)
+    r = oracle.Oracle(patches, config=cfg).trace(o, d, maxb, K=6)
+    assert_same_trace(g, r)
+    st = g["stats"]
+    assert st["rays"] == o.shape[0]
+    assert sum(st["status_hist"]) == o.shape[0]
+    assert st["bounces"] == int(g["bounce_count"].sum())
+    assert st["status_hist"] == list(np.bincount(g["status"], minlength=C.RAY_STATUS_COUNT))
+
+
+@pytest.mark.parametrize("fixture,n,cn,tol", TRACE_FIXTURES)
+def test_trace_matches_reference_fixture(built, fixture, n, cn, tol):
+    fx = golden(fixture)
+    patches, o, d, maxb, cn, tol = _workload(fixture, n, cn, tol)
+    sc = api.Scene(patches, config=C.default_config(coarse_grid_n=cn, newton_tol=tol))
+    g = sc.trace(o, d, maxb, record=fx["hit_object"].shape[1])
+    check_against_fixture(g, fx, tol_point=0.0)
+    err = np.nonzero(fx["err_zone"] >= 0)[0]
+    assert np.array_equal(fx["zone_ids"][g["err_object"][err]], fx["err_zone"][err])
+    assert sc.info()["scene_diagonal"] == float(fx["scene_diagonal"])
+
+
+@pytest.mark.parametrize("mode", [C.QUERY_BVH, C.QUERY_BRUTE])
+def test_single_queries_match_oracle(built, workloads, mode):
+    patches, *_ = workloads("tetra_spheres", 4)
+    cfg = C.default_config(coarse_grid_n=17, newton_tol=1e-12)
+    rng = np.random.Generator(np.random.PCG64(5))
+    n = 4096 if mode == C.QUERY_BVH else 512
+    o = rng.uniform(-3.5, 3.5, (n, 3))
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    g = api.Scene(patches, config=cfg).intersect(o, d, mode)
+    r = oracle.Oracle(patches, config=cfg).intersect(o, d, mode)
+    assert np.array_equal(g, r)
+    assert (g["object"] >= 0).sum() > n // 10
+
+
+def test_single_object_queries(built, workloads):
+    patches, *_ = workloads("two_spheres", 4)
+    cfg = C.default_config(coarse_grid_n=9, newton_tol=1e-12)
+    sc, orc = api.Scene(patches, config=cfg), oracle.Oracle(patches, config=cfg)
+    rng = np.random.Generator(np.random.PCG64(6))
+    for k in (0, 17, 101, 191):
+        c = sc.object_info(k)["centroid"]
+        o = c + rng.normal(size=(256, 3)) * 0.2 + sc.object_info(k)["centroid"] * 0.5
+        d = c - o + rng.normal(size=(256, 3)) * 0.05
+        assert np.array_equal(sc.intersect(o, d, C.QUERY_OBJECT, k), orc.intersect(o, d, C.QUERY_OBJECT, k))
+
+
+def test_reference_triangle_unit_test(built):
+    """tests/Triangle_Intersect.cpp on the GPU: BVH == brute force, t = 1, 1, miss, 5."""
+    fx = golden("triangles")
+    sc = api.Scene(triangles=list(fx["tris"]), config=C.default_config(leaf_threshold=1))
+    bvh = sc.intersect(fx["origins"], fx["dirs"], C.QUERY_BVH)
+    brute = sc.intersect(fx["origins"], fx["dirs"], C.QUERY_BRUTE)
+    t_bvh = np.where(bvh["object"] >= 0, bvh["t"], -1.0)
+    t_brute = np.where(brute["object"] >= 0, brute["t"], -1.0)
+    assert np.array_equal(t_bvh, fx["bvh_t"])
+    assert np.array_equal(t_brute, fx["brute_t"])
+    assert list(bvh["object"]) == list(fx["bvh_obj"])
+
+
+def test_edge_case_rays(built, workloads):
+    patches, *_ = workloads("tetra_spheres", 4)
+    cfg = C.default_config(coarse_grid_n=17, newton_tol=1e-12)
+    c0 = np.array(scenes.tetrahedron_centers()[0])
+    o = np.array([
+        [0.0, 0.0, 6.0], [0.0, 0.0, 6.0], [np.nan, 0.0, 6.0], [0.0, 0.0, 6.0],
+        c0 + [0.0, 0.0, 3.0], c0 + [3.0, 0.0, 0.0], c0,                    # axis-aligned; from the centre
+        c0 + [0.0, 0.0, 1.0 + 1e-9], c0 + [0.0, 1.0, 1.0],                 # grazing the pole
+        [1e6, 1e6, 1e6], [0.0, 0.0, 0.0], c0 + [0.3, 0.2, 0.1],
+    ])
+    d = np.array([
+        [0.0, 0.0, -1.0], [0.0, 0.0, 0.0], [0.0, 0.0, -1.0], [np.inf, 0.0, -1.0],
+        [0.0, 0.0, -1.0], [-1.0, 0.0, 0.0], [0.0, 0.0, 1.0],
+        [1.0, 0.0, 0.0], [0.0, -1.0, 1e-12],
+        [-1.0, -1.0, -1.0], [1e-200, 1e-200, 1e-200], [0.0, 1.0, 0.0],
+    ])
+    sc, orc = api.Scene(patches, config=cfg), oracle.Oracle(patches, config=cfg)
+    for maxb in (0, 1, 50):
+        g = sc.trace(o, d, maxb, record=4)
+        r = orc.trace(o, d, maxb, K=4)
+        for k in ("status", "bounce_count", "hit_object", "err_object"):
+            assert np.array_equal(g[k], r[k]), (maxb, k)
+        for k in ("hit_point", "end_point", "exit_dir"):
+            assert np.array_equal(np.nan_to_num(g[k], nan=7.0), np.nan_to_num(r[k], nan=7.0)), (maxb, k)
+    assert g["status"][1] == C.RAY_BAD_DIR
+    assert g["status"][10] == C.RAY_BAD_DIR          # |d|^2 underflows below 1e-300
+    empty = sc.trace(np.zeros((0, 3)), np.zeros((0, 3)), 10)
+    assert empty["status"].shape == (0,)
+
+
+def test_plane_source_counts(built):
+    fx = golden("plane_counts")
+    patches = scenes.scene_two_spheres()
+    sc = api.Scene(patches, config=C.default_config(coarse_grid_n=9, newton_tol=1e-12))
+    args = (fx["corner0"], fx["corner1"], fx["direction"], int(fx["nx"]), int(fx["ny"]), int(fx["max_bounces"]))
+    assert np.array_equal(sc.plane_source(*args, count_direct_hit=False), fx["counts"])
+    assert np.array_equal(sc.plane_source(*args, count_direct_hit=True), fx["counts_direct"])
+    with pytest.raises(RuntimeError, match="exactly one coordinate"):
+        sc.plane_source((0, 0, 4), (1, 1, 5), (0, 0, -1), 4, 4, 5)
+
+
+def test_bounce_map(built):
+    fx = golden("bounce_map")
+    patches = scenes.scene_two_spheres()
+    order = bounce_map_scene_order(len(patches))
+    sc = api.Scene([patches[k] for k in order], config=C.default_config(coarse_grid_n=9, newton_tol=1e-12))
+    samples = patches[int(fx["first"]) - 1:int(fx["last"])]
+    mb, er, bd = sc.bounce_map(samples, int(fx["grid_n"]), int(fx["theta_n"]), int(fx["phi_n"]),
+                               float(fx["cone"]), int(fx["max_bounces"]))
+    assert np.array_equal(mb, fx["max_b"])
+    assert np.array_equal(er, fx["errors"])
+    orc = oracle.Oracle([patches[k] for k in order], config=C.default_config(coarse_grid_n=9, newton_tol=1e-12))
+    _, _, obd = orc.bounce_map(samples, int(fx["grid_n"]), int(fx["theta_n"]), int(fx["phi_n"]),
+                               float(fx["cone"]), int(fx["max_bounces"]))
+    assert np.array_equal(bd, obd)
+
+
+def test_device_pointer_path_equals_host_path(built, workloads):
+    import torch
+    patches, o, d, maxb, cn, tol = workloads("tetra_spheres", 20000)
+    sc = api.Scene(patches, config=C.default_config(coarse_grid_n=cn, newton_tol=tol))
+    host = sc.trace(o, d, maxb, record=0, outputs=("status", "bounce_count", "exit_dir", "end_point"))
+    to = torch.from_numpy(o).cuda()
+    td = torch.from_numpy(d).cuda()
+    n = o.shape[0]
+    st = torch.zeros(n, dtype=torch.int32, device="cuda")
+    bc = torch.zeros(n, dtype=torch.int32, device="cuda")
+    ed = torch.zeros((n, 3), dtype=torch.float64, device="cuda")
+    ep = torch.zeros((n, 3), dtype=torch.float64, device="cuda")
+    side = torch.cuda.Stream()
+    torch.cuda.set_stream(side)
+    stream = side.cuda_stream
+    stats = sc.trace_device(to.data_ptr(), td.data_ptr(), n, maxb,
+                            dict(status=st.data_ptr(), bounce_count=bc.data_ptr(), exit_dir=ed.data_ptr(),
+                                 end_point=ep.data_ptr()), stream=stream, want_stats=True)
+    torch.cuda.synchronize()
+    assert np.array_equal(st.cpu().numpy(), host["status"])
+    assert np.array_equal(bc.cpu().numpy(), host["bounce_count"])
+    assert np.array_equal(ed.cpu().numpy(), host["exit_dir"])
+    assert np.array_equal(ep.cpu().numpy(), host["end_point"])
+    assert stats["bounces"] == int(host["bounce_count"].sum())
+
+
+def test_full_size_tetra_workload(built, workloads):
+    """The full 1M-ray tetrahedron workload: culled == unculled bit for bit,
+    consistent counters, and a 65k-ray sample against the oracle."""
+    patches, o, d, maxb, cn, tol = workloads("tetra_spheres")
+    outs = ("status", "bounce_count", "exit_dir", "end_point")
+    a = api.Scene(patches, config=C.default_config(coarse_grid_n=cn, newton_tol=tol, cull=1)).trace(
+        o, d, maxb, record=0, outputs=outs)
+    b = api.Scene(patches, config=C.default_config(coarse_grid_n=cn, newton_tol=tol, cull=0)).trace(
+        o, d, maxb, record=0, outputs=outs)
+    for k in outs:
+        assert np.array_equal(a[k], b[k]), k
+    assert a["stats"]["bounces"] == int(a["bounce_count"].sum())
+    assert a["stats"]["tri_tests"] < b["stats"]["tri_tests"] // 4
+    sel = np.arange(0, o.shape[0], 16)
+    r = oracle.Oracle(patches, config=C.default_config(coarse_grid_n=cn, newton_tol=tol)).trace(o[sel], d[sel], maxb, K=0)
+    for k in outs:
+        assert np.array_equal(a[k][sel], r[k]), k
