@@ -147,7 +147,7 @@ class TraceOut(ctypes.Structure):
         ("status", c_int_p), ("bounce_count", c_int_p), ("exit_dir", c_double_p),
         ("end_point", c_double_p), ("record_bounces", ctypes.c_int), ("hit_object", c_int_p),
         ("hit_point", c_double_p), ("hit_uv", c_double_p), ("err_object", c_int_p),
-        ("err_value", c_double_p),
+        ("err_value", c_double_p), ("ray_work", c_ll_p),
     ]
 
 

@@ -113,7 +113,8 @@ class Scene:
         shapes = dict(status=((n,), np.int32), bounce_count=((n,), np.int32), exit_dir=((n, 3), np.float64),
                       end_point=((n, 3), np.float64), hit_object=((n, K), np.int32),
                       hit_point=((n, K, 3), np.float64), hit_uv=((n, K, 2), np.float64),
-                      err_object=((n,), np.int32), err_value=((n, 2), np.float64))
+                      err_object=((n,), np.int32), err_value=((n, 2), np.float64),
+                      ray_work=((n, 4), np.int64))
         r = TraceResult()
         for k in outputs:
             shp, dt = shapes[k]
@@ -121,7 +122,7 @@ class Scene:
         out = C.TraceOut()
         out.record_bounces = K
         for k in shapes:
-            ct = ctypes.c_int if shapes[k][1] == np.int32 else ctypes.c_double
+            ct = {np.int32: ctypes.c_int, np.int64: ctypes.c_longlong}.get(shapes[k][1], ctypes.c_double)
             setattr(out, k, C.ptr(r.get(k), ct))
         st = C.TraceStats()
         C.check(self.lib, self.lib.bbrt_trace(self.h, P(o), P(d), n, max_bounces, 0, ctypes.byref(out),

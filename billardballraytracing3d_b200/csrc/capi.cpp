@@ -12,6 +12,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <filesystem>
 #include <memory>
@@ -27,6 +29,19 @@
 
 namespace bbrt {
 cudaError_t launch_trace(const DScene& S, const TraceArgs& A, cudaStream_t stream, int sm_count);
+size_t wave_workspace_bytes(long long n);
+void wave_layout(void* ws, long long n, WaveArgs& W, NewtonRequest*& req_a, NewtonRequest*& req_b);
+cudaError_t launch_advance(const DScene& S, const TraceArgs& A, const WaveArgs& W, int sm_count,
+                           cudaStream_t stream);
+cudaError_t launch_newton(const DScene& S, const TraceArgs& A, const WaveArgs& W, long long n_req,
+                          cudaStream_t stream);
+cudaError_t launch_resume_warp(const DScene& S, const TraceArgs& A, const WaveArgs& W, const NewtonRequest* reqs,
+                               const int* rays, long long n, int sm_count, cudaStream_t stream);
+cudaError_t launch_resume(const DScene& S, const TraceArgs& A, const WaveArgs& W, const NewtonRequest* reqs,
+                          const int* rays, long long n, cudaStream_t stream);
+size_t ray_order_workspace_bytes(long long n);
+cudaError_t ray_order(const double* o, const double* d, long long n, const double center[3], double radius,
+                      void* ws, int* order, cudaStream_t stream);
 cudaError_t launch_query(const DScene& S, const QueryArgs& Q, cudaStream_t stream);
 }  // namespace bbrt
 
@@ -80,14 +95,16 @@ struct bbrt_scene {
     std::vector<void*> allocs;
     long long device_bytes = 0;
     DevBuf stats, work, in_o, in_d, o_status, o_bounce, o_dir, o_end, o_hobj, o_hpt, o_huv, o_eobj, o_eval,
-        counts, hits;
+        counts, hits, wave, wave_ctr, o_work, order, order_ws;
+    unsigned int* wave_ctr_host = nullptr;   // pinned copy of the round counters
     std::mutex mu;
 
     ~bbrt_scene() {
         for (void* p : allocs) cudaFree(p);
         for (DevBuf* b : { &stats, &work, &in_o, &in_d, &o_status, &o_bounce, &o_dir, &o_end, &o_hobj, &o_hpt,
-                           &o_huv, &o_eobj, &o_eval, &counts, &hits })
+                           &o_huv, &o_eobj, &o_eval, &counts, &hits, &wave, &wave_ctr, &o_work, &order, &order_ws })
             b->release();
+        if (wave_ctr_host) cudaFreeHost(wave_ctr_host);
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
         if (stream) cudaStreamDestroy(stream);
@@ -130,15 +147,40 @@ int ensure_uploaded(bbrt_scene* s) {
     D.eps_factor = H.cfg.self_intersect_eps_factor;
     D.sag_factor = H.cfg.sagitta_clearance_factor;
     D.backface_tol = H.cfg.backface_tol;
-    std::vector<double> nbox(6 * H.nodes.size());
-    std::vector<int> nlink(4 * H.nodes.size());
-    for (size_t k = 0; k < H.nodes.size(); ++k) {
-        std::memcpy(&nbox[6 * k], H.nodes[k].box, sizeof(double) * 6);
-        nlink[4 * k] = H.nodes[k].right;
-        nlink[4 * k + 1] = H.nodes[k].start;
-        nlink[4 * k + 2] = H.nodes[k].count;
-        nlink[4 * k + 3] = H.nodes[k].axis;
+    // Renumber the depth-first tree breadth-first (children explicit), so the
+    // top levels are the first nodes and can be staged in shared memory.
+    const size_t nn = H.nodes.size();
+    std::vector<int> bfs;
+    bfs.reserve(nn);
+    std::vector<int> newid(nn, -1);
+    bfs.push_back(0);
+    for (size_t h = 0; h < bfs.size(); ++h) {
+        const bbrt::BvhNode& nd = H.nodes[bfs[h]];
+        newid[bfs[h]] = static_cast<int>(h);
+        if (nd.right >= 0) {
+            bfs.push_back(bfs[h] + 1);   // left child follows its parent in the depth-first layout
+            bfs.push_back(nd.right);
+        }
     }
+    std::vector<double> nbox(6 * nn);
+    std::vector<int> nlink(4 * nn);
+    for (size_t h = 0; h < nn; ++h) {
+        const bbrt::BvhNode& nd = H.nodes[bfs[h]];
+        std::memcpy(&nbox[6 * h], nd.box, sizeof(double) * 6);
+        if (nd.right >= 0) {
+            nlink[4 * h] = newid[bfs[h] + 1];
+            nlink[4 * h + 1] = newid[nd.right];
+            nlink[4 * h + 2] = 0;
+            nlink[4 * h + 3] = nd.axis;
+        } else {
+            nlink[4 * h] = nd.start;
+            nlink[4 * h + 1] = -1;
+            nlink[4 * h + 2] = nd.count;
+            nlink[4 * h + 3] = 0;
+        }
+    }
+    // up to 96 KB of nodes (64 bytes each) in shared memory
+    D.smem_nodes = static_cast<int>(std::min<size_t>(nn, 1536));
     std::vector<int> dims(2 * static_cast<size_t>(H.n_patches));
     for (int q = 0; q < H.n_patches; ++q) { dims[2 * q] = H.p_imax[q]; dims[2 * q + 1] = H.p_jmax[q]; }
     int rc;
@@ -239,6 +281,110 @@ void fill_stats(bbrt_scene* s, const long long* st, long long n, float kernel_ms
     (void)s;
 }
 
+// Batches at least this large run as a wavefront of advance / Newton rounds;
+// smaller ones (and the last few rays of a wavefront) run one ray per thread
+// to the end.
+struct Tuning {
+    long long wave_min_rays = 8192;   // smaller batches: one ray per thread to the end
+    long long wave_tail = 16384;      // last requests finished one ray per thread
+    int order_rays = 1;               // bucket rays by origin / direction before round 0
+    int log_rounds = 0;               // print per-round counts and times to stderr
+    int warp_tail = 1;                // finish the tail one warp per ray (else one thread per ray)
+};
+
+// Launch-shape knobs; defaults tuned on B200, overridable for experiments by
+// the environment (BBRT_WAVE_MIN, BBRT_WAVE_TAIL, BBRT_ORDER_RAYS,
+// BBRT_LOG_ROUNDS).  Read once per process.
+const Tuning& tuning() {
+    static const Tuning t = [] {
+        Tuning v;
+        if (const char* e = std::getenv("BBRT_WAVE_MIN")) v.wave_min_rays = std::atoll(e);
+        if (const char* e = std::getenv("BBRT_WAVE_TAIL")) v.wave_tail = std::atoll(e);
+        if (const char* e = std::getenv("BBRT_ORDER_RAYS")) v.order_rays = std::atoi(e);
+        if (const char* e = std::getenv("BBRT_LOG_ROUNDS")) v.log_rounds = std::atoi(e);
+        if (const char* e = std::getenv("BBRT_WARP_TAIL")) v.warp_tail = std::atoi(e);
+        return v;
+    }();
+    return t;
+}
+
+// The wavefront trace: k_advance moves every runnable ray until its query
+// meets a patch whose Newton solve is not yet known (or the ray finishes);
+// k_newton solves all such requests; the rays that asked become the next
+// round's runnable set.  Rounds end when no ray is waiting; a small last
+// set, and rays whose query needed more solves than the resolved list holds,
+// are finished by k_resume.
+// Finishes the rays of `reqs` (or `rays`) from their saved state.
+cudaError_t run_tail(bbrt_scene* s, const bbrt::TraceArgs& A, const bbrt::WaveArgs& W,
+                     const bbrt::NewtonRequest* reqs, const int* rays, long long n, cudaStream_t st) {
+    if (tuning().warp_tail) return bbrt::launch_resume_warp(s->dev, A, W, reqs, rays, n, s->sm_count, st);
+    return bbrt::launch_resume(s->dev, A, W, reqs, rays, n, st);
+}
+
+int run_wavefront(bbrt_scene* s, const bbrt::TraceArgs& A, cudaStream_t st) {
+    const long long n = A.n;
+    const Tuning& T = tuning();
+    BBRT_CUDA(s->wave.ensure(bbrt::wave_workspace_bytes(n)));
+    BBRT_CUDA(s->wave_ctr.ensure(3 * sizeof(unsigned int)));
+    if (!s->wave_ctr_host) BBRT_CUDA(cudaMallocHost(&s->wave_ctr_host, 2 * sizeof(unsigned int)));
+    bbrt::WaveArgs W;
+    bbrt::NewtonRequest *req_a = nullptr, *req_b = nullptr;
+    bbrt::wave_layout(s->wave.p, n, W, req_a, req_b);
+    W.counters = static_cast<unsigned int*>(s->wave_ctr.p);
+    W.runnable = nullptr;
+    W.n_runnable = n;
+    W.req = req_a;
+    if (T.order_rays) {
+        BBRT_CUDA(s->order_ws.ensure(bbrt::ray_order_workspace_bytes(n)));
+        BBRT_CUDA(s->order.ensure(sizeof(int) * static_cast<size_t>(n)));
+        BBRT_CUDA(bbrt::ray_order(A.origins, A.dirs, n, s->cull.center, s->cull.radius > 0.0 ? s->cull.radius
+                                                                                              : s->host.scene_diagonal,
+                                  s->order_ws.p, static_cast<int*>(s->order.p), st));
+        W.order = static_cast<const int*>(s->order.p);
+    }
+    BBRT_CUDA(cudaMemsetAsync(W.counters, 0, 3 * sizeof(unsigned int), st));
+    // every round finishes at least one query or one Newton solve of each runnable ray
+    const long long max_rounds = 4 + static_cast<long long>(A.max_bounces + 1) * (s->host.n_objects + 1);
+    long long overflowed = 0;
+    for (long long round = 0; round < max_rounds; ++round) {
+        if (T.log_rounds) BBRT_CUDA(cudaEventRecord(s->ev[2], st));
+        BBRT_CUDA(cudaMemsetAsync(W.counters, 0, sizeof(unsigned int), st));
+        BBRT_CUDA(cudaMemsetAsync(W.counters + 2, 0, sizeof(unsigned int), st));
+        BBRT_CUDA(bbrt::launch_advance(s->dev, A, W, s->sm_count, st));
+        if (T.log_rounds) BBRT_CUDA(cudaEventRecord(s->ev[3], st));
+        BBRT_CUDA(cudaMemcpyAsync(s->wave_ctr_host, W.counters, 2 * sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
+        BBRT_CUDA(cudaStreamSynchronize(st));
+        const long long n_req = s->wave_ctr_host[0];
+        overflowed = s->wave_ctr_host[1];
+        if (T.log_rounds) {
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, s->ev[2], s->ev[3]);
+            std::fprintf(stderr, "bbrt round %lld: runnable %lld advance %.3f ms -> requests %lld overflow %lld\n",
+                         round, W.n_runnable, ms, n_req, overflowed);
+        }
+        if (n_req == 0) break;
+        if (n_req <= T.wave_tail) {
+            BBRT_CUDA(run_tail(s, A, W, W.req, nullptr, n_req, st));
+            break;
+        }
+        if (T.log_rounds) BBRT_CUDA(cudaEventRecord(s->ev[2], st));
+        BBRT_CUDA(bbrt::launch_newton(s->dev, A, W, n_req, st));
+        if (T.log_rounds) {
+            BBRT_CUDA(cudaEventRecord(s->ev[3], st));
+            BBRT_CUDA(cudaEventSynchronize(s->ev[3]));
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, s->ev[2], s->ev[3]);
+            std::fprintf(stderr, "bbrt round %lld: newton %.3f ms\n", round, ms);
+        }
+        W.runnable = W.req;
+        W.n_runnable = n_req;
+        W.req = (W.req == req_a) ? req_b : req_a;
+        if (round + 1 == max_rounds) return fail(BBRT_ERR_KERNEL, "bbrt_trace: wavefront round bound reached");
+    }
+    if (overflowed > 0) BBRT_CUDA(run_tail(s, A, W, nullptr, W.overflow, overflowed, st));
+    return BBRT_OK;
+}
+
 // Launches the trace kernel on device arrays.  hit_counts (device, may be
 // null) receives per-object counts for bounces with index >= count_from.
 int run_trace_device(bbrt_scene* s, const double* d_o, const double* d_d, long long n, int max_bounces,
@@ -261,6 +407,7 @@ int run_trace_device(bbrt_scene* s, const double* d_o, const double* d_d, long l
         A.hit_uv = out_dev->hit_uv;
         A.err_object = out_dev->err_object;
         A.err_value = out_dev->err_value;
+        A.ray_work = out_dev->ray_work;
     }
     if (A.record < 0) return fail(BBRT_ERR_ARG, "bbrt_trace: record_bounces < 0");
     A.hit_counts = hit_counts;
@@ -270,7 +417,12 @@ int run_trace_device(bbrt_scene* s, const double* d_o, const double* d_d, long l
     if (want_stats) BBRT_CUDA(cudaMemsetAsync(s->stats.p, 0, sizeof(long long) * bbrt::ST_COUNT, st));
     BBRT_CUDA(cudaMemsetAsync(s->work.p, 0, sizeof(unsigned long long), st));
     BBRT_CUDA(cudaEventRecord(s->ev[0], st));
-    BBRT_CUDA(bbrt::launch_trace(s->dev, A, st, s->sm_count));
+    if (n < tuning().wave_min_rays) {
+        BBRT_CUDA(bbrt::launch_trace(s->dev, A, st, s->sm_count));
+    } else {
+        const int rc = run_wavefront(s, A, st);
+        if (rc) return rc;
+    }
     BBRT_CUDA(cudaEventRecord(s->ev[1], st));
     if (want_stats) {
         BBRT_CUDA(cudaMemcpyAsync(host_stats, s->stats.p, sizeof(long long) * bbrt::ST_COUNT,
@@ -531,6 +683,7 @@ BBRT_API int bbrt_trace(bbrt_scene_t s, const double* origins, const double* dir
         if ((rc = bind(out->hit_uv, s->o_huv, sizeof(double) * 2 * N * K, dev.hit_uv))) return rc;
         if ((rc = bind(out->err_object, s->o_eobj, sizeof(int) * N, dev.err_object))) return rc;
         if ((rc = bind(out->err_value, s->o_eval, sizeof(double) * 2 * N, dev.err_value))) return rc;
+        if ((rc = bind(out->ray_work, s->o_work, sizeof(long long) * 4 * N, dev.ray_work))) return rc;
     }
     rc = run_trace_device(s, static_cast<const double*>(s->in_o.p), static_cast<const double*>(s->in_d.p), n,
                           max_bounces, out ? &dev : nullptr, nullptr, 1, st, stats != nullptr, hs, nullptr);

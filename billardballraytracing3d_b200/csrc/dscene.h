@@ -19,10 +19,13 @@ struct DScene {
     double sag_factor = 5.0;        // kSagittaClearanceFactor
     double backface_tol = 1e-9;     // kBackfaceHitTol
 
-    // BVH (depth-first, left child = parent + 1)
+    // BVH nodes renumbered breadth-first (the top levels come first) with
+    // explicit children; the tree and its child order are the reference's.
     const double* node_box = nullptr;      // [n_nodes][6]  min xyz, max xyz
-    const int* node_link = nullptr;        // [n_nodes][4]  right (-1 leaf), start, count, axis
+    const int* node_link = nullptr;        // [n_nodes][4]  internal: left, right, 0, axis
+                                           //               leaf:     start, -1, count, 0
     const int* leaf_objects = nullptr;
+    int smem_nodes = 0;                    // nodes [0, smem_nodes) staged in shared memory
 
     // objects
     const int* obj_kind = nullptr;         // BBRT_OBJ_*
@@ -78,10 +81,44 @@ struct TraceArgs {
     double* hit_uv = nullptr;          // [n][K][2]
     int* err_object = nullptr;
     double* err_value = nullptr;       // [n][2]
+    long long* ray_work = nullptr;     // [n][4] node tests, box tests, MT tests, Newton iterations
     unsigned long long* hit_counts = nullptr;  // per object (plane source), may be null
     int count_from = 1;                // first bounce index that is counted
     long long* stats = nullptr;        // [ST_COUNT], may be null
     unsigned long long* work_counter = nullptr;  // persistent-launch ray counter (zeroed by host)
+};
+
+// A patch query of the current bounce whose stage-1 winner needs Newton.
+struct NewtonRequest {
+    int ray;      // ray index
+    int entry;    // slot in the ray's resolved list
+    int obj;      // object index of the patch
+    int key;      // stage-1 winner
+    double t0;    // stage-1 t
+};
+
+// Resolved Newton results of a ray's current query: res_obj[ray][k] and
+// res_data[ray][k][kResData] = t, point xyz, normal xyz, u, v, ev0, ev1.
+constexpr int kResolved = 4;
+constexpr int kResData = 11;
+
+// Workspace of the wavefront trace (advance / Newton rounds).
+struct WaveArgs {
+    double* o = nullptr;       // [n][3] ray state between rounds
+    double* d = nullptr;
+    double* end = nullptr;
+    int* bounces = nullptr;
+    int* nres = nullptr;
+    int* res_obj = nullptr;    // [n][kResolved]
+    int* res_err = nullptr;    // [n][kResolved]
+    double* res_data = nullptr;  // [n][kResolved][kResData]
+    const NewtonRequest* runnable = nullptr;   // previous round's requests (null: round 0, all rays)
+    const int* order = nullptr;                // round 0 processing order (null: index order)
+    long long n_runnable = 0;
+    NewtonRequest* req = nullptr;              // this round's requests
+    unsigned int* counters = nullptr;          // [0] requests of the round, [1] overflowed rays (cumulative),
+                                               // [2] runnable rays fetched this round
+    int* overflow = nullptr;                   // rays whose query needs more than kResolved solves
 };
 
 struct QueryArgs {

@@ -109,11 +109,10 @@ __device__ __forceinline__ void stage1_cell(const double* __restrict__ X, const 
     }
 }
 
-// SurfacePatch::intersect: stage 1 over the coarse triangulation (all cells,
-// or only cells whose inflated box the ray crosses), then Newton from the
-// winning triangle's (u, v) centroid and its t.
-__device__ __forceinline__ int patch_intersect(const DScene& S, int pidx, const V3& o, const V3& d, bool use_cull,
-                               const CullRay& cr, QHit& h, Counters& ctr) {
+// SurfacePatch::intersect stage 1: the winning (t, key) over the coarse
+// triangulation (all cells, or only cells whose inflated box the ray crosses).
+__device__ __forceinline__ Stage1 patch_stage1(const DScene& S, int pidx, const V3& o, const V3& d, bool use_cull,
+                                               const CullRay& cr, Counters& ctr) {
     const int n = S.coarse_n, nc = n - 1;
     const double* X = S.c_xyz + static_cast<long long>(pidx) * n * n * 3;
     const double* CC = S.c_cell + static_cast<long long>(pidx) * nc * nc * 4;
@@ -143,25 +142,39 @@ __device__ __forceinline__ int patch_intersect(const DScene& S, int pidx, const 
             for (int j = 0; j < nc; ++j) stage1_cell(X, CC, n, i, j, o, d, best);
         ctr.tri_tests += 6LL * nc * nc;
     }
-    if (!best.have) return 0;
-    const int cell = best.key / 6;
-    const bool second = (best.key & 1) != 0;
+    return best;
+}
+
+// triangle_uv_centroid (SurfacePatch.hpp:499-510) of the stage-1 winner `key`.
+__device__ __forceinline__ void key_to_uv(const DScene& S, int key, double& u0, double& v0) {
+    const int nc = S.coarse_n - 1;
+    const int cell = key / 6;
+    const bool second = (key & 1) != 0;
     const int bi = cell / nc, bj = cell % nc;
     const double ui = S.coarse_uv[bi], ui1 = S.coarse_uv[bi + 1];
     const double vj = S.coarse_uv[bj], vj1 = S.coarse_uv[bj + 1];
-    double u0, v0;
     if (!second) { u0 = (ui + ui1 + ui1) / 3.0; v0 = (vj + vj + vj1) / 3.0; }
     else         { u0 = (ui + ui + ui1) / 3.0; v0 = (vj + vj1 + vj1) / 3.0; }
+}
+
+// SurfacePatch::intersect: stage 1, then Newton from the winning triangle's
+// (u, v) centroid and its t.
+__device__ __forceinline__ int patch_intersect(const DScene& S, int pidx, const V3& o, const V3& d, bool use_cull,
+                                               const CullRay& cr, QHit& h, Counters& ctr) {
+    const Stage1 best = patch_stage1(S, pidx, o, d, use_cull, cr, ctr);
+    if (!best.have) return 0;
+    double u0, v0;
+    key_to_uv(S, best.key, u0, v0);
     return newton_exact(S, pidx, o, d, u0, v0, best.t, h, ctr.newton_iters);
 }
 
-// ScatObject::intersect for object `obj`: 1 hit, 0 miss (h.err set on a
-// Newton failure).
-__device__ __forceinline__ int object_intersect(const DScene& S, int obj, const V3& o, const V3& d, bool use_cull,
-                                                const CullRay& cr, QHit& h, Counters& ctr) {
+// Triangle::intersect (Triangle.hpp:26-28): Moller-Trumbore, point o + t d,
+// normal normalize(e1 x e2).
+__device__ __forceinline__ int triangle_intersect(const DScene& S, int sub, const V3& o, const V3& d, QHit& h,
+                                                  Counters& ctr) {
     h.err = 0;
-    const int sub = S.obj_sub[obj];
-    if (S.obj_kind[obj] == BBRT_OBJ_PATCH) return patch_intersect(S, sub, o, d, use_cull, cr, h, ctr);
+    h.ev0 = 0.0;
+    h.ev1 = 0.0;
     const double* v = S.tri + static_cast<long long>(sub) * 9;
     const V3 v0 = load3(v), v1 = load3(v + 3), v2 = load3(v + 6);
     double t, u, w;
@@ -173,6 +186,18 @@ __device__ __forceinline__ int object_intersect(const DScene& S, int obj, const 
     h.u = u;
     h.v = w;
     return 1;
+}
+
+// ScatObject::intersect for object `obj`: 1 hit, 0 miss (h.err set on a
+// Newton failure).
+__device__ __forceinline__ int object_intersect(const DScene& S, int obj, const V3& o, const V3& d, bool use_cull,
+                                                const CullRay& cr, QHit& h, Counters& ctr) {
+    h.err = 0;
+    h.ev0 = 0.0;
+    h.ev1 = 0.0;
+    const int sub = S.obj_sub[obj];
+    if (S.obj_kind[obj] == BBRT_OBJ_PATCH) return patch_intersect(S, sub, o, d, use_cull, cr, h, ctr);
+    return triangle_intersect(S, sub, o, d, h, ctr);
 }
 
 // BVH::intersect with a 64-entry stack.  Returns the closest hit (obj >= 0),
@@ -196,9 +221,8 @@ __device__ QHit bvh_query(const DScene& S, const V3& o, const V3& d, int cull_fl
         ++ctr.node_tests;
         if (!ray_box_exact(o, inv, S.node_box + 6LL * idx, best_t)) continue;
         const int* link = S.node_link + 4LL * idx;
-        const int right = link[0];
-        if (right < 0) {
-            const int start = link[1], count = link[2];
+        if (link[1] < 0) {
+            const int start = link[0], count = link[2];
             for (int k = 0; k < count; ++k) {
                 const int obj = S.leaf_objects[start + k];
                 QHit h;
@@ -220,7 +244,7 @@ __device__ QHit bvh_query(const DScene& S, const V3& o, const V3& d, int cull_fl
             best.obj = -1;
             return best;
         }
-        const int left = idx + 1;
+        const int left = link[0], right = link[1];
         if (neg[link[3]]) { stack[sp++] = left; stack[sp++] = right; }
         else              { stack[sp++] = right; stack[sp++] = left; }
     }
@@ -233,81 +257,135 @@ __device__ __forceinline__ void warp_add(long long* dst, long long v) {
     if ((threadIdx.x & 31) == 0 && v) atomicAdd(reinterpret_cast<unsigned long long*>(dst), static_cast<unsigned long long>(v));
 }
 
-// The bounce loop for one ray (RayTracingDriver::trace_ray).
-__device__ void trace_one(const DScene& S, const TraceArgs& A, long long i, Counters& ctr, long long& bounces_out,
-                          long long& queries_out, int& status_out) {
-    const V3 origin = load3(A.origins + 3 * i);
-    const V3 dir_in = load3(A.dirs + 3 * i);
+// ---- the bounce loop (RayTracingDriver::trace_ray) as per-ray state steps ----
+
+// Registers of one ray between queries.
+struct RayCtx {
+    V3 o, d, end;
+    int bounces;
+    int status;      // final status once set; -1 while the ray is running
+    int err_obj;
+    double ev0, ev1;
+};
+
+__device__ __forceinline__ void init_outputs(const TraceArgs& A, long long i) {
+    if (A.ray_work) for (int k = 0; k < 4; ++k) A.ray_work[4 * i + k] = 0;
     const int K = A.record;
     for (int k = 0; k < K; ++k) {
         if (A.hit_object) A.hit_object[i * K + k] = -1;
         if (A.hit_point) { double* p = A.hit_point + (i * K + k) * 3; p[0] = 0.0; p[1] = 0.0; p[2] = 0.0; }
         if (A.hit_uv) { double* p = A.hit_uv + (i * K + k) * 2; p[0] = 0.0; p[1] = 0.0; }
     }
-    int status = BBRT_RAY_MAX_BOUNCES, bounces = 0, err_obj = -1;
-    long long queries = 0;
-    double ev0 = 0.0, ev1 = 0.0;
-    V3 end = origin;
-    V3 d = v3(0.0, 0.0, 0.0);
-    const double len2 = dir_in.x * dir_in.x + dir_in.y * dir_in.y + dir_in.z * dir_in.z;
-    if (len2 < 1e-300) {
-        status = BBRT_RAY_BAD_DIR;
-    } else {
-        const double len = sqrt(dir_in.x * dir_in.x + dir_in.y * dir_in.y + dir_in.z * dir_in.z);
-        d = v3(dir_in.x / len, dir_in.y / len, dir_in.z / len);
-        V3 o = origin;
-        status = BBRT_RAY_MAX_BOUNCES;
-        for (int b = 0; b < A.max_bounces; ++b) {
-            ++queries;
-            const QHit h = bvh_query(S, o, d, A.cull, ctr);
-            if (h.err) {
-                status = h.err;
-                err_obj = h.obj;
-                ev0 = h.ev0;
-                ev1 = h.ev1;
-                break;
-            }
-            if (h.obj < 0) {
-                status = BBRT_RAY_ESCAPED;
-                end = v3(o.x + d.x * S.scene_diagonal, o.y + d.y * S.scene_diagonal, o.z + d.z * S.scene_diagonal);
-                break;
-            }
-            if (vdot(d, h.n) > S.backface_tol) { status = BBRT_RAY_WENT_INSIDE; break; }
-            if (bounces < K) {
-                if (A.hit_object) A.hit_object[i * K + bounces] = h.obj;
-                if (A.hit_point) {
-                    double* p = A.hit_point + (i * K + bounces) * 3;
-                    p[0] = h.p.x; p[1] = h.p.y; p[2] = h.p.z;
-                }
-                if (A.hit_uv) { double* p = A.hit_uv + (i * K + bounces) * 2; p[0] = h.u; p[1] = h.v; }
-            }
-            if (A.hit_counts && bounces >= A.count_from) atomicAdd(A.hit_counts + h.obj, 1ULL);
-            ++bounces;
-            end = h.p;
-            const double dn = d.x * h.n.x + d.y * h.n.y + d.z * h.n.z;
-            d = v3(d.x - 2.0 * dn * h.n.x, d.y - 2.0 * dn * h.n.y, d.z - 2.0 * dn * h.n.z);
-            const double eps = smax(S.eps_factor * S.scene_diagonal, S.sag_factor * S.obj_pad[h.obj]);
-            o = v3(h.p.x + d.x * eps, h.p.y + d.y * eps, h.p.z + d.z * eps);
-        }
-    }
-    if (A.status) A.status[i] = status;
-    if (A.bounce_count) A.bounce_count[i] = bounces;
-    if (A.exit_dir) { double* p = A.exit_dir + 3 * i; p[0] = d.x; p[1] = d.y; p[2] = d.z; }
-    if (A.end_point) { double* p = A.end_point + 3 * i; p[0] = end.x; p[1] = end.y; p[2] = end.z; }
-    if (A.err_object) A.err_object[i] = err_obj;
-    if (A.err_value) { A.err_value[2 * i] = ev0; A.err_value[2 * i + 1] = ev1; }
-    bounces_out = bounces;
-    queries_out = queries;
-    status_out = status;
 }
 
-// Persistent trace kernel: warps pull 32-ray batches until none are left.
+// Start of trace_ray: zero-length check, normalisation (RayTracingDriver.hpp:174-184).
+__device__ __forceinline__ RayCtx start_ray(const TraceArgs& A, long long i) {
+    RayCtx r;
+    r.o = load3(A.origins + 3 * i);
+    const V3 dir_in = load3(A.dirs + 3 * i);
+    r.end = r.o;
+    r.d = v3(0.0, 0.0, 0.0);
+    r.bounces = 0;
+    r.status = -1;
+    r.err_obj = -1;
+    r.ev0 = r.ev1 = 0.0;
+    const double len2 = dir_in.x * dir_in.x + dir_in.y * dir_in.y + dir_in.z * dir_in.z;
+    if (len2 < 1e-300) {
+        r.status = BBRT_RAY_BAD_DIR;
+    } else {
+        const double len = sqrt(dir_in.x * dir_in.x + dir_in.y * dir_in.y + dir_in.z * dir_in.z);
+        r.d = v3(dir_in.x / len, dir_in.y / len, dir_in.z / len);
+    }
+    return r;
+}
+
+// One bounce of trace_ray given the query result h (RayTracingDriver.hpp:187-237).
+// Returns true when the ray goes on to another query.
+__device__ __forceinline__ bool step_ray(const DScene& S, const TraceArgs& A, long long i, RayCtx& r, const QHit& h,
+                                        bool write = true) {
+    if (h.err) {
+        r.status = h.err;
+        r.err_obj = h.obj;
+        r.ev0 = h.ev0;
+        r.ev1 = h.ev1;
+        return false;
+    }
+    if (h.obj < 0) {
+        r.status = BBRT_RAY_ESCAPED;
+        r.end = v3(r.o.x + r.d.x * S.scene_diagonal, r.o.y + r.d.y * S.scene_diagonal, r.o.z + r.d.z * S.scene_diagonal);
+        return false;
+    }
+    if (vdot(r.d, h.n) > S.backface_tol) { r.status = BBRT_RAY_WENT_INSIDE; return false; }
+    const int K = A.record;
+    if (write && r.bounces < K) {
+        if (A.hit_object) A.hit_object[i * K + r.bounces] = h.obj;
+        if (A.hit_point) { double* p = A.hit_point + (i * K + r.bounces) * 3; p[0] = h.p.x; p[1] = h.p.y; p[2] = h.p.z; }
+        if (A.hit_uv) { double* p = A.hit_uv + (i * K + r.bounces) * 2; p[0] = h.u; p[1] = h.v; }
+    }
+    if (write && A.hit_counts && r.bounces >= A.count_from) atomicAdd(A.hit_counts + h.obj, 1ULL);
+    ++r.bounces;
+    r.end = h.p;
+    const V3 d = r.d;
+    const double dn = d.x * h.n.x + d.y * h.n.y + d.z * h.n.z;
+    r.d = v3(d.x - 2.0 * dn * h.n.x, d.y - 2.0 * dn * h.n.y, d.z - 2.0 * dn * h.n.z);
+    const double eps = smax(S.eps_factor * S.scene_diagonal, S.sag_factor * S.obj_pad[h.obj]);
+    r.o = v3(h.p.x + r.d.x * eps, h.p.y + r.d.y * eps, h.p.z + r.d.z * eps);
+    return true;
+}
+
+__device__ __forceinline__ void finish_ray(const TraceArgs& A, long long i, const RayCtx& r) {
+    if (A.status) A.status[i] = r.status;
+    if (A.bounce_count) A.bounce_count[i] = r.bounces;
+    if (A.exit_dir) { double* p = A.exit_dir + 3 * i; p[0] = r.d.x; p[1] = r.d.y; p[2] = r.d.z; }
+    if (A.end_point) { double* p = A.end_point + 3 * i; p[0] = r.end.x; p[1] = r.end.y; p[2] = r.end.z; }
+    if (A.err_object) A.err_object[i] = r.err_obj;
+    if (A.err_value) { A.err_value[2 * i] = r.ev0; A.err_value[2 * i + 1] = r.ev1; }
+}
+
+// Runs the bounce loop of one ray to the end with inline queries.
+__device__ __forceinline__ void run_ray(const DScene& S, const TraceArgs& A, long long i, RayCtx& r, Counters& ctr,
+                                        long long& queries) {
+    while (r.status < 0) {
+        if (r.bounces >= A.max_bounces) { r.status = BBRT_RAY_MAX_BOUNCES; break; }
+        ++queries;
+        const QHit h = bvh_query(S, r.o, r.d, A.cull, ctr);
+        if (!step_ray(S, A, i, r, h)) break;
+    }
+}
+
+// Adds one thread's work counters for ray i to the optional per-ray profile
+// (a ray is owned by one thread at a time, so no atomics are needed).
+__device__ __forceinline__ void add_ray_work(const TraceArgs& A, long long i, const Counters& c) {
+    if (!A.ray_work || i < 0) return;
+    long long* w = A.ray_work + 4 * i;
+    w[0] += c.node_tests;
+    w[1] += c.cell_tests;
+    w[2] += c.tri_tests;
+    w[3] += c.newton_iters;
+}
+
+struct RayTally {
+    long long bounces = 0, queries = 0;
+    long long hist[BBRT_RAY_STATUS_COUNT] = { 0, 0, 0, 0, 0, 0, 0, 0 };
+};
+
+__device__ __forceinline__ void flush_stats(const TraceArgs& A, const Counters& ctr, const RayTally& t) {
+    if (!A.stats) return;
+    warp_add(A.stats + ST_BOUNCES, t.bounces);
+    warp_add(A.stats + ST_QUERIES, t.queries);
+    warp_add(A.stats + ST_NODE_TESTS, ctr.node_tests);
+    warp_add(A.stats + ST_PATCH_TESTS, ctr.patch_tests);
+    warp_add(A.stats + ST_CELL_TESTS, ctr.cell_tests);
+    warp_add(A.stats + ST_TRI_TESTS, ctr.tri_tests);
+    warp_add(A.stats + ST_NEWTON_ITERS, ctr.newton_iters);
+#pragma unroll
+    for (int k = 0; k < BBRT_RAY_STATUS_COUNT; ++k) warp_add(A.stats + ST_HIST0 + k, t.hist[k]);
+}
+
+// Fused per-ray kernel (small batches): warps pull 32-ray batches until none are left.
 __global__ void __launch_bounds__(128) k_trace(DScene S, TraceArgs A) {
     Counters ctr;
-    long long bounces = 0, queries = 0;
-    long long hist[BBRT_RAY_STATUS_COUNT];
-#pragma unroll
-    for (int k = 0; k < BBRT_RAY_STATUS_COUNT; ++k) hist[k] = 0;
+    RayTally tally;
     const int lane = threadIdx.x & 31;
     while (true) {
         unsigned long long base = 0;
@@ -316,25 +394,636 @@ __global__ void __launch_bounds__(128) k_trace(DScene S, TraceArgs A) {
         if (base >= static_cast<unsigned long long>(A.n)) break;
         const long long i = static_cast<long long>(base) + lane;
         if (i < A.n) {
-            long long b = 0, q = 0;
-            int st = 0;
-            trace_one(S, A, i, ctr, b, q, st);
-            bounces += b;
-            queries += q;
-            hist[st]++;
+            init_outputs(A, i);
+            RayCtx r = start_ray(A, i);
+            Counters c1;
+            run_ray(S, A, i, r, c1, tally.queries);
+            add_ray_work(A, i, c1);
+            ctr.node_tests += c1.node_tests; ctr.patch_tests += c1.patch_tests; ctr.cell_tests += c1.cell_tests;
+            ctr.tri_tests += c1.tri_tests; ctr.newton_iters += c1.newton_iters;
+            finish_ray(A, i, r);
+            tally.bounces += r.bounces;
+            tally.hist[r.status]++;
         }
     }
-    if (A.stats) {
-        warp_add(A.stats + ST_BOUNCES, bounces);
-        warp_add(A.stats + ST_QUERIES, queries);
-        warp_add(A.stats + ST_NODE_TESTS, ctr.node_tests);
-        warp_add(A.stats + ST_PATCH_TESTS, ctr.patch_tests);
-        warp_add(A.stats + ST_CELL_TESTS, ctr.cell_tests);
-        warp_add(A.stats + ST_TRI_TESTS, ctr.tri_tests);
-        warp_add(A.stats + ST_NEWTON_ITERS, ctr.newton_iters);
-#pragma unroll
-        for (int k = 0; k < BBRT_RAY_STATUS_COUNT; ++k) warp_add(A.stats + ST_HIST0 + k, hist[k]);
+    flush_stats(A, ctr, tally);
+}
+
+// ---- wavefront form: advance rays until they need a Newton solve ----------
+
+__device__ __forceinline__ void save_ray(const WaveArgs& W, long long i, const RayCtx& r, int nres) {
+    double* o = W.o + 3 * i;
+    double* d = W.d + 3 * i;
+    double* e = W.end + 3 * i;
+    o[0] = r.o.x; o[1] = r.o.y; o[2] = r.o.z;
+    d[0] = r.d.x; d[1] = r.d.y; d[2] = r.d.z;
+    e[0] = r.end.x; e[1] = r.end.y; e[2] = r.end.z;
+    W.bounces[i] = r.bounces;
+    W.nres[i] = nres;
+}
+
+__device__ __forceinline__ RayCtx load_ray(const WaveArgs& W, long long i, int& nres) {
+    RayCtx r;
+    r.o = load3(W.o + 3 * i);
+    r.d = load3(W.d + 3 * i);
+    r.end = load3(W.end + 3 * i);
+    r.bounces = W.bounces[i];
+    r.status = -1;
+    r.err_obj = -1;
+    r.ev0 = r.ev1 = 0.0;
+    nres = W.nres[i];
+    return r;
+}
+
+// Warp-aggregated append: returns this lane's slot (or -1 when !want).
+__device__ __forceinline__ long long warp_append(unsigned int* counter, bool want) {
+    const unsigned mask = __ballot_sync(0xffffffffu, want);
+    const int lane = threadIdx.x & 31;
+    unsigned int base = 0;
+    if (lane == 0 && mask) base = atomicAdd(counter, static_cast<unsigned int>(__popc(mask)));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (!want) return -1;
+    return static_cast<long long>(base) + __popc(mask & ((1u << lane) - 1u));
+}
+
+// Advance-kernel modes.  The kernel is persistent: each lane owns one ray at
+// a time and the body is one flat loop in which every iteration does one
+// small unit of work for the lane's ray (one BVH node test, one leaf object,
+// one block or cell box, one Moller-Trumbore test).  A lane whose ray
+// suspends or finishes fetches the next runnable ray at once, so lanes stay
+// busy and the warp reconverges every iteration instead of waiting on its
+// slowest ray.
+enum AdvMode {
+    M_NODE = 0,      // pop and test a BVH node
+    M_LEAF = 1,      // next object of the current leaf
+    M_BLOCK = 2,     // next stage-1 block box
+    M_CELL = 3,      // next cell box of the current block
+    M_CELL_ALL = 4,  // next cell, culling off
+    M_TRI = 5,       // next of the six triangle tests of a cell
+    M_S1_DONE = 6,   // stage 1 of the current patch finished
+    M_RESOLVE = 7,   // query finished: bounce, escape or error
+    M_FINISH = 8,    // ray finished
+    M_SUSPEND = 9,   // waiting for a Newton solve
+    M_OVERFLOW = 10, // more solves than the resolved list holds
+    M_IDLE = 11,     // lane has no ray
+    M_DRAINED = 12   // no runnable ray left
+};
+
+struct AdvState {
+    // query
+    double inv[3];
+    bool neg[3];
+    bool use_cull;
+    CullRay cr;
+    double best_t;
+    int best_obj;    // -1: no hit yet
+    int best_e;      // resolved entry of the best patch hit, -1 for a triangle
+    double tri_u, tri_v;
+    int err, err_obj;
+    double ev0, ev1;
+    int sp;
+    int leaf_start, leaf_count, leaf_k;
+    // stage 1 of the current patch
+    int obj, pidx, bi, bj, ci, cj, i1, j0, j1;
+    int tci, tcj, tri, tri_ret;   // cell and step of the triangle tests
+    Stage1 s1;
+};
+
+__device__ __forceinline__ void adv_start_query(const DScene& S, const TraceArgs& A, const RayCtx& r, AdvState& q,
+                                                int* stack) {
+    q.inv[0] = 1.0 / r.d.x;
+    q.inv[1] = 1.0 / r.d.y;
+    q.inv[2] = 1.0 / r.d.z;
+    q.neg[0] = q.inv[0] < 0.0;
+    q.neg[1] = q.inv[1] < 0.0;
+    q.neg[2] = q.inv[2] < 0.0;
+    q.use_cull = cull_ok(S, A.cull, r.o, r.d);
+    if (q.use_cull) q.cr = make_cull_ray(S, r.o, r.d);
+    q.best_t = CUDART_INF;
+    q.best_obj = -1;
+    q.best_e = -1;
+    q.err = 0;
+    q.err_obj = -1;
+    q.ev0 = q.ev1 = 0.0;
+    q.sp = 0;
+    stack[q.sp++] = 0;
+}
+
+// One of the six Moller-Trumbore tests of cell (i, j): step = 2 * sign + triangle,
+// sign order 0, +1, -1 of the sagitta along the cell normal, triangles
+// (q00,q10,q11) then (q00,q11,q01) — the order and arithmetic of stage1_cell.
+__device__ __forceinline__ void stage1_tri(const double* __restrict__ X, const double* __restrict__ CC, int n, int i,
+                                           int j, int step, const V3& o, const V3& d, Stage1& best) {
+    const int nc = n - 1;
+    const double* r0 = X + static_cast<long long>(i * n + j) * 3;
+    const double* r1 = r0 + 3 * n;
+    const double* c = CC + static_cast<long long>(i * nc + j) * 4;
+    const V3 cn = v3(c[0], c[1], c[2]);
+    const int k = step >> 1;
+    const double sg = (k == 0) ? 0.0 : ((k == 1) ? 1.0 : -1.0);
+    const double dd = sg * c[3];
+    const V3 p00 = load3(r0), p11 = load3(r1 + 3);
+    const V3 pm = (step & 1) ? load3(r0 + 3) : load3(r1);   // p01 for the second triangle, p10 for the first
+    const V3 q00 = v3(p00.x + cn.x * dd, p00.y + cn.y * dd, p00.z + cn.z * dd);
+    const V3 q11 = v3(p11.x + cn.x * dd, p11.y + cn.y * dd, p11.z + cn.z * dd);
+    const V3 qm = v3(pm.x + cn.x * dd, pm.y + cn.y * dd, pm.z + cn.z * dd);
+    double t;
+    const bool hit = (step & 1) ? mt_exact(o, d, q00, q11, qm, t) : mt_exact(o, d, q00, qm, q11, t);
+    if (hit) best.consider(t, (i * nc + j) * 6 + step);
+}
+
+// Advances runnable rays until each needs a Newton solve, overflows its
+// resolved list, or finishes.  Persistent: lanes fetch rays from the
+// runnable set until it is drained.
+__global__ void __launch_bounds__(128) k_advance(DScene S, TraceArgs A, WaveArgs W) {
+    Counters ctr, cray;
+    RayTally tally;
+    NewtonRequest rq;
+    rq.ray = -1;
+    long long i = -1;
+    int mode = M_IDLE;
+    RayCtx r;
+    int nres = 0;
+    AdvState q;
+    int stack[64];
+    const int n = S.coarse_n, nc = n - 1, NB = S.n_blocks_side, B = S.block_cells;
+    // The first S.smem_nodes BVH nodes (breadth-first order: the top levels)
+    // are staged in shared memory for the whole launch.
+    extern __shared__ double smem_bvh[];
+    double* sbox = smem_bvh;
+    int* slink = reinterpret_cast<int*>(smem_bvh + 6 * S.smem_nodes);
+    for (int k = threadIdx.x; k < 6 * S.smem_nodes; k += blockDim.x) sbox[k] = S.node_box[k];
+    for (int k = threadIdx.x; k < 4 * S.smem_nodes; k += blockDim.x) slink[k] = S.node_link[k];
+    __syncthreads();
+    while (true) {
+        // ---- one unit of work
+        if (mode == M_NODE) {
+            if (q.sp == 0) {
+                mode = M_RESOLVE;
+            } else {
+                const int idx = stack[--q.sp];
+                ++cray.node_tests;
+                const bool staged = idx < S.smem_nodes;
+                const double* box = staged ? sbox + 6 * idx : S.node_box + 6LL * idx;
+                if (ray_box_exact(r.o, q.inv, box, q.best_t)) {
+                    const int* link = staged ? slink + 4 * idx : S.node_link + 4LL * idx;
+                    if (link[1] < 0) {
+                        q.leaf_start = link[0];
+                        q.leaf_count = link[2];
+                        q.leaf_k = 0;
+                        mode = M_LEAF;
+                    } else if (q.sp + 2 > 64) {
+                        q.err = BBRT_RAY_STACK_OVERFLOW;
+                        q.err_obj = -1;
+                        mode = M_RESOLVE;
+                    } else {
+                        const int left = link[0], right = link[1];
+                        if (q.neg[link[3]]) { stack[q.sp++] = left; stack[q.sp++] = right; }
+                        else                { stack[q.sp++] = right; stack[q.sp++] = left; }
+                    }
+                }
+            }
+        } else if (mode == M_LEAF) {
+            if (q.leaf_k >= q.leaf_count) {
+                mode = M_NODE;
+            } else {
+                const int obj = S.leaf_objects[q.leaf_start + q.leaf_k];
+                if (S.obj_kind[obj] != BBRT_OBJ_PATCH) {
+                    QHit h;
+                    if (triangle_intersect(S, S.obj_sub[obj], r.o, r.d, h, cray) && h.t < q.best_t) {
+                        q.best_t = h.t;
+                        q.best_obj = obj;
+                        q.best_e = -1;
+                        q.tri_u = h.u;
+                        q.tri_v = h.v;
+                    }
+                    ++q.leaf_k;
+                } else {
+                    int e = -1;
+                    for (int k = 0; k < nres; ++k)
+                        if (W.res_obj[i * kResolved + k] == obj) { e = k; break; }
+                    if (e >= 0) {
+                        const long long ei = i * kResolved + e;
+                        const int err = W.res_err[ei];
+                        if (err) {
+                            q.err = err;
+                            q.err_obj = obj;
+                            q.ev0 = W.res_data[ei * kResData + 9];
+                            q.ev1 = W.res_data[ei * kResData + 10];
+                            mode = M_RESOLVE;
+                        } else {
+                            const double t = W.res_data[ei * kResData];
+                            if (t < q.best_t) {
+                                q.best_t = t;
+                                q.best_obj = obj;
+                                q.best_e = e;
+                            }
+                            ++q.leaf_k;
+                        }
+                    } else {
+                        q.obj = obj;
+                        q.pidx = S.obj_sub[obj];
+                        q.s1.have = false;
+                        ++cray.patch_tests;
+                        if (q.use_cull) {
+                            q.bi = 0;
+                            q.bj = 0;
+                            mode = M_BLOCK;
+                        } else {
+                            q.ci = 0;
+                            mode = M_CELL_ALL;
+                        }
+                    }
+                }
+            }
+        } else if (mode == M_BLOCK) {
+            if (q.bi >= NB) {
+                mode = M_S1_DONE;
+            } else {
+                const float* bb = S.c_block_box + (static_cast<long long>(q.pidx) * NB * NB + q.bi * NB + q.bj) * 6;
+                ++cray.cell_tests;
+                const bool pass = cull_box(bb, q.cr);
+                const int bi = q.bi, bj = q.bj;
+                if (++q.bj == NB) { q.bj = 0; ++q.bi; }
+                if (pass) {
+                    q.ci = bi * B;
+                    q.cj = bj * B;
+                    q.j0 = q.cj;
+                    q.i1 = min(nc, (bi + 1) * B);
+                    q.j1 = min(nc, (bj + 1) * B);
+                    mode = M_CELL;
+                }
+            }
+        } else if (mode == M_CELL) {
+            if (q.ci >= q.i1) {
+                mode = M_BLOCK;
+            } else {
+                const int ci = q.ci, cj = q.cj;
+                if (++q.cj == q.j1) { q.cj = q.j0; ++q.ci; }
+                ++cray.cell_tests;
+                const float* cb = S.c_cell_box + (static_cast<long long>(q.pidx) * nc * nc + ci * nc + cj) * 6;
+                if (cull_box(cb, q.cr)) {
+                    q.tci = ci;
+                    q.tcj = cj;
+                    q.tri = 0;
+                    q.tri_ret = M_CELL;
+                    mode = M_TRI;
+                }
+            }
+        } else if (mode == M_CELL_ALL) {
+            if (q.ci >= nc * nc) {
+                mode = M_S1_DONE;
+            } else {
+                q.tci = q.ci / nc;
+                q.tcj = q.ci % nc;
+                ++q.ci;
+                q.tri = 0;
+                q.tri_ret = M_CELL_ALL;
+                mode = M_TRI;
+            }
+        } else if (mode == M_TRI) {
+            ++cray.tri_tests;
+            stage1_tri(S.c_xyz + static_cast<long long>(q.pidx) * n * n * 3,
+                       S.c_cell + static_cast<long long>(q.pidx) * nc * nc * 4, n, q.tci, q.tcj, q.tri, r.o, r.d, q.s1);
+            if (++q.tri == 6) mode = q.tri_ret;
+        } else if (mode == M_S1_DONE) {
+            if (!q.s1.have) {
+                ++q.leaf_k;
+                mode = M_LEAF;
+            } else if (nres >= kResolved) {
+                mode = M_OVERFLOW;
+            } else {
+                W.res_obj[i * kResolved + nres] = q.obj;
+                rq.ray = static_cast<int>(i);
+                rq.entry = nres;
+                rq.obj = q.obj;
+                rq.key = q.s1.key;
+                rq.t0 = q.s1.t;
+                mode = M_SUSPEND;
+            }
+        } else if (mode == M_RESOLVE) {
+            ++tally.queries;
+            QHit h;
+            h.err = q.err;
+            h.obj = q.err ? q.err_obj : q.best_obj;
+            h.ev0 = q.ev0;
+            h.ev1 = q.ev1;
+            if (!q.err && q.best_obj >= 0) {
+                if (q.best_e >= 0) {
+                    const double* rd = W.res_data + (i * kResolved + q.best_e) * kResData;
+                    h.t = rd[0];
+                    h.p = v3(rd[1], rd[2], rd[3]);
+                    h.n = v3(rd[4], rd[5], rd[6]);
+                    h.u = rd[7];
+                    h.v = rd[8];
+                } else {
+                    const double* v = S.tri + static_cast<long long>(S.obj_sub[q.best_obj]) * 9;
+                    const V3 v0 = load3(v), v1 = load3(v + 3), v2 = load3(v + 6);
+                    h.t = q.best_t;
+                    h.p = v3(r.o.x + h.t * r.d.x, r.o.y + h.t * r.d.y, r.o.z + h.t * r.d.z);
+                    h.n = vnormalize(vcross(vsub(v1, v0), vsub(v2, v0)));
+                    h.u = q.tri_u;
+                    h.v = q.tri_v;
+                }
+            }
+            nres = 0;
+            if (!step_ray(S, A, i, r, h)) {
+                mode = M_FINISH;
+            } else if (r.bounces >= A.max_bounces) {
+                r.status = BBRT_RAY_MAX_BOUNCES;
+                mode = M_FINISH;
+            } else {
+                adv_start_query(S, A, r, q, stack);
+                mode = M_NODE;
+            }
+        }
+        // Only when some lane's ray left its working modes (one vote in the
+        // common case): retire suspended / overflowed / finished rays, then
+        // let idle lanes fetch the next runnable ray.
+        if (__ballot_sync(0xffffffffu, mode >= M_FINISH) == 0u) continue;
+        const long long rs = warp_append(&W.counters[0], mode == M_SUSPEND);
+        if (rs >= 0) W.req[rs] = rq;
+        const long long os = warp_append(&W.counters[1], mode == M_OVERFLOW);
+        if (os >= 0) W.overflow[os] = static_cast<int>(i);
+        if (mode == M_SUSPEND || mode == M_OVERFLOW || mode == M_FINISH) {
+            add_ray_work(A, i, cray);
+            ctr.node_tests += cray.node_tests;
+            ctr.patch_tests += cray.patch_tests;
+            ctr.cell_tests += cray.cell_tests;
+            ctr.tri_tests += cray.tri_tests;
+            if (mode == M_SUSPEND) {
+                save_ray(W, i, r, nres + 1);
+            } else if (mode == M_OVERFLOW) {
+                save_ray(W, i, r, nres);
+            } else {
+                finish_ray(A, i, r);
+                tally.bounces += r.bounces;
+                tally.hist[r.status]++;
+            }
+            mode = M_IDLE;
+        }
+        const bool need = (mode == M_IDLE);
+        const long long fs = warp_append(&W.counters[2], need);
+        if (need) {
+            if (fs < W.n_runnable) {
+                cray = Counters();
+                nres = 0;
+                if (W.runnable == nullptr) {
+                    i = W.order ? W.order[fs] : fs;
+                    init_outputs(A, i);
+                    r = start_ray(A, i);
+                } else {
+                    i = W.runnable[fs].ray;
+                    r = load_ray(W, i, nres);
+                }
+                mode = M_FINISH;
+                if (r.status < 0) {
+                    if (r.bounces >= A.max_bounces) {
+                        r.status = BBRT_RAY_MAX_BOUNCES;
+                    } else {
+                        adv_start_query(S, A, r, q, stack);
+                        mode = M_NODE;
+                    }
+                }
+            } else {
+                mode = M_DRAINED;
+            }
+        }
+        if (__all_sync(0xffffffffu, mode == M_DRAINED)) break;
     }
+    flush_stats(A, ctr, tally);
+}
+
+// Newton solves of one round, one request per thread.
+__global__ void __launch_bounds__(128) k_newton(DScene S, TraceArgs A, WaveArgs W, long long n_req) {
+    const long long j = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    long long iters = 0;
+    if (j < n_req) {
+        const NewtonRequest q = W.req[j];
+        const V3 o = load3(W.o + 3LL * q.ray);
+        const V3 d = load3(W.d + 3LL * q.ray);
+        double u0, v0;
+        key_to_uv(S, q.key, u0, v0);
+        QHit h;
+        h.err = 0;
+        h.ev0 = h.ev1 = 0.0;
+        h.t = 0.0;
+        h.p = h.n = v3(0.0, 0.0, 0.0);
+        h.u = h.v = 0.0;
+        newton_exact(S, S.obj_sub[q.obj], o, d, u0, v0, q.t0, h, iters);
+        const long long e = static_cast<long long>(q.ray) * kResolved + q.entry;
+        double* rd = W.res_data + e * kResData;
+        rd[0] = h.t; rd[1] = h.p.x; rd[2] = h.p.y; rd[3] = h.p.z;
+        rd[4] = h.n.x; rd[5] = h.n.y; rd[6] = h.n.z; rd[7] = h.u; rd[8] = h.v; rd[9] = h.ev0; rd[10] = h.ev1;
+        W.res_err[e] = h.err;
+        if (A.ray_work) A.ray_work[4LL * q.ray + 3] += iters;
+    }
+    if (A.stats) warp_add(A.stats + ST_NEWTON_ITERS, iters);
+}
+
+// Finishes rays from their saved state with inline queries (the tail of a
+// wavefront trace, and rays whose query overflowed the resolved list).  The
+// current bounce's query restarts from the root, so the result is the same.
+__global__ void __launch_bounds__(128) k_resume(DScene S, TraceArgs A, WaveArgs W, const NewtonRequest* reqs,
+                                                const int* rays, long long n) {
+    const long long slot = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    Counters ctr;
+    RayTally tally;
+    if (slot < n) {
+        const long long i = reqs ? reqs[slot].ray : rays[slot];
+        int nres;
+        RayCtx r = load_ray(W, i, nres);
+        run_ray(S, A, i, r, ctr, tally.queries);
+        add_ray_work(A, i, ctr);
+        finish_ray(A, i, r);
+        tally.bounces += r.bounces;
+        tally.hist[r.status]++;
+    }
+    flush_stats(A, ctr, tally);
+}
+
+// ---- warp-per-ray form: 32 lanes cooperate on one ray ----------------------
+//
+// Used for the last rays of a wavefront trace, where too few rays are left
+// to fill the GPU and one lane per ray would run each ray's long chain of
+// dependent queries alone.  Traversal, bookkeeping and Newton run on every
+// lane with identical values (the warp stays converged); the stage-1 box and
+// triangle tests of a patch are split over the lanes and the winner is the
+// (t, key) minimum over the warp, which is what the reference's ordered loop
+// keeps for finite t.  Non-finite rays take the ordered per-lane loop.
+
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ void warp_min_stage1(Stage1& s) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const int oh = __shfl_xor_sync(kFull, s.have ? 1 : 0, off);
+        const double ot = __shfl_xor_sync(kFull, s.t, off);
+        const int ok = __shfl_xor_sync(kFull, s.key, off);
+        if (oh) s.consider(ot, ok);
+    }
+}
+
+// Lane `lane` runs the `k`-th of the six triangle tests of each passing cell in
+// `cm` (cells enumerated by the set bits of cm, offsets into (ci0, cj0) grid of
+// width w), 32 tests at a time.
+__device__ __forceinline__ void warp_cell_tris(const double* X, const double* CC, int n, unsigned cm, int base_i,
+                                               int base_j, int w, int c0, const V3& o, const V3& d, int lane,
+                                               Stage1& best) {
+    const int total = __popc(cm) * 6;
+    for (int p0 = 0; p0 < total; p0 += 32) {
+        const int p = p0 + lane;
+        if (p < total) {
+            const int bit = __fns(cm, 0, p / 6 + 1);
+            const int c = c0 + bit;
+            stage1_tri(X, CC, n, base_i + c / w, base_j + c % w, p % 6, o, d, best);
+        }
+    }
+}
+
+__device__ Stage1 warp_patch_stage1(const DScene& S, int pidx, const V3& o, const V3& d, bool use_cull,
+                                    const CullRay& cr, int lane, Counters& ctr) {
+    const int n = S.coarse_n, nc = n - 1;
+    const double* X = S.c_xyz + static_cast<long long>(pidx) * n * n * 3;
+    const double* CC = S.c_cell + static_cast<long long>(pidx) * nc * nc * 4;
+    Stage1 best;
+    if (lane == 0) ++ctr.patch_tests;
+    if (!(finite3(o) && finite3(d))) {
+        // ordered loop on every lane (same result everywhere)
+        Counters dummy;
+        best = patch_stage1(S, pidx, o, d, false, cr, dummy);
+        if (lane == 0) ctr.tri_tests += 6LL * nc * nc;
+        return best;
+    }
+    if (use_cull) {
+        const int B = S.block_cells, NB = S.n_blocks_side, NB2 = NB * NB;
+        const float* BB = S.c_block_box + static_cast<long long>(pidx) * NB2 * 6;
+        const float* CB = S.c_cell_box + static_cast<long long>(pidx) * nc * nc * 6;
+        for (int b0 = 0; b0 < NB2; b0 += 32) {
+            const int b = b0 + lane;
+            unsigned bm = __ballot_sync(kFull, b < NB2 && cull_box(BB + b * 6, cr));
+            if (lane == 0) ctr.cell_tests += min(32, NB2 - b0);
+            while (bm) {
+                const int bl = __ffs(bm) - 1;
+                bm &= bm - 1;
+                const int bi = (b0 + bl) / NB, bj = (b0 + bl) % NB;
+                const int i0 = bi * B, j0 = bj * B;
+                const int h = min(nc, i0 + B) - i0, w = min(nc, j0 + B) - j0;
+                for (int c0 = 0; c0 < h * w; c0 += 32) {
+                    const int c = c0 + lane;
+                    const unsigned cm = __ballot_sync(kFull, c < h * w && cull_box(CB + ((i0 + c / w) * nc + j0 + c % w) * 6, cr));
+                    if (lane == 0) { ctr.cell_tests += min(32, h * w - c0); ctr.tri_tests += 6 * __popc(cm); }
+                    warp_cell_tris(X, CC, n, cm, i0, j0, w, c0, o, d, lane, best);
+                }
+            }
+        }
+    } else {
+        const int total = nc * nc * 6;
+        for (int p = lane; p < total; p += 32) stage1_tri(X, CC, n, (p / 6) / nc, (p / 6) % nc, p % 6, o, d, best);
+        if (lane == 0) ctr.tri_tests += total;
+    }
+    warp_min_stage1(best);
+    return best;
+}
+
+// BVH::intersect for one ray with a whole warp (every lane returns the same result).
+__device__ QHit warp_bvh_query(const DScene& S, const V3& o, const V3& d, int cull_flag, int lane, Counters& ctr) {
+    QHit best;
+    best.obj = -1;
+    best.err = 0;
+    best.t = CUDART_INF;
+    const double inv[3] = { 1.0 / d.x, 1.0 / d.y, 1.0 / d.z };
+    const bool neg[3] = { inv[0] < 0.0, inv[1] < 0.0, inv[2] < 0.0 };
+    const bool use_cull = cull_ok(S, cull_flag, o, d);
+    CullRay cr;
+    if (use_cull) cr = make_cull_ray(S, o, d);
+    double best_t = CUDART_INF;
+    int stack[64];
+    int sp = 0;
+    stack[sp++] = 0;
+    while (sp > 0) {
+        const int idx = stack[--sp];
+        if (lane == 0) ++ctr.node_tests;
+        if (!ray_box_exact(o, inv, S.node_box + 6LL * idx, best_t)) continue;
+        const int* link = S.node_link + 4LL * idx;
+        if (link[1] < 0) {
+            const int start = link[0], count = link[2];
+            for (int k = 0; k < count; ++k) {
+                const int obj = S.leaf_objects[start + k];
+                QHit h;
+                h.err = 0;
+                h.ev0 = h.ev1 = 0.0;
+                int r = 0;
+                if (S.obj_kind[obj] == BBRT_OBJ_PATCH) {
+                    const int pidx = S.obj_sub[obj];
+                    const Stage1 s1 = warp_patch_stage1(S, pidx, o, d, use_cull, cr, lane, ctr);
+                    if (s1.have) {
+                        double u0, v0;
+                        key_to_uv(S, s1.key, u0, v0);
+                        long long it = 0;
+                        r = newton_exact(S, pidx, o, d, u0, v0, s1.t, h, it);
+                        if (lane == 0) ctr.newton_iters += it;
+                    }
+                } else {
+                    Counters dummy;
+                    r = triangle_intersect(S, S.obj_sub[obj], o, d, h, dummy);
+                }
+                if (h.err) {
+                    h.obj = obj;
+                    return h;
+                }
+                if (r && h.t < best_t) {
+                    best_t = h.t;
+                    best = h;
+                    best.obj = obj;
+                }
+            }
+            continue;
+        }
+        if (sp + 2 > 64) {
+            best.err = BBRT_RAY_STACK_OVERFLOW;
+            best.obj = -1;
+            return best;
+        }
+        const int left = link[0], right = link[1];
+        if (neg[link[3]]) { stack[sp++] = left; stack[sp++] = right; }
+        else              { stack[sp++] = right; stack[sp++] = left; }
+    }
+    return best;
+}
+
+// Finishes rays from their saved state, one warp per ray.
+__global__ void __launch_bounds__(128) k_resume_warp(DScene S, TraceArgs A, WaveArgs W, const NewtonRequest* reqs,
+                                                     const int* rays, long long n) {
+    const int lane = threadIdx.x & 31;
+    const long long warp = (blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x) >> 5;
+    const long long n_warps = (static_cast<long long>(gridDim.x) * blockDim.x) >> 5;
+    Counters ctr;
+    RayTally tally;
+    for (long long slot = warp; slot < n; slot += n_warps) {
+        const long long i = reqs ? reqs[slot].ray : rays[slot];
+        int nres;
+        RayCtx r = load_ray(W, i, nres);
+        Counters c1;
+        while (r.status < 0) {
+            if (r.bounces >= A.max_bounces) { r.status = BBRT_RAY_MAX_BOUNCES; break; }
+            if (lane == 0) ++tally.queries;
+            const QHit h = warp_bvh_query(S, r.o, r.d, A.cull, lane, c1);
+            if (!step_ray(S, A, i, r, h, lane == 0)) break;
+        }
+        if (lane == 0) {
+            add_ray_work(A, i, c1);
+            finish_ray(A, i, r);
+            tally.bounces += r.bounces;
+            tally.hist[r.status]++;
+        }
+        ctr.node_tests += c1.node_tests;
+        ctr.patch_tests += c1.patch_tests;
+        ctr.cell_tests += c1.cell_tests;
+        ctr.tri_tests += c1.tri_tests;
+        ctr.newton_iters += c1.newton_iters;
+    }
+    flush_stats(A, ctr, tally);
 }
 
 // One query per ray: BVH, brute force over all objects, or one object.
@@ -406,6 +1095,73 @@ cudaError_t launch_trace(const DScene& S, const TraceArgs& A, cudaStream_t strea
     const long long need = (A.n + 127) / 128;
     if (blocks > need) blocks = need;
     k_trace<<<static_cast<unsigned>(blocks), 128, 0, stream>>>(S, A);
+    return cudaGetLastError();
+}
+
+size_t wave_bytes_per_ray() {
+    return sizeof(double) * 9 + sizeof(int) * 2 + sizeof(int) * 2 * kResolved + sizeof(double) * kResolved * kResData +
+           2 * sizeof(NewtonRequest) + sizeof(int);
+}
+
+// Carves the wavefront workspace for n rays out of `ws` (wave_bytes_per_ray() * n bytes).
+void wave_layout(void* ws, long long n, WaveArgs& W, NewtonRequest*& req_a, NewtonRequest*& req_b) {
+    char* p = static_cast<char*>(ws);
+    auto take = [&](size_t bytes) { char* q = p; p += (bytes + 255) & ~static_cast<size_t>(255); return q; };
+    W.o = reinterpret_cast<double*>(take(sizeof(double) * 3 * n));
+    W.d = reinterpret_cast<double*>(take(sizeof(double) * 3 * n));
+    W.end = reinterpret_cast<double*>(take(sizeof(double) * 3 * n));
+    W.bounces = reinterpret_cast<int*>(take(sizeof(int) * n));
+    W.nres = reinterpret_cast<int*>(take(sizeof(int) * n));
+    W.res_obj = reinterpret_cast<int*>(take(sizeof(int) * kResolved * n));
+    W.res_err = reinterpret_cast<int*>(take(sizeof(int) * kResolved * n));
+    W.res_data = reinterpret_cast<double*>(take(sizeof(double) * kResolved * kResData * n));
+    req_a = reinterpret_cast<NewtonRequest*>(take(sizeof(NewtonRequest) * n));
+    req_b = reinterpret_cast<NewtonRequest*>(take(sizeof(NewtonRequest) * n));
+    W.overflow = reinterpret_cast<int*>(take(sizeof(int) * n));
+}
+
+size_t wave_workspace_bytes(long long n) { return wave_bytes_per_ray() * n + 16 * 256; }
+
+cudaError_t launch_advance(const DScene& S, const TraceArgs& A, const WaveArgs& W, int sm_count, cudaStream_t stream) {
+    if (W.n_runnable <= 0) return cudaSuccess;
+    const size_t smem = static_cast<size_t>(S.smem_nodes) * (6 * sizeof(double) + 4 * sizeof(int));
+    cudaError_t e = cudaFuncSetAttribute(k_advance, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_advance, 128, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    long long blocks = static_cast<long long>(per_sm) * sm_count;
+    const long long need = (W.n_runnable + 127) / 128;
+    if (blocks > need) blocks = need;
+    k_advance<<<static_cast<unsigned>(blocks), 128, smem, stream>>>(S, A, W);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_newton(const DScene& S, const TraceArgs& A, const WaveArgs& W, long long n_req, cudaStream_t stream) {
+    if (n_req <= 0) return cudaSuccess;
+    k_newton<<<static_cast<unsigned>((n_req + 127) / 128), 128, 0, stream>>>(S, A, W, n_req);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_resume(const DScene& S, const TraceArgs& A, const WaveArgs& W, const NewtonRequest* reqs,
+                          const int* rays, long long n, cudaStream_t stream) {
+    if (n <= 0) return cudaSuccess;
+    k_resume<<<static_cast<unsigned>((n + 127) / 128), 128, 0, stream>>>(S, A, W, reqs, rays, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_resume_warp(const DScene& S, const TraceArgs& A, const WaveArgs& W, const NewtonRequest* reqs,
+                               const int* rays, long long n, int sm_count, cudaStream_t stream) {
+    if (n <= 0) return cudaSuccess;
+    int per_sm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_resume_warp, 128, 0);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    long long blocks = static_cast<long long>(per_sm) * sm_count;
+    const long long need = (n + 3) / 4;   // four warps (rays) per block
+    if (blocks > need) blocks = need;
+    k_resume_warp<<<static_cast<unsigned>(blocks), 128, 0, stream>>>(S, A, W, reqs, rays, n);
     return cudaGetLastError();
 }
 

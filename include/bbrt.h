@@ -181,6 +181,8 @@ typedef struct bbrt_trace_out {
     double* hit_uv;         /* [n*K*2] Newton (u,v) of each recorded hit */
     int*    err_object;     /* [n] object whose intersect failed (Newton kinds), else -1 */
     double* err_value;      /* [n*2] the number the reference's message quotes */
+    long long* ray_work;    /* [n*4] optional work profile per ray: BVH node tests, stage-1
+                               block/cell box tests, Moller-Trumbore tests, Newton iterations */
 } bbrt_trace_out;
 
 typedef struct bbrt_trace_stats {

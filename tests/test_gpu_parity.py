@@ -80,7 +80,9 @@ def test_single_object_queries(built, workloads):
         c = sc.object_info(k)["centroid"]
         o = c + rng.normal(size=(256, 3)) * 0.2 + sc.object_info(k)["centroid"] * 0.5
         d = c - o + rng.normal(size=(256, 3)) * 0.05
-        assert np.array_equal(sc.intersect(o, d, C.QUERY_OBJECT, k), orc.intersect(o, d, C.QUERY_OBJECT, k))
+        g, r = sc.intersect(o, d, C.QUERY_OBJECT, k), orc.intersect(o, d, C.QUERY_OBJECT, k)
+        diff = [i for i in range(len(g)) if g[i].tobytes() != r[i].tobytes()]
+        assert not diff, (k, diff[:5], g[diff[0]], r[diff[0]], o[diff[0]], d[diff[0]])
 
 
 def test_reference_triangle_unit_test(built):
@@ -196,3 +198,54 @@ def test_full_size_tetra_workload(built, workloads):
     r = oracle.Oracle(patches, config=C.default_config(coarse_grid_n=cn, newton_tol=tol)).trace(o[sel], d[sel], maxb, K=0)
     for k in outs:
         assert np.array_equal(a[k][sel], r[k]), k
+
+
+def test_nested_spheres_many_solves_per_query(built):
+    """Concentric spheres: a ray through the centre crosses many patches, so a
+    single query needs several Newton solves (more than the wavefront's
+    resolved list holds for some rays) — wavefront, overflow and tail paths
+    against the oracle, plus the fused per-ray kernel on a small batch."""
+    patches = []
+    for k, r in enumerate((1.0, 1.4, 1.9, 2.5, 3.2)):
+        patches += scenes.obstacle_patches(k, (0.0, 0.0, 0.0), (r, r, r), None, m=2, n_nodes=5)
+    rng = np.random.Generator(np.random.PCG64(11))
+    n = 20000
+    o = rng.normal(size=(n, 3))
+    o = 6.0 * o / np.linalg.norm(o, axis=1, keepdims=True)
+    d = -o + rng.normal(size=(n, 3)) * 0.8
+    cfg = C.default_config(coarse_grid_n=9, newton_tol=1e-12)
+    sc, orc = api.Scene(patches, config=cfg), oracle.Oracle(patches, config=cfg)
+    g = sc.trace(o, d, 30, record=4)
+    r = orc.trace(o, d, 30, K=4)
+    assert_same_trace(g, r)
+    small = sc.trace(o[:500], d[:500], 30, record=4)
+    for k in ("status", "bounce_count", "hit_object", "hit_point", "end_point", "exit_dir"):
+        assert np.array_equal(small[k], g[k][:500]), k
+
+
+TUNING_SCRIPT = r'''
+import sys, numpy as np
+sys.path.insert(0, sys.argv[1])
+from billardballraytracing3d_b200 import scenes, api, _capi as C
+patches, o, d, maxb, cn, tol = scenes.workload("tetra_spheres", 40000)
+g = api.Scene(patches, config=C.default_config(coarse_grid_n=cn, newton_tol=tol)).trace(o, d, maxb, record=4)
+np.savez(sys.argv[2], **{k: g[k] for k in ("status", "bounce_count", "hit_object", "hit_point", "end_point", "exit_dir")})
+'''
+
+
+@pytest.mark.parametrize("env", [{"BBRT_WAVE_TAIL": "0"}, {"BBRT_WARP_TAIL": "0"}, {"BBRT_WAVE_TAIL": "100000"},
+                                 {"BBRT_ORDER_RAYS": "0", "BBRT_WAVE_MIN": "1000000"}])
+def test_launch_shape_knobs_do_not_change_results(built, workloads, tmp_path, env):
+    """Every schedule (all wavefront rounds, per-thread or per-warp tail, fused
+    kernel only, unordered rays) gives the oracle's results bit for bit."""
+    import os
+    import subprocess
+    import sys
+    from conftest import ROOT
+    out = tmp_path / "r.npz"
+    subprocess.run([sys.executable, "-c", TUNING_SCRIPT, ROOT, str(out)], check=True, env={**os.environ, **env})
+    g = np.load(out)
+    patches, o, d, maxb, cn, tol = workloads("tetra_spheres", 40000)
+    r = oracle.Oracle(patches, config=C.default_config(coarse_grid_n=cn, newton_tol=tol)).trace(o, d, maxb, K=4)
+    for k in g.files:
+        assert np.array_equal(g[k], r[k]), (env, k)
