@@ -43,6 +43,8 @@ size_t ray_order_workspace_bytes(long long n);
 cudaError_t ray_order(const double* o, const double* d, long long n, const double center[3], double radius,
                       void* ws, int* order, cudaStream_t stream);
 cudaError_t launch_query(const DScene& S, const QueryArgs& Q, cudaStream_t stream);
+cudaError_t launch_trace_noalloc(const DScene& S, TraceArgs A, bool count_hits, long long* hit_counts_out,
+                                 long long* host_stats, cudaStream_t stream, int sm_count);
 }  // namespace bbrt
 
 namespace {
@@ -869,6 +871,59 @@ BBRT_API int bbrt_bounce_map(bbrt_scene_t s, const bbrt_patch_desc* samples, int
         err_out[q] = nerr;
         if (best_out) best_out[q] = bdir;
     }
+    return BBRT_OK;
+}
+
+// Allocation-free trace: scratch in the library's static device array (see
+// include/bbrt.h).  No cudaMalloc / cudaFree / event or stream creation here.
+BBRT_API int bbrt_trace_noalloc(bbrt_scene_t s, const double* origins, const double* dirs, long long n,
+                                int max_bounces, const bbrt_trace_out* out, long long* hit_counts,
+                                int count_from, bbrt_trace_stats* stats, void* stream) {
+    if (!s) return fail(BBRT_ERR_ARG, "bbrt_trace_noalloc: NULL scene");
+    if (n < 0) return fail(BBRT_ERR_ARG, "bbrt_trace_noalloc: n < 0");
+    if (n > 0 && (!origins || !dirs)) return fail(BBRT_ERR_ARG, "bbrt_trace_noalloc: NULL rays");
+    if (max_bounces < 0) return fail(BBRT_ERR_ARG, "bbrt_trace_noalloc: max_bounces < 0");
+    if (out && out->record_bounces < 0) return fail(BBRT_ERR_ARG, "bbrt_trace_noalloc: record_bounces < 0");
+    if (hit_counts && s->host.n_objects > BBRT_NOALLOC_MAX_OBJECTS)
+        return fail(BBRT_ERR_ARG, "bbrt_trace_noalloc: hit counts need a scene of at most " +
+                                      std::to_string(BBRT_NOALLOC_MAX_OBJECTS) + " objects (this one has " +
+                                      std::to_string(s->host.n_objects) + ")");
+    std::lock_guard<std::mutex> g(s->mu);
+    if (!s->uploaded)
+        return fail(BBRT_ERR_STATE, "bbrt_trace_noalloc: the scene is not on the device yet (bbrt_scene_upload)");
+    int dev = -1;
+    BBRT_CUDA(cudaGetDevice(&dev));
+    if (dev != s->device)
+        return fail(BBRT_ERR_STATE, "bbrt_trace_noalloc: the current device is not the scene's device");
+    cudaStream_t st = pick_stream(s, stream);
+    long long hs[bbrt::ST_COUNT] = { 0 };
+    if (n > 0) {
+        bbrt::TraceArgs A;
+        A.origins = origins;
+        A.dirs = dirs;
+        A.n = n;
+        A.max_bounces = max_bounces;
+        A.cull = s->host.cfg.cull;
+        if (out) {
+            A.record = out->record_bounces;
+            A.status = out->status;
+            A.bounce_count = out->bounce_count;
+            A.exit_dir = out->exit_dir;
+            A.end_point = out->end_point;
+            A.hit_object = out->hit_object;
+            A.hit_point = out->hit_point;
+            A.hit_uv = out->hit_uv;
+            A.err_object = out->err_object;
+            A.err_value = out->err_value;
+            A.ray_work = out->ray_work;
+        }
+        A.count_from = count_from;
+        BBRT_CUDA(bbrt::launch_trace_noalloc(s->dev, A, hit_counts != nullptr, hit_counts, stats ? hs : nullptr, st,
+                                             s->sm_count));
+    } else if (hit_counts) {
+        BBRT_CUDA(cudaMemsetAsync(hit_counts, 0, sizeof(long long) * s->host.n_objects, st));
+    }
+    if (stats) fill_stats(s, hs, n, 0.0f, 0.0f, stats);
     return BBRT_OK;
 }
 

@@ -16,6 +16,8 @@
 #include <cuda_runtime.h>
 #include <math_constants.h>
 
+#include <mutex>
+
 #include "../../include/bbrt.h"
 #include "exact.cuh"
 
@@ -1096,6 +1098,69 @@ cudaError_t launch_trace(const DScene& S, const TraceArgs& A, cudaStream_t strea
     if (blocks > need) blocks = need;
     k_trace<<<static_cast<unsigned>(blocks), 128, 0, stream>>>(S, A);
     return cudaGetLastError();
+}
+
+// ---- allocation-free trace (bbrt_trace_noalloc) ----------------------------
+//
+// The fused trace kernel's scratch — its ray counter, its statistics block
+// and per-object hit counters — lives in this file-scope device array
+// instead of memory allocated per scene or per call: word 0 is the counter,
+// words [1, 1 + ST_COUNT) the statistics, words [kNoAllocHeader,
+// kNoAllocHeader + n_objects) the hit counters.  One copy exists per device
+// that loads the library, for the life of the process.  Host code must not
+// use the array's name as a device address; noalloc_scratch() returns the
+// address the device sees.
+constexpr int kNoAllocHeader = 32;
+static __device__ __align__(256) unsigned long long g_noalloc_scratch[kNoAllocHeader + BBRT_NOALLOC_MAX_OBJECTS];
+
+// Device address of g_noalloc_scratch on the current device, looked up with
+// cudaGetSymbolAddress the first time each device asks.
+cudaError_t noalloc_scratch(unsigned long long** out) {
+    constexpr int kMaxDevices = 64;
+    static std::mutex mu;
+    static void* addr[kMaxDevices] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> g(mu);
+    if (addr[dev] == nullptr) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        addr[dev] = p;
+    }
+    *out = static_cast<unsigned long long*>(addr[dev]);
+    return cudaSuccess;
+}
+
+// The fused trace kernel with its scratch in g_noalloc_scratch.  Clears the
+// words this call uses first, then traces; hit counters (when asked for) are
+// copied to the caller's device array and the statistics to `host_stats`.
+cudaError_t launch_trace_noalloc(const DScene& S, TraceArgs A, bool count_hits, long long* hit_counts_out,
+                                 long long* host_stats, cudaStream_t stream, int sm_count) {
+    unsigned long long* scratch = nullptr;
+    cudaError_t e = noalloc_scratch(&scratch);
+    if (e != cudaSuccess) return e;
+    const size_t words = kNoAllocHeader + (count_hits ? static_cast<size_t>(S.n_objects) : 0);
+    e = cudaMemsetAsync(scratch, 0, words * sizeof(unsigned long long), stream);
+    if (e != cudaSuccess) return e;
+    A.work_counter = scratch;
+    A.stats = reinterpret_cast<long long*>(scratch + 1);
+    A.hit_counts = count_hits ? scratch + kNoAllocHeader : nullptr;
+    e = launch_trace(S, A, stream, sm_count);
+    if (e != cudaSuccess) return e;
+    if (count_hits) {
+        e = cudaMemcpyAsync(hit_counts_out, scratch + kNoAllocHeader, sizeof(long long) * S.n_objects,
+                            cudaMemcpyDeviceToDevice, stream);
+        if (e != cudaSuccess) return e;
+    }
+    if (host_stats) {
+        e = cudaMemcpyAsync(host_stats, scratch + 1, sizeof(long long) * ST_COUNT, cudaMemcpyDeviceToHost, stream);
+        if (e != cudaSuccess) return e;
+        e = cudaStreamSynchronize(stream);
+    }
+    return e;
 }
 
 size_t wave_bytes_per_ray() {

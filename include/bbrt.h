@@ -300,6 +300,41 @@ enum {
  * the trace kernel's pipes). */
 BBRT_API int bbrt_measure_pipe_peak(int pipe, double* value);
 
+/* ---- allocation-free trace ------------------------------------------------
+ * No counterpart in the reference (it has no device memory at all).
+ *
+ * For callers that must not allocate device memory while tracing: a host
+ * framework whose device memory is all owned by its own arena or fixed
+ * budget, or a latency-critical loop that cannot pay for cudaMalloc /
+ * cudaFree (which synchronise the device).  This call allocates nothing: it
+ * calls no cudaMalloc, cudaFree or allocating library routine.  The caller
+ * owns every input and output (device arrays), and the scene must already be
+ * on the device (bbrt_scene_upload, or any earlier compute call).
+ *
+ * It traces like bbrt_trace with BBRT_DEVICE_PTRS, always one GPU thread per
+ * ray to the end.  Its scratch — the ray counter, the statistics block and,
+ * when hit_counts is not NULL, one hit counter per object — lives in a
+ * static device array of the library, one per device, held until the process
+ * exits.  Limits: with hit_counts the scene may hold at most
+ * BBRT_NOALLOC_MAX_OBJECTS objects (BBRT_ERR_ARG otherwise).
+ *
+ *   hit_counts  device array [n_objects] of long long, or NULL: per object,
+ *               the recorded bounces with index >= count_from (the counting
+ *               of PlaneSourceDriver::run with count_from = 1, or 0 with
+ *               count_direct_hit)
+ *   stats       host struct or NULL (filled after a stream synchronize;
+ *               kernel_ms and total_ms are 0)
+ *
+ * Every call shares the one array per device and clears what it uses at its
+ * start, so calls whose work overlaps on the GPU (different streams or host
+ * threads) race and give wrong results: serialise them.  The first call on
+ * each device looks up the array's device address (cudaGetSymbolAddress);
+ * make that first call before any stream capture. */
+#define BBRT_NOALLOC_MAX_OBJECTS 32768
+BBRT_API int bbrt_trace_noalloc(bbrt_scene_t scene, const double* origins, const double* dirs, long long n,
+                                int max_bounces, const bbrt_trace_out* out, long long* hit_counts,
+                                int count_from, bbrt_trace_stats* stats, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
