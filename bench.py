@@ -130,18 +130,58 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def fp64_flop_model(st, nodes_per_axis):
-    """Executed FP64 work of one trace launch from its counters (the model is
-    stated in DESIGN.md): node slab tests 12, Moller-Trumbore up to the
-    u pre-test 28 (+23 past it, bounded by counting all tests at 51 below),
-    corner offsets 72 per tested cell, Newton 18N^2+24N+70 per iteration,
-    reflection and nudge 18 per bounce."""
-    N = nodes_per_axis
-    tested_cells = st["tri_tests"] / 6.0
-    lo = (12 * st["node_tests"] + 28 * st["tri_tests"] + 72 * tested_cells +
-          (18 * N * N + 24 * N + 70) * st["newton_iters"] + 18 * st["bounces"])
-    hi = lo + 23 * st["tri_tests"]
-    return lo, hi
+def _hbm_peak():
+    """Measured copy bandwidth of this pool's B200 (MEASURED_PEAKS.json), else
+    the pool's earlier measurement."""
+    try:
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
+    except (OSError, ValueError, KeyError):
+        return 6650.0
+
+
+HBM_PEAK_GBS = _hbm_peak()
+PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "k_advance_traffic.json")
+
+
+def advance_roofline(st, fp64_peak, fp32_peak, l2_peak):
+    """Roofline of the dominant kernel, k_advance, from its own counters and its
+    own device time (CUDA events around each launch inside the library).
+
+    Work per unit (the model DESIGN.md states):
+      BVH node test          12 FP64 FLOP, 64 B (box + links)
+      block / cell box test  18 FP32 FLOP, 24 B
+      Moller-Trumbore test   28 FP64 FLOP up to the division-free rejection
+                             (51 when it passes), 18 FP64 FLOP of corner
+                             offsets, 104 B (three corners + cell normal/sagitta)
+    The headline pipe is the one with the largest fraction of its peak."""
+    nodes = st["node_tests"] - st["tail_node_tests"]
+    boxes = st["cell_tests"] - st["tail_cell_tests"]
+    mts = st["tri_tests"] - st["tail_tri_tests"]
+    secs = st["advance_ms"] / 1e3
+    if secs <= 0:
+        return None
+    pipes = {
+        "fp64": ((12 * nodes + (28 + 18) * mts) / secs / 1e12, fp64_peak, "TFLOP/s"),
+        "fp32": (18 * boxes / secs / 1e12, fp32_peak, "TFLOP/s"),
+        "l2": ((64 * nodes + 24 * boxes + 104 * mts) / secs / 1e9, l2_peak, "GB/s"),
+        "hbm": ((64 * nodes + 24 * boxes + 104 * mts) / secs / 1e9, HBM_PEAK_GBS, "GB/s"),
+    }
+    best = max(pipes, key=lambda k: pipes[k][0] / pipes[k][1])
+    a, p, u = pipes[best]
+    traffic = None
+    if os.path.exists(PROFILE_TRAFFIC):
+        prof = json.load(open(PROFILE_TRAFFIC))
+        # scale the captured launch's DRAM bytes to a whole step of k_advance launches by the work done
+        if prof.get("node_tests"):
+            traffic = prof["dram_bytes"] * nodes / prof["node_tests"] / max(1, st["rounds"])
+    return {"bound": best, "achieved": a, "peak": p, "unit": u, "frac": a / p, "traffic": traffic,
+            "kernel": "k_advance", "launches_per_step": int(st["rounds"]),
+            "pipes": {k: {"achieved": v[0], "peak": v[1], "unit": v[2], "frac": v[0] / v[1]} for k, v in pipes.items()},
+            "note": "algorithmic work of the k_advance launches of one step (device counters) over their summed "
+                    "CUDA-event time; peaks: FP64/FP32 FMA and L2-resident reads measured in this process "
+                    "(bbrt_measure_pipe_peak), HBM from MEASURED_PEAKS.json, all of measured; the exact FP64 "
+                    "path runs unfused mul/add (half the FMA peak at most); traffic per launch from the ncu "
+                    "capture in profiles/, scaled by node tests"}
 
 
 def cpu_baseline(patches, o, d, maxb, cn, tol, target_s):
@@ -230,6 +270,8 @@ def run_ours(args, rank, world, local_rank):
     fp64_peak = peak.value
     C.check(lib, lib.bbrt_measure_pipe_peak(C.PIPE_FP32, ctypes.byref(peak)), "bbrt_measure_pipe_peak")
     fp32_peak = peak.value
+    C.check(lib, lib.bbrt_measure_pipe_peak(C.PIPE_L2, ctypes.byref(peak)), "bbrt_measure_pipe_peak")
+    l2_peak = peak.value
 
     to = torch.from_numpy(np.ascontiguousarray(o)).to(dev)
     td = torch.from_numpy(np.ascontiguousarray(d)).to(dev)
@@ -314,16 +356,7 @@ def run_ours(args, rank, world, local_rank):
     if rank != 0:
         return
     per_launch_s = kern_s / args.steps
-    flop_lo, flop_hi = fp64_flop_model(stats, patches[0].imax) if stats else (0.0, 0.0)
-    achieved = flop_lo / per_launch_s / 1e12
-    roofline = {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
-                "frac": achieved / fp64_peak, "traffic": None,
-                "kernel": "k_trace",
-                "note": "executed FP64 work from device counters (lower bound of the model; upper bound "
-                        f"{flop_hi / per_launch_s / 1e12:.3f} TFLOP/s) over the mean CUDA-event launch time; peak = "
-                        "FP64 FMA throughput measured in this process (bbrt_measure_pipe_peak), of measured; "
-                        "the exact path runs with -fmad=false so unfused mul/add cap it at half that peak",
-                "fp32_peak_tflops": fp32_peak}
+    roofline = advance_roofline(stats, fp64_peak, fp32_peak, l2_peak) if stats else None
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * per_launch_s, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -332,7 +365,10 @@ def run_ours(args, rank, world, local_rank):
                                        "cull": args.cull,
                                        "l2": "flushed before each step (256 MiB write), flush outside the timed events",
                                        "bounces_per_step": bounces_per_step}),
-            "e2e": e2e, "gpu_launches": args.steps, "roofline": roofline, "clocks": clk,
+            "e2e": e2e, "gpu_launches": int(stats["launches"]) * args.steps if stats else None,
+            "roofline": roofline, "clocks": clk,
+            "kernel_ms_per_step": {k: stats[k] for k in ("order_ms", "advance_ms", "newton_ms", "tail_ms")}
+            if stats else None,
             "wall_s_timed_region": wall,
             "counters_per_step": {k: v for k, v in (stats or {}).items() if k not in ("kernel_ms", "total_ms")}}
     if world == 1 and not args.no_cpu_baseline:

@@ -159,6 +159,11 @@ class TraceStats(ctypes.Structure):
         ("newton_iters", ctypes.c_longlong), ("newton_iters_fp32", ctypes.c_longlong),
         ("status_hist", ctypes.c_longlong * RAY_STATUS_COUNT),
         ("kernel_ms", ctypes.c_double), ("total_ms", ctypes.c_double),
+        ("order_ms", ctypes.c_double), ("advance_ms", ctypes.c_double), ("newton_ms", ctypes.c_double),
+        ("tail_ms", ctypes.c_double), ("rounds", ctypes.c_longlong), ("tail_rays", ctypes.c_longlong),
+        ("tail_node_tests", ctypes.c_longlong), ("tail_cell_tests", ctypes.c_longlong),
+        ("tail_tri_tests", ctypes.c_longlong), ("tail_newton_iters", ctypes.c_longlong),
+        ("launches", ctypes.c_longlong),
     ]
 
     def as_dict(self):

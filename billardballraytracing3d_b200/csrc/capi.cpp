@@ -99,6 +99,13 @@ struct bbrt_scene {
     DevBuf stats, work, in_o, in_d, o_status, o_bounce, o_dir, o_end, o_hobj, o_hpt, o_huv, o_eobj, o_eval,
         counts, hits, wave, wave_ctr, o_work, order, order_ws;
     unsigned int* wave_ctr_host = nullptr;   // pinned copy of the round counters
+    // per-launch timing of calls that collect statistics
+    static constexpr int kTimerEvents = 96;
+    cudaEvent_t kev[kTimerEvents] = {};
+    int kev_used = 0;
+    bool timing = false;
+    long long rounds = 0, launches = 0;
+    std::vector<std::pair<int, int>> kspans;   // (kernel kind, first event)
     std::mutex mu;
 
     ~bbrt_scene() {
@@ -108,6 +115,8 @@ struct bbrt_scene {
             b->release();
         if (wave_ctr_host) cudaFreeHost(wave_ctr_host);
         for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+        for (auto& e : kev)
             if (e) cudaEventDestroy(e);
         if (stream) cudaStreamDestroy(stream);
     }
@@ -136,6 +145,7 @@ int ensure_uploaded(bbrt_scene* s) {
     BBRT_CUDA(cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, s->device));
     BBRT_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
     for (auto& e : s->ev) BBRT_CUDA(cudaEventCreate(&e));
+    for (auto& e : s->kev) BBRT_CUDA(cudaEventCreate(&e));
     const bbrt::HostScene& H = s->host;
     bbrt::DScene& D = s->dev;
     D = bbrt::DScene();
@@ -280,7 +290,37 @@ void fill_stats(bbrt_scene* s, const long long* st, long long n, float kernel_ms
     for (int k = 0; k < BBRT_RAY_STATUS_COUNT; ++k) out->status_hist[k] = st[bbrt::ST_HIST0 + k];
     out->kernel_ms = kernel_ms;
     out->total_ms = total_ms;
-    (void)s;
+    out->tail_node_tests = st[bbrt::ST_TAIL_NODE_TESTS];
+    out->tail_cell_tests = st[bbrt::ST_TAIL_CELL_TESTS];
+    out->tail_tri_tests = st[bbrt::ST_TAIL_TRI_TESTS];
+    out->tail_newton_iters = st[bbrt::ST_TAIL_NEWTON_ITERS];
+    out->tail_rays = st[bbrt::ST_TAIL_RAYS];
+    double* dst[4] = { &out->order_ms, &out->advance_ms, &out->newton_ms, &out->tail_ms };
+    for (const auto& sp : s->kspans) {
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, s->kev[sp.second], s->kev[sp.second + 1]) == cudaSuccess) *dst[sp.first] += ms;
+    }
+    out->rounds = s->rounds;
+    out->launches = s->launches;
+}
+
+enum { K_ORDER = 0, K_ADVANCE = 1, K_NEWTON = 2, K_TAIL = 3 };
+
+// Records a pair of events around one launch when the call collects statistics.
+template <class F>
+cudaError_t timed(bbrt_scene* s, int kind, cudaStream_t st, F&& launch) {
+    s->launches += (kind == K_ORDER) ? 3 : 1;   // ray ordering is three kernels
+    if (!s->timing || s->kev_used + 2 > bbrt_scene::kTimerEvents) return launch();
+    const int k = s->kev_used;
+    cudaError_t e = cudaEventRecord(s->kev[k], st);
+    if (e != cudaSuccess) return e;
+    e = launch();
+    if (e != cudaSuccess) return e;
+    e = cudaEventRecord(s->kev[k + 1], st);
+    if (e != cudaSuccess) return e;
+    s->kspans.emplace_back(kind, k);
+    s->kev_used += 2;
+    return cudaSuccess;
 }
 
 // Batches at least this large run as a wavefront of advance / Newton rounds;
@@ -339,9 +379,11 @@ int run_wavefront(bbrt_scene* s, const bbrt::TraceArgs& A, cudaStream_t st) {
     if (T.order_rays) {
         BBRT_CUDA(s->order_ws.ensure(bbrt::ray_order_workspace_bytes(n)));
         BBRT_CUDA(s->order.ensure(sizeof(int) * static_cast<size_t>(n)));
-        BBRT_CUDA(bbrt::ray_order(A.origins, A.dirs, n, s->cull.center, s->cull.radius > 0.0 ? s->cull.radius
-                                                                                              : s->host.scene_diagonal,
-                                  s->order_ws.p, static_cast<int*>(s->order.p), st));
+        const double radius = s->cull.radius > 0.0 ? s->cull.radius : s->host.scene_diagonal;
+        BBRT_CUDA(timed(s, K_ORDER, st, [&] {
+            return bbrt::ray_order(A.origins, A.dirs, n, s->cull.center, radius, s->order_ws.p,
+                                   static_cast<int*>(s->order.p), st);
+        }));
         W.order = static_cast<const int*>(s->order.p);
     }
     BBRT_CUDA(cudaMemsetAsync(W.counters, 0, 3 * sizeof(unsigned int), st));
@@ -352,7 +394,8 @@ int run_wavefront(bbrt_scene* s, const bbrt::TraceArgs& A, cudaStream_t st) {
         if (T.log_rounds) BBRT_CUDA(cudaEventRecord(s->ev[2], st));
         BBRT_CUDA(cudaMemsetAsync(W.counters, 0, sizeof(unsigned int), st));
         BBRT_CUDA(cudaMemsetAsync(W.counters + 2, 0, sizeof(unsigned int), st));
-        BBRT_CUDA(bbrt::launch_advance(s->dev, A, W, s->sm_count, st));
+        BBRT_CUDA(timed(s, K_ADVANCE, st, [&] { return bbrt::launch_advance(s->dev, A, W, s->sm_count, st); }));
+        ++s->rounds;
         if (T.log_rounds) BBRT_CUDA(cudaEventRecord(s->ev[3], st));
         BBRT_CUDA(cudaMemcpyAsync(s->wave_ctr_host, W.counters, 2 * sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
         BBRT_CUDA(cudaStreamSynchronize(st));
@@ -366,11 +409,11 @@ int run_wavefront(bbrt_scene* s, const bbrt::TraceArgs& A, cudaStream_t st) {
         }
         if (n_req == 0) break;
         if (n_req <= T.wave_tail) {
-            BBRT_CUDA(run_tail(s, A, W, W.req, nullptr, n_req, st));
+            BBRT_CUDA(timed(s, K_TAIL, st, [&] { return run_tail(s, A, W, W.req, nullptr, n_req, st); }));
             break;
         }
         if (T.log_rounds) BBRT_CUDA(cudaEventRecord(s->ev[2], st));
-        BBRT_CUDA(bbrt::launch_newton(s->dev, A, W, n_req, st));
+        BBRT_CUDA(timed(s, K_NEWTON, st, [&] { return bbrt::launch_newton(s->dev, A, W, n_req, st); }));
         if (T.log_rounds) {
             BBRT_CUDA(cudaEventRecord(s->ev[3], st));
             BBRT_CUDA(cudaEventSynchronize(s->ev[3]));
@@ -383,7 +426,8 @@ int run_wavefront(bbrt_scene* s, const bbrt::TraceArgs& A, cudaStream_t st) {
         W.req = (W.req == req_a) ? req_b : req_a;
         if (round + 1 == max_rounds) return fail(BBRT_ERR_KERNEL, "bbrt_trace: wavefront round bound reached");
     }
-    if (overflowed > 0) BBRT_CUDA(run_tail(s, A, W, nullptr, W.overflow, overflowed, st));
+    if (overflowed > 0)
+        BBRT_CUDA(timed(s, K_TAIL, st, [&] { return run_tail(s, A, W, nullptr, W.overflow, overflowed, st); }));
     return BBRT_OK;
 }
 
@@ -418,9 +462,14 @@ int run_trace_device(bbrt_scene* s, const double* d_o, const double* d_d, long l
     A.work_counter = static_cast<unsigned long long*>(s->work.p);
     if (want_stats) BBRT_CUDA(cudaMemsetAsync(s->stats.p, 0, sizeof(long long) * bbrt::ST_COUNT, st));
     BBRT_CUDA(cudaMemsetAsync(s->work.p, 0, sizeof(unsigned long long), st));
+    s->timing = want_stats;
+    s->kev_used = 0;
+    s->kspans.clear();
+    s->rounds = 0;
+    s->launches = 0;
     BBRT_CUDA(cudaEventRecord(s->ev[0], st));
     if (n < tuning().wave_min_rays) {
-        BBRT_CUDA(bbrt::launch_trace(s->dev, A, st, s->sm_count));
+        BBRT_CUDA(timed(s, K_TAIL, st, [&] { return bbrt::launch_trace(s->dev, A, st, s->sm_count); }));
     } else {
         const int rc = run_wavefront(s, A, st);
         if (rc) return rc;
@@ -897,6 +946,9 @@ BBRT_API int bbrt_trace_noalloc(bbrt_scene_t s, const double* origins, const dou
         return fail(BBRT_ERR_STATE, "bbrt_trace_noalloc: the current device is not the scene's device");
     cudaStream_t st = pick_stream(s, stream);
     long long hs[bbrt::ST_COUNT] = { 0 };
+    s->kspans.clear();   // no per-kernel timing here (keeps capacity: no allocation)
+    s->rounds = 0;
+    s->launches = n > 0 ? 1 : 0;
     if (n > 0) {
         bbrt::TraceArgs A;
         A.origins = origins;

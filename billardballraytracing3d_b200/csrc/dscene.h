@@ -62,7 +62,10 @@ struct DScene {
 // Counter slots of the per-launch statistics buffer (long long each).
 enum StatSlot {
     ST_BOUNCES = 0, ST_QUERIES, ST_NODE_TESTS, ST_PATCH_TESTS, ST_CELL_TESTS, ST_TRI_TESTS,
-    ST_NEWTON_ITERS, ST_NEWTON_ITERS_FP32, ST_HIST0, ST_COUNT = ST_HIST0 + 8
+    ST_NEWTON_ITERS, ST_NEWTON_ITERS_FP32, ST_HIST0,
+    // share of the tail kernels (also included in the totals above)
+    ST_TAIL_NODE_TESTS = ST_HIST0 + 8, ST_TAIL_CELL_TESTS, ST_TAIL_TRI_TESTS, ST_TAIL_NEWTON_ITERS, ST_TAIL_RAYS,
+    ST_COUNT
 };
 
 struct TraceArgs {

@@ -371,8 +371,19 @@ struct RayTally {
     long long hist[BBRT_RAY_STATUS_COUNT] = { 0, 0, 0, 0, 0, 0, 0, 0 };
 };
 
-__device__ __forceinline__ void flush_stats(const TraceArgs& A, const Counters& ctr, const RayTally& t) {
+__device__ __forceinline__ void flush_stats(const TraceArgs& A, const Counters& ctr, const RayTally& t,
+                                            bool tail = false) {
     if (!A.stats) return;
+    if (tail) {
+        long long rays = 0;
+#pragma unroll
+        for (int k = 0; k < BBRT_RAY_STATUS_COUNT; ++k) rays += t.hist[k];
+        warp_add(A.stats + ST_TAIL_NODE_TESTS, ctr.node_tests);
+        warp_add(A.stats + ST_TAIL_CELL_TESTS, ctr.cell_tests);
+        warp_add(A.stats + ST_TAIL_TRI_TESTS, ctr.tri_tests);
+        warp_add(A.stats + ST_TAIL_NEWTON_ITERS, ctr.newton_iters);
+        warp_add(A.stats + ST_TAIL_RAYS, rays);
+    }
     warp_add(A.stats + ST_BOUNCES, t.bounces);
     warp_add(A.stats + ST_QUERIES, t.queries);
     warp_add(A.stats + ST_NODE_TESTS, ctr.node_tests);
@@ -408,7 +419,7 @@ __global__ void __launch_bounds__(128) k_trace(DScene S, TraceArgs A) {
             tally.hist[r.status]++;
         }
     }
-    flush_stats(A, ctr, tally);
+    flush_stats(A, ctr, tally, true);
 }
 
 // ---- wavefront form: advance rays until they need a Newton solve ----------
@@ -841,7 +852,7 @@ __global__ void __launch_bounds__(128) k_resume(DScene S, TraceArgs A, WaveArgs 
         tally.bounces += r.bounces;
         tally.hist[r.status]++;
     }
-    flush_stats(A, ctr, tally);
+    flush_stats(A, ctr, tally, true);
 }
 
 // ---- warp-per-ray form: 32 lanes cooperate on one ray ----------------------
@@ -1025,7 +1036,7 @@ __global__ void __launch_bounds__(128) k_resume_warp(DScene S, TraceArgs A, Wave
         ctr.tri_tests += c1.tri_tests;
         ctr.newton_iters += c1.newton_iters;
     }
-    flush_stats(A, ctr, tally);
+    flush_stats(A, ctr, tally, true);
 }
 
 // One query per ray: BVH, brute force over all objects, or one object.

@@ -198,6 +198,15 @@ typedef struct bbrt_trace_stats {
     long long status_hist[BBRT_RAY_STATUS_COUNT];
     double kernel_ms;         /* device time of the trace kernel(s), CUDA events */
     double total_ms;          /* device time of the whole call incl. copies */
+    /* Per-kernel breakdown (CUDA events around each launch): */
+    double order_ms;          /* ray ordering */
+    double advance_ms;        /* wavefront advance rounds */
+    double newton_ms;         /* wavefront Newton rounds */
+    double tail_ms;           /* rays finished one warp (or thread) per ray, incl. small batches */
+    long long rounds;         /* wavefront rounds */
+    long long tail_rays;      /* rays finished by the tail kernel */
+    long long tail_node_tests, tail_cell_tests, tail_tri_tests, tail_newton_iters;   /* the tail's share */
+    long long launches;       /* kernels this library launched for the call */
 } bbrt_trace_stats;
 
 /* ---- library ---------------------------------------------------------- */
