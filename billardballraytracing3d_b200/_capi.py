@@ -257,6 +257,8 @@ def _declare(lib):
     lib.bbrt_measure_pipe_peak.argtypes = [I, c_double_p]
     lib.bbrt_bounce_map.argtypes = [V, ctypes.POINTER(PatchDesc), I, I, I, I, D, I, c_int_p, c_int_p,
                                     c_int_p, ctypes.POINTER(TraceStats), V]
+    lib.bbrt_bounce_map_rays.argtypes = [V, ctypes.POINTER(PatchDesc), I, I, I, I, D, c_ll_p, LL,
+                                         c_double_p, c_double_p]
 
 
 def check(lib, rc, what="bbrt call"):

@@ -170,6 +170,26 @@ class Scene:
                 "bbrt_bounce_map")
         return mb, er, bd
 
+    def bounce_map_rays(self, sample_patches: Sequence, grid_n: int, theta_n: int, phi_n: int,
+                        cone_angle_deg: float = 180.0, ray_index=None):
+        """The launch rays bounce_map traces, as (origins[n,3], dirs[n,3]).
+
+        Ray r = ((p * grid_n**2 + k) * theta_n + ti) * phi_n + pj; ray_index
+        picks some (default: all, in that order)."""
+        t = C.ObjectTable(sample_patches)
+        if ray_index is None:
+            n = len(sample_patches) * grid_n * grid_n * theta_n * phi_n
+            idx_p = None
+        else:
+            idx = np.ascontiguousarray(ray_index, dtype=np.int64)
+            n = idx.size
+            idx_p = C.ptr(idx, ctypes.c_longlong)
+        o = np.zeros((n, 3)); d = np.zeros((n, 3))
+        C.check(self.lib, self.lib.bbrt_bounce_map_rays(self.h, t.pdescs, len(sample_patches), grid_n, theta_n, phi_n,
+                                                        float(cone_angle_deg), idx_p, n, C.ptr(o), C.ptr(d)),
+                "bbrt_bounce_map_rays")
+        return o, d
+
 
 def sample_grid(patch, n: int):
     """SurfacePatch::sample_grid(n) through the C ABI: (xyz, normal, dX/du)."""

@@ -822,22 +822,27 @@ BBRT_API int bbrt_patch_sample_grid(const bbrt_patch_desc* p, int n, double* xyz
     return BBRT_OK;
 }
 
-BBRT_API int bbrt_bounce_map(bbrt_scene_t s, const bbrt_patch_desc* samples, int n_sample, int grid_n, int theta_n,
-                             int phi_n, double cone_angle_deg, int max_bounces, int* max_out, int* err_out,
-                             int* best_out, bbrt_trace_stats* stats, void* stream) {
-    if (!s || !samples || !max_out || !err_out) return fail(BBRT_ERR_ARG, "bbrt_bounce_map: NULL argument");
+// BounceMapDriver::run's validation (BounceMapDriver.hpp:103-117).
+static int check_bounce_map_args(int grid_n, int theta_n, int phi_n, double cone_angle_deg) {
     if (grid_n < 2) return fail(BBRT_ERR_ARG, "BounceMapDriver::run: position_grid_n must be >= 2");
     if (theta_n < 1 || phi_n < 1) return fail(BBRT_ERR_ARG, "BounceMapDriver::run: theta_n and phi_n must both be >= 1");
     if (!(cone_angle_deg > 0.0) || cone_angle_deg > 180.0)
         return fail(BBRT_ERR_ARG, "BounceMapDriver::run: cone_angle_deg must be in (0, 180]");
-    if (n_sample < 1) return fail(BBRT_ERR_ARG, "bbrt_bounce_map: no sample patches");
-    // Ray generation on the host, in the reference's arithmetic
-    // (BounceMapDriver.hpp:119-237, build_tangent_frame :499-519).
+    return BBRT_OK;
+}
+
+// Bounce-map launch rays on the host, in the reference's arithmetic
+// (BounceMapDriver.hpp:119-237, build_tangent_frame :499-519).  Ray r is
+// ((p * grid_n^2 + k) * theta_n + ti) * phi_n + pj for sample patch p, grid
+// point k, polar index ti and azimuth index pj.  With idx == NULL all rays
+// are written in that order (n must be their count); otherwise ray idx[i]
+// goes to slot i.
+static void gen_bounce_rays(const bbrt_scene* s, const bbrt_patch_desc* samples, int n_sample, int grid_n, int theta_n,
+                            int phi_n, double cone_angle_deg, const long long* idx, long long n, double* org,
+                            double* dir) {
     const double kTwoPi = 6.283185307179586476925286766559;
     const double cos_max = std::cos(cone_angle_deg / 2.0 * kTwoPi / 360.0);
     const long long per = static_cast<long long>(grid_n) * grid_n, dirs_per = static_cast<long long>(theta_n) * phi_n;
-    const long long N = static_cast<long long>(n_sample) * per * dirs_per;
-    std::vector<double> org(3 * N), dir(3 * N);
     std::vector<double> cphi(phi_n), sphi(phi_n), mu(theta_n), sth(theta_n);
     for (int ti = 0; ti < theta_n; ++ti) {
         mu[ti] = cos_max + (static_cast<double>(ti) + 0.5) / static_cast<double>(theta_n) * (1.0 - cos_max);
@@ -848,55 +853,108 @@ BBRT_API int bbrt_bounce_map(bbrt_scene_t s, const bbrt_patch_desc* samples, int
         cphi[pj] = std::cos(phi);
         sphi[pj] = std::sin(phi);
     }
-    try {
-        for (int p = 0; p < n_sample; ++p) {
-            bbrt::HostScene one;
-            bbrt_object_desc od{};
-            od.kind = BBRT_OBJ_PATCH;
-            od.patch = &samples[p];
-            bbrt::build_host_scene(&od, 1, s->host.cfg, one);
-            const double a = s->host.cfg.self_intersect_eps_factor * s->host.scene_diagonal;
-            const double b = s->host.cfg.sagitta_clearance_factor * one.padding[0];
-            const double eps = (a < b) ? b : a;
-            std::vector<double> xyz(3 * per), nrm(3 * per), du(3 * per);
-            bbrt::sample_grid(samples[p], grid_n, xyz.data(), nrm.data(), du.data());
-            for (long long k = 0; k < per; ++k) {
-                const double* P = &xyz[3 * k];
-                double n0 = nrm[3 * k], n1 = nrm[3 * k + 1], n2 = nrm[3 * k + 2];
-                const double nl = std::sqrt(n0 * n0 + n1 * n1 + n2 * n2);
-                n0 /= nl; n1 /= nl; n2 /= nl;
-                const double d0 = du[3 * k], d1 = du[3 * k + 1], d2 = du[3 * k + 2];
-                const double du2 = d0 * d0 + d1 * d1 + d2 * d2, dn = d0 * n0 + d1 * n1 + d2 * n2;
-                const double q0 = d0 - dn * n0, q1 = d1 - dn * n1, q2 = d2 - dn * n2;
-                const double qq = q0 * q0 + q1 * q1 + q2 * q2;
-                double t1[3], t2[3];
-                if (qq > 1e-6 * 1e-6 * du2) {
-                    const double l = std::sqrt(q0 * q0 + q1 * q1 + q2 * q2);
-                    t1[0] = q0 / l; t1[1] = q1 / l; t1[2] = q2 / l;
-                } else {
-                    double ax[3] = { 0, 0, 0 };
-                    if (std::fabs(n0) <= std::fabs(n1) && std::fabs(n0) <= std::fabs(n2)) ax[0] = 1.0;
-                    else if (std::fabs(n1) <= std::fabs(n2)) ax[1] = 1.0;
-                    else ax[2] = 1.0;
-                    const double c0v = n1 * ax[2] - n2 * ax[1], c1v = n2 * ax[0] - n0 * ax[2], c2v = n0 * ax[1] - n1 * ax[0];
-                    const double l = std::sqrt(c0v * c0v + c1v * c1v + c2v * c2v);
-                    t1[0] = c0v / l; t1[1] = c1v / l; t1[2] = c2v / l;
-                }
-                t2[0] = n1 * t1[2] - n2 * t1[1];
-                t2[1] = n2 * t1[0] - n0 * t1[2];
-                t2[2] = n0 * t1[1] - n1 * t1[0];
-                const double o0 = P[0] + n0 * eps, o1 = P[1] + n1 * eps, o2 = P[2] + n2 * eps;
-                for (int ti = 0; ti < theta_n; ++ti)
-                    for (int pj = 0; pj < phi_n; ++pj) {
-                        const long long r = ((static_cast<long long>(p) * per + k) * dirs_per) + ti * phi_n + pj;
-                        org[3 * r] = o0; org[3 * r + 1] = o1; org[3 * r + 2] = o2;
-                        const double st_ = sth[ti], m = mu[ti], cp = cphi[pj], sp = sphi[pj];
-                        dir[3 * r] = t1[0] * st_ * cp + t2[0] * st_ * sp + n0 * m;
-                        dir[3 * r + 1] = t1[1] * st_ * cp + t2[1] * st_ * sp + n1 * m;
-                        dir[3 * r + 2] = t1[2] * st_ * cp + t2[2] * st_ * sp + n2 * m;
-                    }
+    // Per sample patch, built on first use: launch origin and frame
+    // (origin, t1, t2, n) of every grid point.
+    std::vector<std::vector<double>> frames(n_sample);
+    auto frame_of = [&](int p) -> const std::vector<double>& {
+        std::vector<double>& f = frames[p];
+        if (!f.empty()) return f;
+        bbrt::HostScene one;
+        bbrt_object_desc od{};
+        od.kind = BBRT_OBJ_PATCH;
+        od.patch = &samples[p];
+        bbrt::build_host_scene(&od, 1, s->host.cfg, one);
+        const double a = s->host.cfg.self_intersect_eps_factor * s->host.scene_diagonal;
+        const double b = s->host.cfg.sagitta_clearance_factor * one.padding[0];
+        const double eps = (a < b) ? b : a;
+        std::vector<double> xyz(3 * per), nrm(3 * per), du(3 * per);
+        bbrt::sample_grid(samples[p], grid_n, xyz.data(), nrm.data(), du.data());
+        f.resize(12 * per);
+        for (long long k = 0; k < per; ++k) {
+            const double* P = &xyz[3 * k];
+            double n0 = nrm[3 * k], n1 = nrm[3 * k + 1], n2 = nrm[3 * k + 2];
+            const double nl = std::sqrt(n0 * n0 + n1 * n1 + n2 * n2);
+            n0 /= nl; n1 /= nl; n2 /= nl;
+            const double d0 = du[3 * k], d1 = du[3 * k + 1], d2 = du[3 * k + 2];
+            const double du2 = d0 * d0 + d1 * d1 + d2 * d2, dn = d0 * n0 + d1 * n1 + d2 * n2;
+            const double q0 = d0 - dn * n0, q1 = d1 - dn * n1, q2 = d2 - dn * n2;
+            const double qq = q0 * q0 + q1 * q1 + q2 * q2;
+            double* F = &f[12 * k];
+            double* t1 = F + 3;
+            double* t2 = F + 6;
+            if (qq > 1e-6 * 1e-6 * du2) {
+                const double l = std::sqrt(q0 * q0 + q1 * q1 + q2 * q2);
+                t1[0] = q0 / l; t1[1] = q1 / l; t1[2] = q2 / l;
+            } else {
+                double ax[3] = { 0, 0, 0 };
+                if (std::fabs(n0) <= std::fabs(n1) && std::fabs(n0) <= std::fabs(n2)) ax[0] = 1.0;
+                else if (std::fabs(n1) <= std::fabs(n2)) ax[1] = 1.0;
+                else ax[2] = 1.0;
+                const double c0v = n1 * ax[2] - n2 * ax[1], c1v = n2 * ax[0] - n0 * ax[2], c2v = n0 * ax[1] - n1 * ax[0];
+                const double l = std::sqrt(c0v * c0v + c1v * c1v + c2v * c2v);
+                t1[0] = c0v / l; t1[1] = c1v / l; t1[2] = c2v / l;
             }
+            t2[0] = n1 * t1[2] - n2 * t1[1];
+            t2[1] = n2 * t1[0] - n0 * t1[2];
+            t2[2] = n0 * t1[1] - n1 * t1[0];
+            F[0] = P[0] + n0 * eps; F[1] = P[1] + n1 * eps; F[2] = P[2] + n2 * eps;
+            F[9] = n0; F[10] = n1; F[11] = n2;
         }
+        return f;
+    };
+    for (long long i = 0; i < n; ++i) {
+        const long long r = idx ? idx[i] : i;
+        const long long q = r / dirs_per, dk = r % dirs_per;
+        const int p = static_cast<int>(q / per);
+        const long long k = q % per;
+        const int ti = static_cast<int>(dk / phi_n), pj = static_cast<int>(dk % phi_n);
+        const double* F = &frame_of(p)[12 * k];
+        const double *t1 = F + 3, *t2 = F + 6;
+        const double n0 = F[9], n1 = F[10], n2 = F[11];
+        org[3 * i] = F[0]; org[3 * i + 1] = F[1]; org[3 * i + 2] = F[2];
+        const double st_ = sth[ti], m = mu[ti], cp = cphi[pj], sp = sphi[pj];
+        dir[3 * i] = t1[0] * st_ * cp + t2[0] * st_ * sp + n0 * m;
+        dir[3 * i + 1] = t1[1] * st_ * cp + t2[1] * st_ * sp + n1 * m;
+        dir[3 * i + 2] = t1[2] * st_ * cp + t2[2] * st_ * sp + n2 * m;
+    }
+}
+
+BBRT_API int bbrt_bounce_map_rays(bbrt_scene_t s, const bbrt_patch_desc* samples, int n_sample, int grid_n,
+                                  int theta_n, int phi_n, double cone_angle_deg, const long long* ray_index,
+                                  long long n, double* origins, double* dirs) {
+    if (!s || !samples || !origins || !dirs) return fail(BBRT_ERR_ARG, "bbrt_bounce_map_rays: NULL argument");
+    int rc = check_bounce_map_args(grid_n, theta_n, phi_n, cone_angle_deg);
+    if (rc) return rc;
+    if (n_sample < 1) return fail(BBRT_ERR_ARG, "bbrt_bounce_map_rays: no sample patches");
+    const long long total = static_cast<long long>(n_sample) * grid_n * grid_n * theta_n * phi_n;
+    if (n < 0 || (!ray_index && n != total))
+        return fail(BBRT_ERR_ARG, "bbrt_bounce_map_rays: n must be the ray count (" + std::to_string(total) +
+                                      ") when ray_index is NULL");
+    if (ray_index)
+        for (long long i = 0; i < n; ++i)
+            if (ray_index[i] < 0 || ray_index[i] >= total)
+                return fail(BBRT_ERR_ARG, "bbrt_bounce_map_rays: ray_index[" + std::to_string(i) + "] out of range");
+    try {
+        gen_bounce_rays(s, samples, n_sample, grid_n, theta_n, phi_n, cone_angle_deg, ray_index, n, origins, dirs);
+    } catch (const std::exception& e) {
+        return fail(BBRT_ERR_ARG, e.what());
+    }
+    return BBRT_OK;
+}
+
+BBRT_API int bbrt_bounce_map(bbrt_scene_t s, const bbrt_patch_desc* samples, int n_sample, int grid_n, int theta_n,
+                             int phi_n, double cone_angle_deg, int max_bounces, int* max_out, int* err_out,
+                             int* best_out, bbrt_trace_stats* stats, void* stream) {
+    if (!s || !samples || !max_out || !err_out) return fail(BBRT_ERR_ARG, "bbrt_bounce_map: NULL argument");
+    int rc0 = check_bounce_map_args(grid_n, theta_n, phi_n, cone_angle_deg);
+    if (rc0) return rc0;
+    if (n_sample < 1) return fail(BBRT_ERR_ARG, "bbrt_bounce_map: no sample patches");
+    const long long per = static_cast<long long>(grid_n) * grid_n, dirs_per = static_cast<long long>(theta_n) * phi_n;
+    const long long N = static_cast<long long>(n_sample) * per * dirs_per;
+    std::vector<double> org(3 * N), dir(3 * N);
+    try {
+        gen_bounce_rays(s, samples, n_sample, grid_n, theta_n, phi_n, cone_angle_deg, nullptr, N, org.data(),
+                        dir.data());
     } catch (const std::exception& e) {
         return fail(BBRT_ERR_ARG, e.what());
     }

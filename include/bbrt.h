@@ -297,6 +297,17 @@ BBRT_API int  bbrt_bounce_map(bbrt_scene_t scene, const bbrt_patch_desc* sample_
                               double cone_angle_deg, int max_bounces,
                               int* max_bounces_out, int* error_counts_out, int* best_dir_out,
                               bbrt_trace_stats* stats, void* stream);
+/* The launch rays bbrt_bounce_map traces (BounceMapDriver.hpp:119-237), for
+ * re-tracing chosen ones with their full paths (what run(...,
+ * capture_best_rays = true) keeps, :183-201).  Ray r is
+ * ((p * grid_n^2 + k) * theta_n + ti) * phi_n + pj: sample patch p, grid
+ * point k, direction index ti * phi_n + pj (best_dir_out's numbering).  With
+ * ray_index NULL, all rays in that order (n must be their count); otherwise
+ * ray ray_index[i] is written to origins[3i..], dirs[3i..] (host arrays). */
+BBRT_API int  bbrt_bounce_map_rays(bbrt_scene_t scene, const bbrt_patch_desc* sample_patches,
+                                   int n_sample, int grid_n, int theta_n, int phi_n,
+                                   double cone_angle_deg, const long long* ray_index, long long n,
+                                   double* origins, double* dirs);
 
 /* ---- diagnostics ------------------------------------------------------ */
 enum {

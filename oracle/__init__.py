@@ -96,6 +96,8 @@ class Oracle:
             L.oracle_sample_grid.argtypes = [ctypes.POINTER(C.PatchDesc), ctypes.c_int, V, V, V]
             L.oracle_bounce_map.argtypes = [V, ctypes.POINTER(C.PatchDesc), ctypes.c_int, ctypes.c_int,
                                             ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int, V, V, V]
+            L.oracle_bounce_map_rays.argtypes = [V, ctypes.POINTER(C.PatchDesc), ctypes.c_int, ctypes.c_int,
+                                                 ctypes.c_int, ctypes.c_int, ctypes.c_double, V, V]
             cls._lib = L
         return cls._lib
 
@@ -172,6 +174,15 @@ class Oracle:
         self.lib().oracle_bounce_map(self.h, t.pdescs, len(sample_patches), grid_n, theta_n, phi_n,
                                      cone_deg, max_bounces, P(mb), P(er), P(bd))
         return mb, er, bd
+
+    def bounce_map_rays(self, sample_patches, grid_n, theta_n, phi_n, cone_deg):
+        """Every launch ray of bounce_map, ray r at ((p*grid_n**2 + k)*theta_n + ti)*phi_n + pj."""
+        t = C.ObjectTable(sample_patches)
+        n = len(sample_patches) * grid_n * grid_n * theta_n * phi_n
+        o = np.zeros((n, 3)); d = np.zeros((n, 3))
+        self.lib().oracle_bounce_map_rays(self.h, t.pdescs, len(sample_patches), grid_n, theta_n, phi_n,
+                                          cone_deg, P(o), P(d))
+        return o, d
 
 
 class Reference:

@@ -808,60 +808,98 @@ int oracle_sample_grid(const bbrt_patch_desc* d, int n, double* xyz, double* nrm
 // BounceMapDriver::run, BounceMapDriver.hpp:103-259, for sample patches given
 // as descriptors (the reference loads them by file range).  eps per sample
 // patch is the scene's self_intersect_epsilon of that patch's own padding.
-int oracle_bounce_map(void* s, const bbrt_patch_desc* samples, int n_sample, int grid_n, int theta_n,
-                      int phi_n, double cone_deg, int max_bounces, int* max_b, int* errors, int* best_dir) {
-    auto* S = static_cast<Scene*>(s);
+}  // extern "C"
+
+// Every launch ray of one sample patch, in BounceMapDriver::run's order
+// (BounceMapDriver.hpp:119-237): fn(k, ti, pj, origin, dir) per grid point k
+// and direction (ti, pj).
+template <class Fn>
+static void bounce_rays_of_patch(const Scene& S, const bbrt_patch_desc& sample, int grid_n, int theta_n, int phi_n,
+                                 double cone_deg, Fn&& fn) {
     const double kTwoPi = 6.283185307179586476925286766559;
     const double half = cone_deg / 2.0;
     const double cos_max = std::cos(half * kTwoPi / 360.0);
     const long long per = static_cast<long long>(grid_n) * grid_n;
-    #pragma omp parallel for schedule(dynamic)
-    for (int p = 0; p < n_sample; ++p) {
-        Object P;
-        setup_patch(P, samples[p], S->cfg);
-        const double eps = std::max(S->cfg.eps_factor * S->diag, S->cfg.sag_factor * P.max_sag);
-        std::vector<double> xyz(3 * per), nrm(3 * per), du(3 * per);
-        oracle_sample_grid(&samples[p], grid_n, xyz.data(), nrm.data(), du.data());
-        for (long long k = 0; k < per; ++k) {
-            const V3 pt{ xyz[3 * k], xyz[3 * k + 1], xyz[3 * k + 2] };
-            const V3 nv = normalize({ nrm[3 * k], nrm[3 * k + 1], nrm[3 * k + 2] });
-            const V3 dv{ du[3 * k], du[3 * k + 1], du[3 * k + 2] };
-            // build_tangent_frame, BounceMapDriver.hpp:499-519
-            V3 t1, t2;
-            const double du2 = dot(dv, dv), dn = dot(dv, nv);
-            const V3 dp{ dv.x - dn * nv.x, dv.y - dn * nv.y, dv.z - dn * nv.z };
-            const double dp2 = dot(dp, dp);
-            const double rel = 1e-6;
-            if (dp2 > rel * rel * du2) t1 = normalize(dp);
-            else {
-                const V3 a = (std::fabs(nv.x) <= std::fabs(nv.y) && std::fabs(nv.x) <= std::fabs(nv.z)) ? V3{ 1, 0, 0 }
-                           : (std::fabs(nv.y) <= std::fabs(nv.z) ? V3{ 0, 1, 0 } : V3{ 0, 0, 1 });
-                t1 = normalize(cross(nv, a));
+    Object P;
+    setup_patch(P, sample, S.cfg);
+    const double eps = std::max(S.cfg.eps_factor * S.diag, S.cfg.sag_factor * P.max_sag);
+    std::vector<double> xyz(3 * per), nrm(3 * per), du(3 * per);
+    oracle_sample_grid(&sample, grid_n, xyz.data(), nrm.data(), du.data());
+    for (long long k = 0; k < per; ++k) {
+        const V3 pt{ xyz[3 * k], xyz[3 * k + 1], xyz[3 * k + 2] };
+        const V3 nv = normalize({ nrm[3 * k], nrm[3 * k + 1], nrm[3 * k + 2] });
+        const V3 dv{ du[3 * k], du[3 * k + 1], du[3 * k + 2] };
+        // build_tangent_frame, BounceMapDriver.hpp:499-519
+        V3 t1, t2;
+        const double du2 = dot(dv, dv), dn = dot(dv, nv);
+        const V3 dp{ dv.x - dn * nv.x, dv.y - dn * nv.y, dv.z - dn * nv.z };
+        const double dp2 = dot(dp, dp);
+        const double rel = 1e-6;
+        if (dp2 > rel * rel * du2) t1 = normalize(dp);
+        else {
+            const V3 a = (std::fabs(nv.x) <= std::fabs(nv.y) && std::fabs(nv.x) <= std::fabs(nv.z)) ? V3{ 1, 0, 0 }
+                       : (std::fabs(nv.y) <= std::fabs(nv.z) ? V3{ 0, 1, 0 } : V3{ 0, 0, 1 });
+            t1 = normalize(cross(nv, a));
+        }
+        t2 = cross(nv, t1);
+        const V3 org{ pt.x + nv.x * eps, pt.y + nv.y * eps, pt.z + nv.z * eps };
+        for (int ti = 0; ti < theta_n; ++ti) {
+            const double mu = cos_max + (static_cast<double>(ti) + 0.5) / static_cast<double>(theta_n) * (1.0 - cos_max);
+            const double st = std::sqrt(std::max(0.0, 1.0 - mu * mu));
+            for (int pj = 0; pj < phi_n; ++pj) {
+                const double phi = (static_cast<double>(pj) + 0.5) * kTwoPi / static_cast<double>(phi_n);
+                const double cp = std::cos(phi), sp = std::sin(phi);
+                const V3 dir{ t1.x * st * cp + t2.x * st * sp + nv.x * mu,
+                              t1.y * st * cp + t2.y * st * sp + nv.y * mu,
+                              t1.z * st * cp + t2.z * st * sp + nv.z * mu };
+                fn(k, ti, pj, org, dir);
             }
-            t2 = cross(nv, t1);
-            const V3 org{ pt.x + nv.x * eps, pt.y + nv.y * eps, pt.z + nv.z * eps };
-            int best = 0, nerr = 0, bdir = -1;
-            for (int ti = 0; ti < theta_n; ++ti) {
-                const double mu = cos_max + (static_cast<double>(ti) + 0.5) / static_cast<double>(theta_n) * (1.0 - cos_max);
-                const double st = std::sqrt(std::max(0.0, 1.0 - mu * mu));
-                for (int pj = 0; pj < phi_n; ++pj) {
-                    const double phi = (static_cast<double>(pj) + 0.5) * kTwoPi / static_cast<double>(phi_n);
-                    const double cp = std::cos(phi), sp = std::sin(phi);
-                    const V3 dir{ t1.x * st * cp + t2.x * st * sp + nv.x * mu,
-                                  t1.y * st * cp + t2.y * st * sp + nv.y * mu,
-                                  t1.z * st * cp + t2.z * st * sp + nv.z * mu };
-                    const TraceOut r = trace_ray(*S, org, dir, max_bounces, nullptr,
-                                                 [](int, int, const V3&, double, double) {});
-                    if (r.status != BBRT_RAY_ESCAPED && r.status != BBRT_RAY_MAX_BOUNCES) { ++nerr; continue; }
-                    if (bdir < 0 || r.bounces > best) bdir = ti * phi_n + pj;   // first maximum, :232-235
-                    best = std::max(best, r.bounces);
-                }
-            }
-            max_b[p * per + k] = best;
-            errors[p * per + k] = nerr;
-            if (best_dir) best_dir[p * per + k] = bdir;
         }
     }
+}
+
+extern "C" {
+
+int oracle_bounce_map(void* s, const bbrt_patch_desc* samples, int n_sample, int grid_n, int theta_n,
+                      int phi_n, double cone_deg, int max_bounces, int* max_b, int* errors, int* best_dir) {
+    auto* S = static_cast<Scene*>(s);
+    const long long per = static_cast<long long>(grid_n) * grid_n;
+    #pragma omp parallel for schedule(dynamic)
+    for (int p = 0; p < n_sample; ++p) {
+        int best = 0, nerr = 0, bdir = -1;
+        bounce_rays_of_patch(*S, samples[p], grid_n, theta_n, phi_n, cone_deg,
+                             [&](long long k, int ti, int pj, const V3& org, const V3& dir) {
+            if (ti == 0 && pj == 0) { best = 0; nerr = 0; bdir = -1; }
+            const TraceOut r = trace_ray(*S, org, dir, max_bounces, nullptr,
+                                         [](int, int, const V3&, double, double) {});
+            if (r.status != BBRT_RAY_ESCAPED && r.status != BBRT_RAY_MAX_BOUNCES) ++nerr;
+            else {
+                if (bdir < 0 || r.bounces > best) bdir = ti * phi_n + pj;   // first maximum, :232-235
+                best = std::max(best, r.bounces);
+            }
+            if (ti == theta_n - 1 && pj == phi_n - 1) {
+                max_b[p * per + k] = best;
+                errors[p * per + k] = nerr;
+                if (best_dir) best_dir[p * per + k] = bdir;
+            }
+        });
+    }
+    return 0;
+}
+
+// The launch rays of oracle_bounce_map, all of them, ray r at
+// ((p * grid_n^2 + k) * theta_n + ti) * phi_n + pj.
+int oracle_bounce_map_rays(void* s, const bbrt_patch_desc* samples, int n_sample, int grid_n, int theta_n,
+                           int phi_n, double cone_deg, double* origins, double* dirs) {
+    auto* S = static_cast<Scene*>(s);
+    const long long per = static_cast<long long>(grid_n) * grid_n;
+    for (int p = 0; p < n_sample; ++p)
+        bounce_rays_of_patch(*S, samples[p], grid_n, theta_n, phi_n, cone_deg,
+                             [&](long long k, int ti, int pj, const V3& org, const V3& dir) {
+            const long long r = ((p * per + k) * theta_n + ti) * phi_n + pj;
+            origins[3 * r] = org.x; origins[3 * r + 1] = org.y; origins[3 * r + 2] = org.z;
+            dirs[3 * r] = dir.x; dirs[3 * r + 1] = dir.y; dirs[3 * r + 2] = dir.z;
+        });
     return 0;
 }
 

@@ -150,3 +150,24 @@ def test_no_cpu_fallback_without_gpu(built, workloads):
         sc.trace(o, d, maxb)
     with pytest.raises(RuntimeError, match="no CUDA device"):
         sc.intersect(o, d)
+
+
+def test_bounce_map_rays_equal_oracle(built):
+    """bbrt_bounce_map_rays is host code: the launch rays of
+    BounceMapDriver::run (BounceMapDriver.hpp:119-237), bit for bit."""
+    patches = scenes.scene_two_spheres()
+    cfg = C.default_config(coarse_grid_n=9, newton_tol=1e-12)
+    sc = api.Scene(patches, config=cfg)
+    orc = oracle.Oracle(patches, config=cfg)
+    samples = patches[3:6]
+    for grid, theta, phi, cone in ((3, 2, 5, 180.0), (4, 3, 4, 37.5)):
+        o, d = sc.bounce_map_rays(samples, grid, theta, phi, cone)
+        ro, rd = orc.bounce_map_rays(samples, grid, theta, phi, cone)
+        assert np.array_equal(o, ro) and np.array_equal(d, rd)
+        pick = np.array([o.shape[0] - 1, 0, 17, 5, 17])
+        so, sd = sc.bounce_map_rays(samples, grid, theta, phi, cone, ray_index=pick)
+        assert np.array_equal(so, ro[pick]) and np.array_equal(sd, rd[pick])
+    with pytest.raises(RuntimeError, match="out of range"):
+        sc.bounce_map_rays(samples, 3, 2, 5, 180.0, ray_index=[3 * 9 * 10])
+    with pytest.raises(RuntimeError, match="position_grid_n must be >= 2"):
+        sc.bounce_map_rays(samples, 1, 2, 5, 180.0)
