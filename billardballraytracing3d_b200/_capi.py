@@ -255,6 +255,8 @@ def _declare(lib):
                                       ctypes.POINTER(TraceStats), V]
     lib.bbrt_patch_sample_grid.argtypes = [ctypes.POINTER(PatchDesc), I, c_double_p, c_double_p, c_double_p]
     lib.bbrt_measure_pipe_peak.argtypes = [I, c_double_p]
+    lib.bbrt_umma_check.argtypes = [ctypes.POINTER(ctypes.c_ushort), ctypes.POINTER(ctypes.c_ushort),
+                                    ctypes.POINTER(ctypes.c_float)]
     lib.bbrt_bounce_map.argtypes = [V, ctypes.POINTER(PatchDesc), I, I, I, I, D, I, c_int_p, c_int_p,
                                     c_int_p, ctypes.POINTER(TraceStats), V]
     lib.bbrt_bounce_map_rays.argtypes = [V, ctypes.POINTER(PatchDesc), I, I, I, I, D, c_ll_p, LL,

@@ -45,6 +45,7 @@ cudaError_t ray_order(const double* o, const double* d, long long n, const doubl
 cudaError_t launch_query(const DScene& S, const QueryArgs& Q, cudaStream_t stream);
 cudaError_t launch_trace_noalloc(const DScene& S, TraceArgs A, bool count_hits, long long* hit_counts_out,
                                  long long* host_stats, cudaStream_t stream, int sm_count);
+int launch_umma_check(const uint16_t* A, const uint16_t* B, float* D, int* err, cudaStream_t st);
 }  // namespace bbrt
 
 namespace {
@@ -1038,3 +1039,37 @@ BBRT_API int bbrt_trace_noalloc(bbrt_scene_t s, const double* origins, const dou
 }
 
 }  // extern "C"
+
+// Tensor-core layout self-check (diagnostic): four staged forms of one product.
+BBRT_API int bbrt_umma_check(const uint16_t* a, const uint16_t* b, float* d) {
+    if (!a || !b || !d) return fail(BBRT_ERR_ARG, "bbrt_umma_check: NULL argument");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0)
+        return fail(BBRT_ERR_CUDA, "bbrt: no CUDA device available (the trace path has no CPU fallback)");
+    uint16_t *da = nullptr, *db = nullptr;
+    float* dd = nullptr;
+    int* de = nullptr;
+    const size_t nab = 128 * 64 * sizeof(uint16_t), nd = 4 * 128 * 128 * sizeof(float);
+    auto cleanup = [&]() { cudaFree(da); cudaFree(db); cudaFree(dd); cudaFree(de); };
+    if (cudaMalloc(&da, nab) != cudaSuccess || cudaMalloc(&db, nab) != cudaSuccess ||
+        cudaMalloc(&dd, nd) != cudaSuccess || cudaMalloc(&de, sizeof(int)) != cudaSuccess) {
+        cleanup();
+        return fail(BBRT_ERR_CUDA, "bbrt_umma_check: cudaMalloc failed");
+    }
+    int herr = 0;
+    cudaMemcpy(da, a, nab, cudaMemcpyHostToDevice);
+    cudaMemcpy(db, b, nab, cudaMemcpyHostToDevice);
+    cudaMemset(dd, 0, nd);
+    cudaMemset(de, 0, sizeof(int));
+    const int rc = bbrt::launch_umma_check(da, db, dd, de, nullptr);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (rc == 0 && e == cudaSuccess) {
+        cudaMemcpy(d, dd, nd, cudaMemcpyDeviceToHost);
+        cudaMemcpy(&herr, de, sizeof(int), cudaMemcpyDeviceToHost);
+    }
+    cleanup();
+    if (rc != 0 || e != cudaSuccess)
+        return fail(BBRT_ERR_CUDA, std::string("bbrt_umma_check: ") + cudaGetErrorString(rc ? cudaError_t(rc) : e));
+    if (herr) return fail(BBRT_ERR_KERNEL, "bbrt_umma_check: an MMA completion wait timed out");
+    return BBRT_OK;
+}

@@ -320,6 +320,14 @@ enum {
  * the trace kernel's pipes). */
 BBRT_API int bbrt_measure_pipe_peak(int pipe, double* value);
 
+/* Tensor-core layout self-check (no reference counterpart): a (128 x 64) and
+ * b (128 x 64), BF16 bit patterns, row-major with the 64-long dimension
+ * contiguous; d receives 4 x 128 x 128 floats, a * b^T computed by tcgen05 MMAs
+ * with the operands staged K-major / MN-major in the four combinations (the
+ * layouts the learned-guess kernels use).  BBRT_ERR_KERNEL when an MMA
+ * completion wait timed out. */
+BBRT_API int bbrt_umma_check(const unsigned short* a, const unsigned short* b, float* d);
+
 /* ---- allocation-free trace ------------------------------------------------
  * No counterpart in the reference (it has no device memory at all).
  *
