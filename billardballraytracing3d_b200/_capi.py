@@ -15,6 +15,7 @@ import numpy as np
 c_double_p = ctypes.POINTER(ctypes.c_double)
 c_int_p = ctypes.POINTER(ctypes.c_int)
 c_ll_p = ctypes.POINTER(ctypes.c_longlong)
+c_float_p = ctypes.POINTER(ctypes.c_float)
 
 # return codes
 BBRT_OK = 0
@@ -164,12 +165,32 @@ class TraceStats(ctypes.Structure):
         ("tail_node_tests", ctypes.c_longlong), ("tail_cell_tests", ctypes.c_longlong),
         ("tail_tri_tests", ctypes.c_longlong), ("tail_newton_iters", ctypes.c_longlong),
         ("launches", ctypes.c_longlong),
+        ("guess_used", ctypes.c_longlong), ("guess_fallback", ctypes.c_longlong), ("guess_ms", ctypes.c_double),
     ]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k != "status_hist"}
         d["status_hist"] = list(self.status_hist)
         return d
+
+
+class GuessTrainConfig(ctypes.Structure):
+    _fields_ = [
+        ("epochs", ctypes.c_int), ("batch", ctypes.c_int), ("lr", ctypes.c_float),
+        ("max_positive", ctypes.c_longlong), ("max_negative", ctypes.c_longlong),
+        ("seed", ctypes.c_ulonglong), ("min_logit", ctypes.c_double), ("t_window", ctypes.c_double),
+    ]
+
+
+class GuessTrainReport(ctypes.Structure):
+    _fields_ = [
+        ("positives", ctypes.c_longlong), ("negatives", ctypes.c_longlong), ("steps", ctypes.c_longlong),
+        ("first_loss", ctypes.c_double), ("last_loss", ctypes.c_double),
+        ("collect_ms", ctypes.c_double), ("train_ms", ctypes.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 def ptr(a, ctype=ctypes.c_double):
@@ -257,6 +278,17 @@ def _declare(lib):
     lib.bbrt_measure_pipe_peak.argtypes = [I, c_double_p]
     lib.bbrt_umma_check.argtypes = [ctypes.POINTER(ctypes.c_ushort), ctypes.POINTER(ctypes.c_ushort),
                                     ctypes.POINTER(ctypes.c_float)]
+    lib.bbrt_scene_set_modes.argtypes = [V, I, I]
+    lib.bbrt_guess_train_config_init.argtypes = [ctypes.POINTER(GuessTrainConfig)]
+    lib.bbrt_guess_train_config_init.restype = None
+    lib.bbrt_guess_train.argtypes = [V, c_double_p, c_double_p, LL, I, ctypes.POINTER(GuessTrainConfig),
+                                     ctypes.POINTER(GuessTrainReport), V]
+    lib.bbrt_guess_param_count.argtypes = [V]
+    lib.bbrt_guess_param_count.restype = LL
+    lib.bbrt_guess_params.argtypes = [V, c_float_p, LL, I]
+    lib.bbrt_mlp_check.argtypes = [c_float_p, I, c_float_p, c_int_p, c_float_p, c_float_p, I, c_float_p,
+                                   c_float_p, c_float_p]
+    lib.bbrt_mlp_infer_check.argtypes = [c_float_p, I, c_float_p, c_int_p, I, c_double_p]
     lib.bbrt_bounce_map.argtypes = [V, ctypes.POINTER(PatchDesc), I, I, I, I, D, I, c_int_p, c_int_p,
                                     c_int_p, ctypes.POINTER(TraceStats), V]
     lib.bbrt_bounce_map_rays.argtypes = [V, ctypes.POINTER(PatchDesc), I, I, I, I, D, c_ll_p, LL,

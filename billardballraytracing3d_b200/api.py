@@ -170,6 +170,37 @@ class Scene:
                 "bbrt_bounce_map")
         return mb, er, bd
 
+    def set_modes(self, precision: int = C.PREC_FP64, guess: int = C.GUESS_TRIANGLE):
+        """Arithmetic mode (PREC_FP64 / PREC_SPLIT) and Newton start (GUESS_TRIANGLE / GUESS_LEARNED)."""
+        C.check(self.lib, self.lib.bbrt_scene_set_modes(self.h, int(precision), int(guess)), "bbrt_scene_set_modes")
+
+    def guess_train(self, origins, dirs, max_bounces: int, **kw) -> Dict:
+        """Records training samples from a plain trace of these rays and trains
+        the learned-guess network on the GPU; returns the training report."""
+        cfg = C.GuessTrainConfig()
+        self.lib.bbrt_guess_train_config_init(ctypes.byref(cfg))
+        for k, v in kw.items():
+            if not hasattr(cfg, k):
+                raise KeyError(k)
+            setattr(cfg, k, v)
+        o = np.ascontiguousarray(origins, dtype=np.float64)
+        d = np.ascontiguousarray(dirs, dtype=np.float64)
+        rep = C.GuessTrainReport()
+        C.check(self.lib, self.lib.bbrt_guess_train(self.h, C.ptr(o), C.ptr(d), o.shape[0], int(max_bounces),
+                                                    ctypes.byref(cfg), ctypes.byref(rep), None), "bbrt_guess_train")
+        return rep.as_dict()
+
+    def guess_params(self, params=None):
+        """Gets (params=None) or sets the network's FP32 parameters."""
+        n = self.lib.bbrt_guess_param_count(self.h)
+        if params is None:
+            out = np.zeros(n, np.float32)
+            C.check(self.lib, self.lib.bbrt_guess_params(self.h, C.ptr(out, ctypes.c_float), n, 0), "bbrt_guess_params")
+            return out
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        C.check(self.lib, self.lib.bbrt_guess_params(self.h, C.ptr(p, ctypes.c_float), n, 1), "bbrt_guess_params")
+        return p
+
     def bounce_map_rays(self, sample_patches: Sequence, grid_n: int, theta_n: int, phi_n: int,
                         cone_angle_deg: float = 180.0, ray_index=None):
         """The launch rays bounce_map traces, as (origins[n,3], dirs[n,3]).

@@ -18,6 +18,8 @@
 #include <filesystem>
 #include <memory>
 #include <mutex>
+#include <numeric>
+#include <random>
 #include <stdexcept>
 #include <string>
 #include <type_traits>
@@ -25,6 +27,7 @@
 
 #include "../../include/bbrt.h"
 #include "dscene.h"
+#include "guess.h"
 #include "scene_host.hpp"
 
 namespace bbrt {
@@ -109,10 +112,26 @@ struct bbrt_scene {
     std::vector<std::pair<int, int>> kspans;   // (kernel kind, first event)
     std::mutex mu;
 
+    // Learned Newton guess: network (FP32 master, BF16 image, Adam moments),
+    // per-patch frames, per-request outputs of the current round.
+    struct Guess {
+        DevBuf P, G, m1, m2, image, loss, err, out, rows;
+        const double* frame = nullptr;     // [n_patches][kFrame] (scene allocation)
+        bool trained = false;
+        long long steps = 0;
+        double min_logit = 0.0, t_window = 0.5;
+    } guess;
+    // Training-sample recording, set only inside bbrt_guess_train.
+    bbrt::GuessSample* rec_samples = nullptr;
+    unsigned long long* rec_count = nullptr;
+    long long rec_cap_pos = 0, rec_cap_neg = 0;
+
     ~bbrt_scene() {
         for (void* p : allocs) cudaFree(p);
         for (DevBuf* b : { &stats, &work, &in_o, &in_d, &o_status, &o_bounce, &o_dir, &o_end, &o_hobj, &o_hpt,
-                           &o_huv, &o_eobj, &o_eval, &counts, &hits, &wave, &wave_ctr, &o_work, &order, &order_ws })
+                           &o_huv, &o_eobj, &o_eval, &counts, &hits, &wave, &wave_ctr, &o_work, &order, &order_ws,
+                           &guess.P, &guess.G, &guess.m1, &guess.m2, &guess.image, &guess.loss, &guess.err,
+                           &guess.out, &guess.rows })
             b->release();
         if (wave_ctr_host) cudaFreeHost(wave_ctr_host);
         for (auto& e : ev)
@@ -136,6 +155,54 @@ struct bbrt_scene {
 };
 
 namespace {
+
+// Per-patch frame of the learned guess (16 doubles, see guess.h): node mean,
+// mean dX/du made orthogonal to the mean normal, the normal, their cross
+// product, half the box diagonal and the box half-extents over it.
+std::vector<double> patch_frames(const bbrt::HostScene& H) {
+    std::vector<double> fr(static_cast<size_t>(H.n_patches) * bbrt::kFrame, 0.0);
+    for (int obj = 0; obj < H.n_objects; ++obj) {
+        if (H.kind[obj] != BBRT_OBJ_PATCH) continue;
+        const int q = H.sub[obj];
+        const int nn = H.p_imax[q] * H.p_jmax[q];
+        const double* F = H.p_fields.data() + H.p_field_off[q];
+        double c[3] = { 0, 0, 0 }, tu[3] = { 0, 0, 0 }, nv[3] = { 0, 0, 0 };
+        for (int k = 0; k < nn; ++k)
+            for (int a = 0; a < 3; ++a) {
+                c[a] += F[k * bbrt::kFields + a];
+                tu[a] += F[k * bbrt::kFields + 3 + a];
+                nv[a] += F[k * bbrt::kFields + 9 + a];
+            }
+        double ln = std::sqrt(nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2]);
+        if (!(ln > 0.0)) { nv[0] = 0; nv[1] = 0; nv[2] = 1; ln = 1.0; }
+        for (int a = 0; a < 3; ++a) { c[a] /= nn; nv[a] /= ln; }
+        const double dn = tu[0] * nv[0] + tu[1] * nv[1] + tu[2] * nv[2];
+        for (int a = 0; a < 3; ++a) tu[a] -= dn * nv[a];
+        double lt = std::sqrt(tu[0] * tu[0] + tu[1] * tu[1] + tu[2] * tu[2]);
+        if (!(lt > 1e-300)) {
+            const double ax[3] = { std::fabs(nv[0]) < 0.9 ? 1.0 : 0.0, std::fabs(nv[0]) < 0.9 ? 0.0 : 1.0, 0.0 };
+            const double p = ax[0] * nv[0] + ax[1] * nv[1];
+            for (int a = 0; a < 3; ++a) tu[a] = ax[a] - p * nv[a];
+            lt = std::sqrt(tu[0] * tu[0] + tu[1] * tu[1] + tu[2] * tu[2]);
+        }
+        for (int a = 0; a < 3; ++a) tu[a] /= lt;
+        const double t2[3] = { nv[1] * tu[2] - nv[2] * tu[1], nv[2] * tu[0] - nv[0] * tu[2], nv[0] * tu[1] - nv[1] * tu[0] };
+        const double* b = H.box.data() + 6 * static_cast<size_t>(obj);
+        const double ex[3] = { 0.5 * (b[3] - b[0]), 0.5 * (b[4] - b[1]), 0.5 * (b[5] - b[2]) };
+        double L = std::sqrt(ex[0] * ex[0] + ex[1] * ex[1] + ex[2] * ex[2]);
+        if (!(L > 0.0)) L = 1.0;
+        double* f = fr.data() + static_cast<size_t>(q) * bbrt::kFrame;
+        for (int a = 0; a < 3; ++a) {
+            f[a] = c[a];
+            f[3 + a] = tu[a];
+            f[6 + a] = t2[a];
+            f[9 + a] = nv[a];
+            f[13 + a] = ex[a] / L;
+        }
+        f[12] = L;
+    }
+    return fr;
+}
 
 int ensure_uploaded(bbrt_scene* s) {
     if (s->uploaded) return BBRT_OK;
@@ -208,6 +275,15 @@ int ensure_uploaded(bbrt_scene* s) {
     if ((rc = s->upload(H.p_field_off, D.p_field_off))) return rc;
     if ((rc = s->upload(H.p_nodes, D.p_nodes))) return rc;
     if ((rc = s->upload(H.p_fields, D.p_fields))) return rc;
+    {
+        const std::vector<float> n32(H.p_nodes.begin(), H.p_nodes.end());
+        const std::vector<float> f32(H.p_fields.begin(), H.p_fields.end());
+        if ((rc = s->upload(n32, D.p_nodes32))) return rc;
+        if ((rc = s->upload(f32, D.p_fields32))) return rc;
+        const std::vector<double> fr = patch_frames(H);
+        if ((rc = s->upload(fr, s->guess.frame))) return rc;
+    }
+    D.precision = H.cfg.precision;
     if ((rc = s->upload(H.coarse_uv, D.coarse_uv))) return rc;
     if ((rc = s->upload(H.c_xyz, D.c_xyz))) return rc;
     if ((rc = s->upload(H.c_cell, D.c_cell))) return rc;
@@ -296,7 +372,9 @@ void fill_stats(bbrt_scene* s, const long long* st, long long n, float kernel_ms
     out->tail_tri_tests = st[bbrt::ST_TAIL_TRI_TESTS];
     out->tail_newton_iters = st[bbrt::ST_TAIL_NEWTON_ITERS];
     out->tail_rays = st[bbrt::ST_TAIL_RAYS];
-    double* dst[4] = { &out->order_ms, &out->advance_ms, &out->newton_ms, &out->tail_ms };
+    out->guess_used = st[bbrt::ST_GUESS_USED];
+    out->guess_fallback = st[bbrt::ST_GUESS_FALLBACK];
+    double* dst[5] = { &out->order_ms, &out->advance_ms, &out->newton_ms, &out->tail_ms, &out->guess_ms };
     for (const auto& sp : s->kspans) {
         float ms = 0.0f;
         if (cudaEventElapsedTime(&ms, s->kev[sp.second], s->kev[sp.second + 1]) == cudaSuccess) *dst[sp.first] += ms;
@@ -305,7 +383,7 @@ void fill_stats(bbrt_scene* s, const long long* st, long long n, float kernel_ms
     out->launches = s->launches;
 }
 
-enum { K_ORDER = 0, K_ADVANCE = 1, K_NEWTON = 2, K_TAIL = 3 };
+enum { K_ORDER = 0, K_ADVANCE = 1, K_NEWTON = 2, K_TAIL = 3, K_GUESS = 4 };
 
 // Records a pair of events around one launch when the call collects statistics.
 template <class F>
@@ -349,6 +427,18 @@ const Tuning& tuning() {
         return v;
     }();
     return t;
+}
+
+// Device view of a scene's network (parameters must be allocated).
+bbrt::MlpNet guess_net(bbrt_scene* s) {
+    bbrt::MlpNet M;
+    M.image = static_cast<const uint8_t*>(s->guess.image.p);
+    M.P = static_cast<float*>(s->guess.P.p);
+    M.G = static_cast<float*>(s->guess.G.p);
+    M.loss = static_cast<float*>(s->guess.loss.p);
+    M.out = nullptr;
+    M.err = static_cast<int*>(s->guess.err.p);
+    return M;
 }
 
 // The wavefront trace: k_advance moves every runnable ray until its query
@@ -414,6 +504,19 @@ int run_wavefront(bbrt_scene* s, const bbrt::TraceArgs& A, cudaStream_t st) {
             break;
         }
         if (T.log_rounds) BBRT_CUDA(cudaEventRecord(s->ev[2], st));
+        W.guess = nullptr;
+        if (s->host.cfg.guess == BBRT_GUESS_LEARNED && s->guess.trained) {
+            BBRT_CUDA(s->guess.out.ensure(sizeof(double) * 4 * static_cast<size_t>(n_req)));
+            const bbrt::MlpNet net = guess_net(s);
+            BBRT_CUDA(timed(s, K_GUESS, st, [&] {
+                return bbrt::mlp_infer_requests(W.req, n_req, W.o, W.d, s->dev.obj_sub, s->guess.frame, net,
+                                                static_cast<double*>(s->guess.out.p), st);
+            }));
+            W.guess = static_cast<const double*>(s->guess.out.p);
+            W.frame = s->guess.frame;
+            W.guess_min_logit = s->guess.min_logit;
+            W.guess_t_window = s->guess.t_window;
+        }
         BBRT_CUDA(timed(s, K_NEWTON, st, [&] { return bbrt::launch_newton(s->dev, A, W, n_req, st); }));
         if (T.log_rounds) {
             BBRT_CUDA(cudaEventRecord(s->ev[3], st));
@@ -461,6 +564,10 @@ int run_trace_device(bbrt_scene* s, const double* d_o, const double* d_d, long l
     A.count_from = count_from;
     A.stats = want_stats ? static_cast<long long*>(s->stats.p) : nullptr;
     A.work_counter = static_cast<unsigned long long*>(s->work.p);
+    A.samples = s->rec_samples;
+    A.sample_count = s->rec_count;
+    A.sample_cap_pos = s->rec_cap_pos;
+    A.sample_cap_neg = s->rec_cap_neg;
     if (want_stats) BBRT_CUDA(cudaMemsetAsync(s->stats.p, 0, sizeof(long long) * bbrt::ST_COUNT, st));
     BBRT_CUDA(cudaMemsetAsync(s->work.p, 0, sizeof(unsigned long long), st));
     s->timing = want_stats;
@@ -1071,5 +1178,360 @@ BBRT_API int bbrt_umma_check(const uint16_t* a, const uint16_t* b, float* d) {
     if (rc != 0 || e != cudaSuccess)
         return fail(BBRT_ERR_CUDA, std::string("bbrt_umma_check: ") + cudaGetErrorString(rc ? cudaError_t(rc) : e));
     if (herr) return fail(BBRT_ERR_KERNEL, "bbrt_umma_check: an MMA completion wait timed out");
+    return BBRT_OK;
+}
+
+// ---- arithmetic modes and the learned guess --------------------------------
+
+BBRT_API int bbrt_scene_set_modes(bbrt_scene_t s, int precision, int guess) {
+    if (!s) return fail(BBRT_ERR_ARG, "bbrt_scene_set_modes: NULL scene");
+    if (precision != BBRT_PREC_FP64 && precision != BBRT_PREC_SPLIT)
+        return fail(BBRT_ERR_ARG, "bbrt_scene_set_modes: unknown precision");
+    if (guess != BBRT_GUESS_TRIANGLE && guess != BBRT_GUESS_LEARNED)
+        return fail(BBRT_ERR_ARG, "bbrt_scene_set_modes: unknown guess");
+    std::lock_guard<std::mutex> g(s->mu);
+    s->host.cfg.precision = precision;
+    s->host.cfg.guess = guess;
+    s->dev.precision = precision;
+    return BBRT_OK;
+}
+
+BBRT_API void bbrt_guess_train_config_init(bbrt_guess_train_config* c) {
+    if (!c) return;
+    c->epochs = 8;
+    c->batch = 65536;
+    c->lr = 1e-3f;
+    c->max_positive = 4LL << 20;
+    c->max_negative = 1LL << 20;
+    c->seed = 1;
+    c->min_logit = 0.0;
+    c->t_window = 0.5;
+}
+
+BBRT_API long long bbrt_guess_param_count(bbrt_scene_t s) {
+    if (!s) return 0;
+    return bbrt::oE + static_cast<long long>(bbrt::kEmb) * s->host.n_patches;
+}
+
+namespace {
+
+// Scaled-uniform weights, zero biases, N(0, 0.1) embeddings; the padded
+// inputs (>= 41) and outputs (>= 4) start, and stay, at zero.
+std::vector<float> init_network(long long n_params, unsigned long long seed) {
+    std::vector<float> P(static_cast<size_t>(n_params), 0.0f);
+    std::mt19937_64 rng(seed);
+    auto fill = [&](int off, int rows, int cols, int used_rows, int used_cols, int fan_in) {
+        const double lim = std::sqrt(6.0 / (fan_in + rows));
+        std::uniform_real_distribution<double> U(-lim, lim);
+        for (int o = 0; o < rows; ++o)
+            for (int i = 0; i < cols; ++i)
+                P[off + o * cols + i] = (o < used_rows && i < used_cols) ? static_cast<float>(U(rng)) : 0.0f;
+    };
+    fill(bbrt::oW0, bbrt::kH, bbrt::kIn, bbrt::kH, bbrt::kGeo + bbrt::kEmb, bbrt::kGeo + bbrt::kEmb);
+    fill(bbrt::oW1, bbrt::kH, bbrt::kH, bbrt::kH, bbrt::kH, bbrt::kH);
+    fill(bbrt::oW2, bbrt::kH, bbrt::kH, bbrt::kH, bbrt::kH, bbrt::kH);
+    fill(bbrt::oW3, bbrt::kOut, bbrt::kH, 4, bbrt::kH, bbrt::kH);
+    std::normal_distribution<double> N(0.0, 0.1);
+    for (long long k = bbrt::oE; k < n_params; ++k) P[k] = static_cast<float>(N(rng));
+    return P;
+}
+
+// Allocates the network buffers of a scene for n_params parameters.
+int guess_alloc(bbrt_scene* s, long long n_params) {
+    const size_t fb = sizeof(float) * static_cast<size_t>(n_params);
+    BBRT_CUDA(s->guess.P.ensure(fb));
+    BBRT_CUDA(s->guess.G.ensure(fb));
+    BBRT_CUDA(s->guess.m1.ensure(fb));
+    BBRT_CUDA(s->guess.m2.ensure(fb));
+    BBRT_CUDA(s->guess.image.ensure(bbrt::kImageBytes));
+    BBRT_CUDA(s->guess.err.ensure(sizeof(int)));
+    return BBRT_OK;
+}
+
+int guess_err_check(bbrt_scene* s, cudaStream_t st) {
+    int e = 0;
+    BBRT_CUDA(cudaMemcpyAsync(&e, s->guess.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    BBRT_CUDA(cudaStreamSynchronize(st));
+    if (e) return fail(BBRT_ERR_KERNEL, "bbrt_guess: a tensor-core completion wait timed out");
+    return BBRT_OK;
+}
+
+}  // namespace
+
+BBRT_API int bbrt_guess_params(bbrt_scene_t s, float* params, long long n, int set) {
+    if (!s || !params) return fail(BBRT_ERR_ARG, "bbrt_guess_params: NULL argument");
+    const long long np = bbrt_guess_param_count(s);
+    if (n != np) return fail(BBRT_ERR_ARG, "bbrt_guess_params: n must be " + std::to_string(np));
+    std::lock_guard<std::mutex> g(s->mu);
+    int rc = ensure_uploaded(s);
+    if (rc) return rc;
+    cudaStream_t st = s->stream;
+    if (!set) {
+        if (!s->guess.trained) return fail(BBRT_ERR_STATE, "bbrt_guess_params: the scene has no trained network");
+        BBRT_CUDA(cudaMemcpyAsync(params, s->guess.P.p, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
+        BBRT_CUDA(cudaStreamSynchronize(st));
+        return BBRT_OK;
+    }
+    if ((rc = guess_alloc(s, np))) return rc;
+    BBRT_CUDA(cudaMemcpyAsync(s->guess.P.p, params, sizeof(float) * n, cudaMemcpyHostToDevice, st));
+    BBRT_CUDA(cudaMemsetAsync(s->guess.m1.p, 0, sizeof(float) * n, st));
+    BBRT_CUDA(cudaMemsetAsync(s->guess.m2.p, 0, sizeof(float) * n, st));
+    BBRT_CUDA(bbrt::mlp_pack(static_cast<const float*>(s->guess.P.p), static_cast<uint8_t*>(s->guess.image.p), st));
+    BBRT_CUDA(cudaStreamSynchronize(st));
+    s->guess.trained = true;
+    return BBRT_OK;
+}
+
+BBRT_API int bbrt_guess_train(bbrt_scene_t s, const double* origins, const double* dirs, long long n, int max_bounces,
+                              const bbrt_guess_train_config* cfg_in, bbrt_guess_train_report* rep, void* stream) {
+    if (!s || !origins || !dirs) return fail(BBRT_ERR_ARG, "bbrt_guess_train: NULL argument");
+    if (n <= 0) return fail(BBRT_ERR_ARG, "bbrt_guess_train: no rays");
+    if (max_bounces < 0) return fail(BBRT_ERR_ARG, "bbrt_guess_train: max_bounces < 0");
+    bbrt_guess_train_config cfg;
+    bbrt_guess_train_config_init(&cfg);
+    if (cfg_in) cfg = *cfg_in;
+    if (cfg.epochs < 1 || cfg.batch < 128 || cfg.max_positive < 1 || cfg.max_negative < 0 || !(cfg.lr > 0.0f))
+        return fail(BBRT_ERR_ARG, "bbrt_guess_train: bad training configuration");
+    std::lock_guard<std::mutex> g(s->mu);
+    int rc = ensure_uploaded(s);
+    if (rc) return rc;
+    if (s->host.n_patches == 0) return fail(BBRT_ERR_ARG, "bbrt_guess_train: the scene has no patches");
+    cudaStream_t st = pick_stream(s, stream);
+    // ---- 1. samples from a plain FP64 trace of the rays
+    const long long cap_p = cfg.max_positive, cap_n = cfg.max_negative;
+    DevBuf samples, counters, rows;
+    BBRT_CUDA(samples.ensure(sizeof(bbrt::GuessSample) * static_cast<size_t>(cap_p + cap_n)));
+    BBRT_CUDA(counters.ensure(2 * sizeof(unsigned long long)));
+    BBRT_CUDA(cudaMemsetAsync(counters.p, 0, 2 * sizeof(unsigned long long), st));
+    BBRT_CUDA(s->in_o.ensure(sizeof(double) * 3 * n));
+    BBRT_CUDA(s->in_d.ensure(sizeof(double) * 3 * n));
+    BBRT_CUDA(cudaMemcpyAsync(s->in_o.p, origins, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, st));
+    BBRT_CUDA(cudaMemcpyAsync(s->in_d.p, dirs, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, st));
+    const int save_prec = s->dev.precision, save_guess = s->host.cfg.guess;
+    s->dev.precision = BBRT_PREC_FP64;
+    s->host.cfg.guess = BBRT_GUESS_TRIANGLE;
+    s->rec_samples = static_cast<bbrt::GuessSample*>(samples.p);
+    s->rec_count = static_cast<unsigned long long*>(counters.p);
+    s->rec_cap_pos = cap_p;
+    s->rec_cap_neg = cap_n;
+    float collect_ms = 0.0f;
+    rc = run_trace_device(s, static_cast<const double*>(s->in_o.p), static_cast<const double*>(s->in_d.p), n,
+                          max_bounces, nullptr, nullptr, 1, st, false, nullptr, &collect_ms);
+    s->rec_samples = nullptr;
+    s->rec_count = nullptr;
+    s->dev.precision = save_prec;
+    s->host.cfg.guess = save_guess;
+    if (rc) return rc;
+    unsigned long long cnt[2] = { 0, 0 };
+    BBRT_CUDA(cudaMemcpyAsync(cnt, counters.p, sizeof cnt, cudaMemcpyDeviceToHost, st));
+    BBRT_CUDA(cudaStreamSynchronize(st));
+    const long long npos = std::min<long long>(static_cast<long long>(cnt[1]), cap_p);
+    const long long nneg = std::min<long long>(static_cast<long long>(cnt[0]), cap_n);
+    const long long N = npos + nneg;
+    if (npos == 0) return fail(BBRT_ERR_STATE, "bbrt_guess_train: the rays produced no Newton solves to learn from");
+    // ---- 2. training rows
+    const size_t rb = static_cast<size_t>(N) * (bbrt::kGeo * 4 + 4 + 3 * 4 + 4 + 4);
+    BBRT_CUDA(rows.ensure(rb));
+    float* feat = static_cast<float*>(rows.p);
+    int* pid = reinterpret_cast<int*>(feat + N * bbrt::kGeo);
+    float* tgt = reinterpret_cast<float*>(pid + N);
+    float* lbl = tgt + 3 * N;
+    int* idx = reinterpret_cast<int*>(lbl + N);
+    const bbrt::GuessSample* S0 = static_cast<const bbrt::GuessSample*>(samples.p);
+    BBRT_CUDA(bbrt::mlp_make_rows(S0, npos, s->guess.frame, feat, pid, tgt, lbl, st));
+    BBRT_CUDA(bbrt::mlp_make_rows(S0 + cap_p, nneg, s->guess.frame, feat + npos * bbrt::kGeo, pid + npos,
+                                  tgt + 3 * npos, lbl + npos, st));
+    // ---- 3. network
+    const long long np = bbrt_guess_param_count(s);
+    if ((rc = guess_alloc(s, np))) return rc;
+    {
+        const std::vector<float> P0 = init_network(np, cfg.seed);
+        BBRT_CUDA(cudaMemcpyAsync(s->guess.P.p, P0.data(), sizeof(float) * np, cudaMemcpyHostToDevice, st));
+        BBRT_CUDA(cudaStreamSynchronize(st));
+    }
+    BBRT_CUDA(cudaMemsetAsync(s->guess.m1.p, 0, sizeof(float) * np, st));
+    BBRT_CUDA(cudaMemsetAsync(s->guess.m2.p, 0, sizeof(float) * np, st));
+    BBRT_CUDA(cudaMemsetAsync(s->guess.G.p, 0, sizeof(float) * np, st));
+    BBRT_CUDA(cudaMemsetAsync(s->guess.err.p, 0, sizeof(int), st));
+    BBRT_CUDA(bbrt::mlp_pack(static_cast<const float*>(s->guess.P.p), static_cast<uint8_t*>(s->guess.image.p), st));
+    // ---- 4. epochs of shuffled batches
+    const int B = static_cast<int>(std::min<long long>(cfg.batch, N));
+    const long long per_epoch = (N + B - 1) / B;
+    const long long steps = per_epoch * cfg.epochs;
+    BBRT_CUDA(s->guess.loss.ensure(sizeof(float) * static_cast<size_t>(steps)));
+    BBRT_CUDA(cudaMemsetAsync(s->guess.loss.p, 0, sizeof(float) * steps, st));
+    std::vector<int> perm(static_cast<size_t>(N));
+    std::iota(perm.begin(), perm.end(), 0);
+    std::mt19937_64 rng(cfg.seed ^ 0x9E3779B97F4A7C15ULL);
+    BBRT_CUDA(cudaEventRecord(s->ev[0], st));
+    bbrt::MlpNet net = guess_net(s);
+    long long step = 0;
+    for (int ep = 0; ep < cfg.epochs; ++ep) {
+        std::shuffle(perm.begin(), perm.end(), rng);
+        BBRT_CUDA(cudaMemcpyAsync(idx, perm.data(), sizeof(int) * N, cudaMemcpyHostToDevice, st));
+        for (long long b0 = 0; b0 < N; b0 += B, ++step) {
+            bbrt::MlpBatch bt;
+            bt.feat = feat;
+            bt.pid = pid;
+            bt.tgt = tgt;
+            bt.lbl = lbl;
+            bt.idx = idx + b0;
+            bt.B = static_cast<int>(std::min<long long>(B, N - b0));
+            bt.inv_b = 1.0f / static_cast<float>(bt.B);
+            net.loss = static_cast<float*>(s->guess.loss.p) + step;
+            BBRT_CUDA(bbrt::mlp_train_batch(bt, net, st));
+            BBRT_CUDA(bbrt::mlp_adam(net, static_cast<float*>(s->guess.m1.p), static_cast<float*>(s->guess.m2.p), np,
+                                     cfg.lr, static_cast<int>(step + 1), st));
+            BBRT_CUDA(cudaMemsetAsync(s->guess.G.p, 0, sizeof(float) * np, st));
+            BBRT_CUDA(bbrt::mlp_pack(static_cast<const float*>(s->guess.P.p), static_cast<uint8_t*>(s->guess.image.p), st));
+        }
+        // the host copy of the permutation must outlive its upload
+        BBRT_CUDA(cudaStreamSynchronize(st));
+    }
+    BBRT_CUDA(cudaEventRecord(s->ev[1], st));
+    if ((rc = guess_err_check(s, st))) return rc;
+    float train_ms = 0.0f;
+    BBRT_CUDA(cudaEventElapsedTime(&train_ms, s->ev[0], s->ev[1]));
+    std::vector<float> losses(static_cast<size_t>(steps));
+    BBRT_CUDA(cudaMemcpy(losses.data(), s->guess.loss.p, sizeof(float) * steps, cudaMemcpyDeviceToHost));
+    s->guess.trained = true;
+    s->guess.steps = steps;
+    s->guess.min_logit = cfg.min_logit;
+    s->guess.t_window = cfg.t_window;
+    if (rep) {
+        std::memset(rep, 0, sizeof *rep);
+        rep->positives = npos;
+        rep->negatives = nneg;
+        rep->steps = steps;
+        double f = 0.0, l = 0.0;
+        for (long long k = 0; k < per_epoch; ++k) {
+            f += losses[k];
+            l += losses[steps - per_epoch + k];
+        }
+        rep->first_loss = f / per_epoch;
+        rep->last_loss = l / per_epoch;
+        rep->collect_ms = collect_ms;
+        rep->train_ms = train_ms;
+    }
+    return BBRT_OK;
+}
+
+namespace {
+
+// Standalone network buffers for the check entry points.
+struct CheckNet {
+    std::vector<void*> bufs;
+    ~CheckNet() {
+        for (void* p : bufs) cudaFree(p);
+    }
+    template <class T>
+    T* alloc(size_t count) {
+        void* p = nullptr;
+        if (cudaMalloc(&p, sizeof(T) * (count ? count : 1)) != cudaSuccess) return nullptr;
+        bufs.push_back(p);
+        return static_cast<T*>(p);
+    }
+};
+
+}  // namespace
+
+BBRT_API int bbrt_mlp_check(const float* params, int n_patches, const float* feat, const int* patch,
+                            const float* target, const float* label, int rows, float* loss, float* out,
+                            float* grads) {
+    if (!params || !feat || !patch || !target || !label || !loss || !out || !grads || rows < 1 || n_patches < 1)
+        return fail(BBRT_ERR_ARG, "bbrt_mlp_check: bad argument");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0)
+        return fail(BBRT_ERR_CUDA, "bbrt: no CUDA device available (the trace path has no CPU fallback)");
+    for (int r = 0; r < rows; ++r)
+        if (patch[r] < 0 || patch[r] >= n_patches) return fail(BBRT_ERR_ARG, "bbrt_mlp_check: patch index out of range");
+    const long long np = bbrt::oE + static_cast<long long>(bbrt::kEmb) * n_patches;
+    CheckNet c;
+    float* P = c.alloc<float>(np);
+    float* G = c.alloc<float>(np);
+    uint8_t* image = c.alloc<uint8_t>(bbrt::kImageBytes);
+    float* dfeat = c.alloc<float>(static_cast<size_t>(rows) * bbrt::kGeo);
+    int* dpid = c.alloc<int>(rows);
+    float* dtgt = c.alloc<float>(3 * static_cast<size_t>(rows));
+    float* dlbl = c.alloc<float>(rows);
+    float* dloss = c.alloc<float>(1);
+    float* dout = c.alloc<float>(4 * static_cast<size_t>(rows));
+    int* derr = c.alloc<int>(1);
+    if (!P || !G || !image || !dfeat || !dpid || !dtgt || !dlbl || !dloss || !dout || !derr)
+        return fail(BBRT_ERR_NOMEM, "bbrt_mlp_check: cudaMalloc failed");
+    BBRT_CUDA(cudaMemcpy(P, params, sizeof(float) * np, cudaMemcpyHostToDevice));
+    BBRT_CUDA(cudaMemset(G, 0, sizeof(float) * np));
+    BBRT_CUDA(cudaMemcpy(dfeat, feat, sizeof(float) * rows * bbrt::kGeo, cudaMemcpyHostToDevice));
+    BBRT_CUDA(cudaMemcpy(dpid, patch, sizeof(int) * rows, cudaMemcpyHostToDevice));
+    BBRT_CUDA(cudaMemcpy(dtgt, target, sizeof(float) * 3 * rows, cudaMemcpyHostToDevice));
+    BBRT_CUDA(cudaMemcpy(dlbl, label, sizeof(float) * rows, cudaMemcpyHostToDevice));
+    BBRT_CUDA(cudaMemset(dloss, 0, sizeof(float)));
+    BBRT_CUDA(cudaMemset(derr, 0, sizeof(int)));
+    BBRT_CUDA(bbrt::mlp_pack(P, image, nullptr));
+    bbrt::MlpNet net;
+    net.image = image;
+    net.P = P;
+    net.G = G;
+    net.loss = dloss;
+    net.out = dout;
+    net.err = derr;
+    bbrt::MlpBatch bt;
+    bt.feat = dfeat;
+    bt.pid = dpid;
+    bt.tgt = dtgt;
+    bt.lbl = dlbl;
+    bt.idx = nullptr;
+    bt.B = rows;
+    bt.inv_b = 1.0f / static_cast<float>(rows);
+    BBRT_CUDA(bbrt::mlp_train_batch(bt, net, nullptr));
+    BBRT_CUDA(cudaDeviceSynchronize());
+    int herr = 0;
+    BBRT_CUDA(cudaMemcpy(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost));
+    if (herr) return fail(BBRT_ERR_KERNEL, "bbrt_mlp_check: a tensor-core completion wait timed out");
+    std::vector<float> gdev(static_cast<size_t>(np));
+    BBRT_CUDA(cudaMemcpy(gdev.data(), G, sizeof(float) * np, cudaMemcpyDeviceToHost));
+    BBRT_CUDA(cudaMemcpy(loss, dloss, sizeof(float), cudaMemcpyDeviceToHost));
+    BBRT_CUDA(cudaMemcpy(out, dout, sizeof(float) * 4 * rows, cudaMemcpyDeviceToHost));
+    for (long long p = 0; p < np; ++p) grads[p] = gdev[static_cast<size_t>(bbrt::grad_index(p))];
+    return BBRT_OK;
+}
+
+BBRT_API int bbrt_mlp_infer_check(const float* params, int n_patches, const float* feat, const int* patch, int rows,
+                                  double* out) {
+    if (!params || !feat || !patch || !out || rows < 1 || n_patches < 1)
+        return fail(BBRT_ERR_ARG, "bbrt_mlp_infer_check: bad argument");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0)
+        return fail(BBRT_ERR_CUDA, "bbrt: no CUDA device available (the trace path has no CPU fallback)");
+    for (int r = 0; r < rows; ++r)
+        if (patch[r] < 0 || patch[r] >= n_patches)
+            return fail(BBRT_ERR_ARG, "bbrt_mlp_infer_check: patch index out of range");
+    const long long np = bbrt::oE + static_cast<long long>(bbrt::kEmb) * n_patches;
+    CheckNet c;
+    float* P = c.alloc<float>(np);
+    uint8_t* image = c.alloc<uint8_t>(bbrt::kImageBytes);
+    float* dfeat = c.alloc<float>(static_cast<size_t>(rows) * bbrt::kGeo);
+    int* dpid = c.alloc<int>(rows);
+    double* dout = c.alloc<double>(4 * static_cast<size_t>(rows));
+    int* derr = c.alloc<int>(1);
+    if (!P || !image || !dfeat || !dpid || !dout || !derr) return fail(BBRT_ERR_NOMEM, "bbrt_mlp_infer_check: cudaMalloc failed");
+    BBRT_CUDA(cudaMemcpy(P, params, sizeof(float) * np, cudaMemcpyHostToDevice));
+    BBRT_CUDA(cudaMemcpy(dfeat, feat, sizeof(float) * rows * bbrt::kGeo, cudaMemcpyHostToDevice));
+    BBRT_CUDA(cudaMemcpy(dpid, patch, sizeof(int) * rows, cudaMemcpyHostToDevice));
+    BBRT_CUDA(cudaMemset(derr, 0, sizeof(int)));
+    BBRT_CUDA(bbrt::mlp_pack(P, image, nullptr));
+    bbrt::MlpNet net;
+    net.image = image;
+    net.P = P;
+    net.G = nullptr;
+    net.loss = nullptr;
+    net.out = nullptr;
+    net.err = derr;
+    BBRT_CUDA(bbrt::mlp_infer_features(dfeat, dpid, rows, net, dout, nullptr));
+    BBRT_CUDA(cudaDeviceSynchronize());
+    int herr = 0;
+    BBRT_CUDA(cudaMemcpy(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost));
+    if (herr) return fail(BBRT_ERR_KERNEL, "bbrt_mlp_infer_check: a tensor-core completion wait timed out");
+    BBRT_CUDA(cudaMemcpy(out, dout, sizeof(double) * 4 * rows, cudaMemcpyDeviceToHost));
     return BBRT_OK;
 }

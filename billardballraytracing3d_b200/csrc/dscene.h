@@ -7,6 +7,8 @@
 
 namespace bbrt {
 
+struct GuessSample;
+
 struct DScene {
     int n_objects = 0;
     int n_nodes = 0;
@@ -38,6 +40,9 @@ struct DScene {
     const long long* p_field_off = nullptr;// node-major, 12 doubles per node
     const double* p_nodes = nullptr;
     const double* p_fields = nullptr;
+    const float* p_nodes32 = nullptr;      // FP32 copies (same offsets) for the FP32 Newton phase
+    const float* p_fields32 = nullptr;
+    int precision = 0;                     // BBRT_PREC_*
     const double* coarse_uv = nullptr;     // [coarse_n]
     const double* c_xyz = nullptr;         // [n_patches][coarse_n^2][3]
     const double* c_cell = nullptr;        // [n_patches][(coarse_n-1)^2][4] normal xyz, sagitta
@@ -65,6 +70,8 @@ enum StatSlot {
     ST_NEWTON_ITERS, ST_NEWTON_ITERS_FP32, ST_HIST0,
     // share of the tail kernels (also included in the totals above)
     ST_TAIL_NODE_TESTS = ST_HIST0 + 8, ST_TAIL_CELL_TESTS, ST_TAIL_TRI_TESTS, ST_TAIL_NEWTON_ITERS, ST_TAIL_RAYS,
+    // learned guess: Newton solves started from the network, and those that fell back to the triangle
+    ST_GUESS_USED, ST_GUESS_FALLBACK,
     ST_COUNT
 };
 
@@ -89,6 +96,12 @@ struct TraceArgs {
     int count_from = 1;                // first bounce index that is counted
     long long* stats = nullptr;        // [ST_COUNT], may be null
     unsigned long long* work_counter = nullptr;  // persistent-launch ray counter (zeroed by host)
+    // Training-sample recording (learned guess): converged Newton solves go to
+    // samples[0, cap_pos), stage-1 misses to samples[cap_pos, cap_pos + cap_neg);
+    // sample_count[1] / [0] count positives / negatives offered (may exceed the caps).
+    GuessSample* samples = nullptr;
+    unsigned long long* sample_count = nullptr;
+    long long sample_cap_pos = 0, sample_cap_neg = 0;
 };
 
 // A patch query of the current bounce whose stage-1 winner needs Newton.
@@ -122,6 +135,11 @@ struct WaveArgs {
     unsigned int* counters = nullptr;          // [0] requests of the round, [1] overflowed rays (cumulative),
                                                // [2] runnable rays fetched this round
     int* overflow = nullptr;                   // rays whose query needs more than kResolved solves
+    // Learned guess of this round's requests: guess[r] = (u, v, t, logit), or null.
+    const double* guess = nullptr;
+    const double* frame = nullptr;             // per-patch frames (size L at [12] of each 16)
+    double guess_min_logit = 0.0;              // confidence needed to start Newton from the guess
+    double guess_t_window = 0.5;               // accepted |t - t_stage1| in units of L
 };
 
 struct QueryArgs {

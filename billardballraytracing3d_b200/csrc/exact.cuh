@@ -220,4 +220,92 @@ __device__ __forceinline__ int newton_exact(const DScene& S, int pidx, const V3 
     return 1;
 }
 
+// ---- FP32 Newton phase (precision split) -----------------------------------
+
+constexpr int kFp32Iters = 8;          // FP32 iterations before giving up on the phase
+constexpr float kFp32Residual = 1e-5f; // |F| at which the FP64 finish takes over
+
+__device__ __forceinline__ void basis_1d_f(const float* nodes, const float* w, int N, float x, float* b) {
+    for (int i = 0; i < N; ++i) b[i] = 0.0f;
+    for (int i = 0; i < N; ++i)
+        if (x == nodes[i]) { b[i] = 1.0f; return; }
+    float denom = 0.0f;
+    for (int i = 0; i < N; ++i) {
+        const float li = w[i] / (x - nodes[i]);
+        b[i] = li;
+        denom += li;
+    }
+    const float inv = 1.0f / denom;
+    for (int i = 0; i < N; ++i) b[i] *= inv;
+}
+
+// Newton on F(u,v,t) in FP32 until |F| < kFp32Residual.  Returns true with
+// the FP32 iterate in (u, v, t); false when it is singular, leaves the
+// neighbourhood of the patch or does not get there in kFp32Iters steps.
+__device__ __forceinline__ bool newton_fp32(const DScene& S, int pidx, const V3& o, const V3& d, double& u,
+                                            double& v, double& t, long long& iters32) {
+    const int I = S.p_dims[2 * pidx], J = S.p_dims[2 * pidx + 1];
+    const float* un = S.p_nodes32 + S.p_node_off[pidx];
+    const float* vn = un + I;
+    const float* uw = vn + J;
+    const float* vw = uw + I;
+    const float* Fd = S.p_fields32 + S.p_field_off[pidx];
+    const float ox = static_cast<float>(o.x), oy = static_cast<float>(o.y), oz = static_cast<float>(o.z);
+    const float dx = static_cast<float>(d.x), dy = static_cast<float>(d.y), dz = static_cast<float>(d.z);
+    float uf = static_cast<float>(u), vf = static_cast<float>(v), tf = static_cast<float>(t);
+    float bu[kDevMaxNodes], bv[kDevMaxNodes];
+    for (int it = 0; it < kFp32Iters; ++it) {
+        ++iters32;
+        basis_1d_f(un, uw, I, uf, bu);
+        basis_1d_f(vn, vw, J, vf, bv);
+        float e[9];
+        for (int f = 0; f < 9; ++f) e[f] = 0.0f;
+        for (int i = 0; i < I; ++i) {
+            const float li = bu[i];
+            if (li == 0.0f) continue;
+            float rs[9];
+            for (int f = 0; f < 9; ++f) rs[f] = 0.0f;
+            const float* row = Fd + static_cast<long long>(i) * J * 12;
+            for (int j = 0; j < J; ++j)
+                for (int f = 0; f < 9; ++f) rs[f] = fmaf(bv[j], row[j * 12 + f], rs[f]);
+            for (int f = 0; f < 9; ++f) e[f] = fmaf(li, rs[f], e[f]);
+        }
+        const float Fx = e[0] - fmaf(tf, dx, ox), Fy = e[1] - fmaf(tf, dy, oy), Fz = e[2] - fmaf(tf, dz, oz);
+        if (fabsf(Fx) < kFp32Residual && fabsf(Fy) < kFp32Residual && fabsf(Fz) < kFp32Residual) {
+            u = uf;
+            v = vf;
+            t = tf;
+            return true;
+        }
+        const float a11 = e[3], a12 = e[6], a13 = -dx, a21 = e[4], a22 = e[7], a23 = -dy, a31 = e[5], a32 = e[8],
+                    a33 = -dz;
+        const float c1 = a22 * a33 - a23 * a32, c2 = a21 * a33 - a23 * a31, c3 = a21 * a32 - a22 * a31;
+        const float det = a11 * c1 - a12 * c2 + a13 * c3;
+        if (!(fabsf(det) > 1e-30f)) return false;
+        const float id = 1.0f / det;
+        const float x0 = (Fx * c1 - a12 * (Fy * a33 - a23 * Fz) + a13 * (Fy * a32 - a22 * Fz)) * id;
+        const float x1 = (a11 * (Fy * a33 - a23 * Fz) - Fx * c2 + a13 * (a21 * Fz - Fy * a31)) * id;
+        const float x2 = (a11 * (a22 * Fz - Fy * a32) - a12 * (a21 * Fz - Fy * a31) + Fx * c3) * id;
+        uf -= x0;
+        vf -= x1;
+        tf -= x2;
+        if (!(fabsf(uf) < 2.0f && fabsf(vf) < 2.0f) || !isfinite(tf)) return false;
+    }
+    return false;
+}
+
+// The precision split: FP32 Newton to |F| < 1e-5 from (u, v, t), then the
+// FP64 loop (the reference's step test and iteration cap) from that iterate.
+// When the FP32 phase fails, the FP64 loop starts from (u, v, t) itself.
+__device__ __forceinline__ int newton_split(const DScene& S, int pidx, const V3 o, const V3 d, double u, double v,
+                                            double t, QHit& h, long long& iters, long long& iters32) {
+    double uu = u, vv = v, tt = t;
+    if (!newton_fp32(S, pidx, o, d, uu, vv, tt, iters32)) {
+        uu = u;
+        vv = v;
+        tt = t;
+    }
+    return newton_exact(S, pidx, o, d, uu, vv, tt, h, iters);
+}
+
 }  // namespace bbrt

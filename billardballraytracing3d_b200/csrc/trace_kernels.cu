@@ -20,6 +20,7 @@
 
 #include "../../include/bbrt.h"
 #include "exact.cuh"
+#include "guess.h"
 
 namespace bbrt {
 
@@ -459,6 +460,20 @@ __device__ __forceinline__ long long warp_append(unsigned int* counter, bool wan
     return static_cast<long long>(base) + __popc(mask & ((1u << lane) - 1u));
 }
 
+// Appends one training sample (learned guess) when recording is on.
+__device__ __forceinline__ void record_sample(const TraceArgs& A, int label, const V3& o, const V3& d, int pidx,
+                                              double u, double v, double t) {
+    const unsigned long long k = atomicAdd(A.sample_count + label, 1ULL);
+    const long long cap = label ? A.sample_cap_pos : A.sample_cap_neg;
+    if (static_cast<long long>(k) >= cap) return;
+    GuessSample* s = A.samples + (label ? 0 : A.sample_cap_pos) + k;
+    s->o[0] = o.x; s->o[1] = o.y; s->o[2] = o.z;
+    s->d[0] = d.x; s->d[1] = d.y; s->d[2] = d.z;
+    s->u = u; s->v = v; s->t = t;
+    s->patch = pidx;
+    s->label = label;
+}
+
 // Advance-kernel modes.  The kernel is persistent: each lane owns one ray at
 // a time and the body is one flat loop in which every iteration does one
 // small unit of work for the lane's ray (one BVH node test, one leaf object,
@@ -701,6 +716,7 @@ __global__ void __launch_bounds__(128) k_advance(DScene S, TraceArgs A, WaveArgs
             if (++q.tri == 6) mode = q.tri_ret;
         } else if (mode == M_S1_DONE) {
             if (!q.s1.have) {
+                if (A.samples) record_sample(A, 0, r.o, r.d, q.pidx, 0.0, 0.0, 0.0);
                 ++q.leaf_k;
                 mode = M_LEAF;
             } else if (nres >= kResolved) {
@@ -807,31 +823,65 @@ __global__ void __launch_bounds__(128) k_advance(DScene S, TraceArgs A, WaveArgs
     flush_stats(A, ctr, tally);
 }
 
-// Newton solves of one round, one request per thread.
+// Newton on patch pidx in the scene's precision mode.
+__device__ __forceinline__ int newton_mode(const DScene& S, int pidx, const V3& o, const V3& d, double u, double v,
+                                           double t, QHit& h, long long& iters, long long& iters32) {
+    if (S.precision == BBRT_PREC_SPLIT) return newton_split(S, pidx, o, d, u, v, t, h, iters, iters32);
+    return newton_exact(S, pidx, o, d, u, v, t, h, iters);
+}
+
+// Newton solves of one round, one request per thread.  With a learned guess,
+// a confident guess is tried first; its root is kept only when it converges
+// inside the patch within guess_t_window patch sizes of the stage-1 t, and
+// otherwise the solve restarts from the stage-1 triangle (the reference's start).
 __global__ void __launch_bounds__(128) k_newton(DScene S, TraceArgs A, WaveArgs W, long long n_req) {
     const long long j = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
-    long long iters = 0;
+    long long iters = 0, iters32 = 0, used = 0, fallback = 0;
     if (j < n_req) {
         const NewtonRequest q = W.req[j];
         const V3 o = load3(W.o + 3LL * q.ray);
         const V3 d = load3(W.d + 3LL * q.ray);
-        double u0, v0;
-        key_to_uv(S, q.key, u0, v0);
+        const int pidx = S.obj_sub[q.obj];
         QHit h;
         h.err = 0;
         h.ev0 = h.ev1 = 0.0;
         h.t = 0.0;
         h.p = h.n = v3(0.0, 0.0, 0.0);
         h.u = h.v = 0.0;
-        newton_exact(S, S.obj_sub[q.obj], o, d, u0, v0, q.t0, h, iters);
+        bool done = false;
+        if (W.guess) {
+            const double* g = W.guess + 4 * j;
+            const double win = W.guess_t_window * W.frame[16LL * pidx + 12];
+            if (g[3] > W.guess_min_logit && isfinite(g[0]) && isfinite(g[1]) && fabs(g[2] - q.t0) <= win) {
+                used = 1;
+                QHit hg = h;
+                if (newton_mode(S, pidx, o, d, g[0], g[1], g[2], hg, iters, iters32) && fabs(hg.t - q.t0) <= win) {
+                    h = hg;
+                    done = true;
+                } else {
+                    fallback = 1;
+                }
+            }
+        }
+        if (!done) {
+            double u0, v0;
+            key_to_uv(S, q.key, u0, v0);
+            newton_mode(S, pidx, o, d, u0, v0, q.t0, h, iters, iters32);
+        }
+        if (A.samples && h.err == 0) record_sample(A, 1, o, d, pidx, h.u, h.v, h.t);
         const long long e = static_cast<long long>(q.ray) * kResolved + q.entry;
         double* rd = W.res_data + e * kResData;
         rd[0] = h.t; rd[1] = h.p.x; rd[2] = h.p.y; rd[3] = h.p.z;
         rd[4] = h.n.x; rd[5] = h.n.y; rd[6] = h.n.z; rd[7] = h.u; rd[8] = h.v; rd[9] = h.ev0; rd[10] = h.ev1;
         W.res_err[e] = h.err;
-        if (A.ray_work) A.ray_work[4LL * q.ray + 3] += iters;
+        if (A.ray_work) A.ray_work[4LL * q.ray + 3] += iters + iters32;
     }
-    if (A.stats) warp_add(A.stats + ST_NEWTON_ITERS, iters);
+    if (A.stats) {
+        warp_add(A.stats + ST_NEWTON_ITERS, iters);
+        warp_add(A.stats + ST_NEWTON_ITERS_FP32, iters32);
+        warp_add(A.stats + ST_GUESS_USED, used);
+        warp_add(A.stats + ST_GUESS_FALLBACK, fallback);
+    }
 }
 
 // Finishes rays from their saved state with inline queries (the tail of a

@@ -78,9 +78,10 @@ __device__ __forceinline__ void mbar_init(uint32_t mbar, uint32_t count) {
 }
 
 // Waits for the phase with the given parity to complete; gives up after
-// `limit` polls and returns false (the caller reports the error).
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, long long limit) {
-    for (long long it = 0; it < limit; ++it) {
+// `max_cycles` SM clock cycles and returns false (the caller reports it).
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, long long max_cycles) {
+    const long long start = clock64();
+    while (clock64() - start < max_cycles) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -110,7 +111,7 @@ __device__ __forceinline__ void tmem_free(uint32_t base, uint32_t ncols) {
 }
 
 // 16 consecutive FP32 columns of this thread's TMEM lane (warp w of the
-// warpgroup reads lanes 32w..32w+31); follow with wait_ld before use.
+// warpgroup reads lanes 32w..32w+31), waited for before returning.
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
     uint32_t r[16];
     asm volatile(

@@ -207,6 +207,9 @@ typedef struct bbrt_trace_stats {
     long long tail_rays;      /* rays finished by the tail kernel */
     long long tail_node_tests, tail_cell_tests, tail_tri_tests, tail_newton_iters;   /* the tail's share */
     long long launches;       /* kernels this library launched for the call */
+    long long guess_used;     /* Newton solves started from the learned guess */
+    long long guess_fallback; /* ... of which restarted from the stage-1 triangle */
+    double guess_ms;          /* learned-guess inference kernels */
 } bbrt_trace_stats;
 
 /* ---- library ---------------------------------------------------------- */
@@ -308,6 +311,62 @@ BBRT_API int  bbrt_bounce_map_rays(bbrt_scene_t scene, const bbrt_patch_desc* sa
                                    int n_sample, int grid_n, int theta_n, int phi_n,
                                    double cone_angle_deg, const long long* ray_index, long long n,
                                    double* origins, double* dirs);
+
+/* ---- arithmetic modes and the learned guess (no reference counterpart) ---
+ *
+ * bbrt_scene_set_modes switches a scene between BBRT_PREC_FP64 (bit-identical
+ * to the reference) and BBRT_PREC_SPLIT (FP32 Newton phase to |F| < 1e-5,
+ * then the reference's FP64 loop), and between the stage-1 triangle and the
+ * learned Newton start (BBRT_GUESS_LEARNED needs a trained network; without
+ * one the triangle start is used).  The learned guess applies to the Newton
+ * solves of the wavefront rounds; the last rays of a trace (the tail) and
+ * batches below the wavefront size start from the triangle.
+ *
+ * bbrt_guess_train traces the given rays with the scene's plain FP64 path,
+ * records every converged Newton solve (ray, patch -> u, v, t) and every
+ * stage-1 miss (ray, patch) as training samples, and trains the network on
+ * the GPU (tensor-core forward and backward kernels, Adam).  The network maps
+ * the ray in the patch's frame, the patch box and a learned 32-wide patch
+ * embedding to (u, v, t) and a confidence. */
+typedef struct bbrt_guess_train_config {
+    int epochs;                  /* passes over the samples (8) */
+    int batch;                   /* rows per step (65536) */
+    float lr;                    /* Adam learning rate (1e-3) */
+    long long max_positive;      /* converged solves kept (4M) */
+    long long max_negative;      /* stage-1 misses kept (1M) */
+    unsigned long long seed;     /* initialisation and shuffling (1) */
+    double min_logit;            /* confidence logit needed to use a guess (0) */
+    double t_window;             /* accepted |t - t_stage1| in patch sizes (0.5) */
+} bbrt_guess_train_config;
+
+typedef struct bbrt_guess_train_report {
+    long long positives, negatives;   /* samples trained on */
+    long long steps;                  /* optimiser steps */
+    double first_loss, last_loss;     /* mean batch loss of the first and last epoch */
+    double collect_ms, train_ms;      /* sample trace, training (device time) */
+} bbrt_guess_train_report;
+
+BBRT_API int  bbrt_scene_set_modes(bbrt_scene_t scene, int precision, int guess);
+BBRT_API void bbrt_guess_train_config_init(bbrt_guess_train_config* cfg);
+BBRT_API int  bbrt_guess_train(bbrt_scene_t scene, const double* origins, const double* dirs, long long n,
+                               int max_bounces, const bbrt_guess_train_config* cfg,
+                               bbrt_guess_train_report* report, void* stream);
+/* Number of FP32 network parameters of a scene: 43408 + 32 * patches. */
+BBRT_API long long bbrt_guess_param_count(bbrt_scene_t scene);
+/* Copies the parameters out (set = 0) or in (set = 1; marks the network trained). */
+BBRT_API int  bbrt_guess_params(bbrt_scene_t scene, float* params, long long n, int set);
+
+/* One forward + backward pass of the network on the device, for checking the
+ * kernels (no reference counterpart): params in the flat layout of
+ * bbrt_guess_params for n_patches patches; rows of 9 geometric features,
+ * patch index, targets (u, v, s) and label.  Returns the loss, the outputs
+ * (u, v, s, logit per row) and the gradients in the params layout. */
+BBRT_API int  bbrt_mlp_check(const float* params, int n_patches, const float* feat, const int* patch,
+                             const float* target, const float* label, int rows, float* loss, float* out,
+                             float* grads);
+/* Inference kernel on the same inputs: out[rows][4] = u, v, s, logit. */
+BBRT_API int  bbrt_mlp_infer_check(const float* params, int n_patches, const float* feat, const int* patch,
+                                   int rows, double* out);
 
 /* ---- diagnostics ------------------------------------------------------ */
 enum {

@@ -23,3 +23,133 @@ def test_umma_operand_layouts(built):
     for v in range(4):
         err = np.max(np.abs(d[v] - want))
         assert err < 1e-3 * np.max(np.abs(want)), (v, err)
+
+
+def _mlp_case(P=7, B=300, seed=3):
+    rng = np.random.default_rng(seed)
+    params = R.init_params(P, seed)
+    off = R.offsets()
+    for name in ("b0", "b1", "b2"):
+        params[off[name]:off[name] + R.N_H] = rng.normal(0.0, 0.05, R.N_H)
+    params[off["b3"]:off["b3"] + 4] = rng.normal(0.0, 0.05, 4)
+    feat = rng.normal(0.0, 1.0, (B, R.N_GEO)).astype(np.float32)
+    pid = rng.integers(0, P, B).astype(np.int32)
+    tgt = rng.normal(0.0, 0.5, (B, 3)).astype(np.float32)
+    lbl = (rng.random(B) < 0.7).astype(np.float32)
+    return params.astype(np.float32), P, feat, pid, tgt, lbl
+
+
+def _device_check(lib, params, P, feat, pid, tgt, lbl):
+    B = feat.shape[0]
+    loss = np.zeros(1, np.float32)
+    out = np.zeros((B, 4), np.float32)
+    grads = np.zeros_like(params)
+    F = ctypes.c_float
+    rc = lib.bbrt_mlp_check(C.ptr(params, F), P, C.ptr(feat, F), C.ptr(pid, ctypes.c_int), C.ptr(tgt, F),
+                            C.ptr(lbl, F), B, C.ptr(loss, F), C.ptr(out, F), C.ptr(grads, F))
+    C.check(lib, rc, "bbrt_mlp_check")
+    return float(loss[0]), out, grads
+
+
+def test_oracle_mlp_gradients_match_finite_differences():
+    """Pins the CPU restatement itself: its analytic backward pass against
+    central differences of its loss (FP64, no BF16 rounding)."""
+    params, P, feat, pid, tgt, lbl = _mlp_case(P=4, B=9, seed=11)
+    p = params.astype(np.float64)
+    _, _, g = R.forward_backward(p, P, feat, pid, tgt, lbl, rounding=False)
+    off = R.offsets()
+    picks = [off["W0"] + 5, off["W0"] + 64 * 3 + 20, off["b0"] + 7, off["W1"] + 300, off["b1"] + 1,
+             off["W2"] + 9000, off["b2"] + 100, off["W3"] + 2 * 128 + 5, off["b3"] + 3, off["E"] + int(pid[0]) * 32 + 4]
+    for k in picks:
+        e = np.zeros_like(p)
+        e[k] = 1e-6
+        lp = R.forward_backward(p + e, P, feat, pid, tgt, lbl, rounding=False)[0]
+        lm = R.forward_backward(p - e, P, feat, pid, tgt, lbl, rounding=False)[0]
+        fd = (lp - lm) / 2e-6
+        assert abs(fd - g[k]) <= 1e-6 + 1e-5 * abs(fd), (k, fd, g[k])
+
+
+@pytest.mark.gpu
+def test_mlp_forward_backward_matches_oracle(built):
+    """Tensor-core forward + backward (BF16 operands, FP32 accumulation)
+    against the oracle with the same BF16 roundings: loss, outputs and the
+    gradient of every parameter block, over three 128-row tiles (one partial)."""
+    lib = C.load_library()
+    params, P, feat, pid, tgt, lbl = _mlp_case()
+    loss, out, grads = _device_check(lib, params, P, feat, pid, tgt, lbl)
+    rl, rout, rg = R.forward_backward(params.astype(np.float64), P, feat, pid, tgt, lbl)
+    assert abs(loss - rl) <= 1e-3 * abs(rl)
+    assert np.max(np.abs(out - rout)) <= 2e-2 * (1.0 + np.max(np.abs(rout)))
+    assert np.mean(np.abs(out - rout)) <= 2e-3
+    off = R.offsets()
+    blocks = [(name, off[name], off[name] + int(np.prod(shp))) for name, shp in R.SHAPES]
+    blocks.append(("E", off["E"], params.size))
+    for name, a, b in blocks:
+        ref = rg[a:b]
+        err = np.linalg.norm(grads[a:b] - ref) / max(np.linalg.norm(ref), 1e-12)
+        assert err < 2e-2, (name, err)
+    # padding rows and columns get no gradient
+    W0 = grads[off["W0"]:off["b0"]].reshape(R.N_H, R.N_IN)
+    assert np.all(W0[:, R.N_GEO + R.N_EMB:] == 0.0)
+    W3 = grads[off["W3"]:off["b3"]].reshape(R.N_OUT, R.N_H)
+    assert np.all(W3[4:] == 0.0)
+
+
+@pytest.mark.gpu
+def test_mlp_inference_equals_training_forward(built):
+    lib = C.load_library()
+    params, P, feat, pid, tgt, lbl = _mlp_case(B=517, seed=8)
+    _, out, _ = _device_check(lib, params, P, feat, pid, tgt, lbl)
+    inf = np.zeros((feat.shape[0], 4))
+    rc = lib.bbrt_mlp_infer_check(C.ptr(params, ctypes.c_float), P, C.ptr(feat, ctypes.c_float),
+                                  C.ptr(pid, ctypes.c_int), feat.shape[0], C.ptr(inf))
+    C.check(lib, rc, "bbrt_mlp_infer_check")
+    assert np.max(np.abs(inf - out)) <= 1e-5 * (1.0 + np.max(np.abs(out)))
+
+
+def _compare_traces(plain, other, K):
+    """Fraction of rays whose status and hit-object sequence match, and the
+    largest hit-point difference over the matching rays."""
+    same = (plain["status"] == other["status"]) & (plain["bounce_count"] == other["bounce_count"])
+    same &= np.all(plain["hit_object"][:, :K] == other["hit_object"][:, :K], axis=1)
+    b = plain["bounce_count"]
+    mask = np.arange(K)[None, :] < np.minimum(b, K)[:, None]
+    diff = np.abs(plain["hit_point"] - other["hit_point"]).max(axis=2)
+    err = np.max(np.where(mask & same[:, None], diff, 0.0))
+    return float(np.mean(same)), float(err)
+
+
+@pytest.mark.gpu
+def test_learned_guess_and_precision_split_trace(built):
+    """Train the network on one seeded ray set of the four-sphere scene, then
+    trace another: the learned and split forms keep the plain FP64 form's
+    statuses and hit sequences on at least 99.9% of rays and its hit points
+    within 1e-10 there; the split moves Newton work to FP32, and a learned
+    start of the split saves FP64 iterations."""
+    from billardballraytracing3d_b200 import api, scenes
+    patches = scenes.scene_tetra_spheres()
+    sc = api.Scene(patches, config=C.default_config(coarse_grid_n=17, newton_tol=1e-12))
+    to, td = scenes.cone_rays(400000, 99, 5.0, 3.0, 10.0)
+    rep = sc.guess_train(to, td, 200, epochs=6)
+    assert rep["positives"] > 50000 and rep["negatives"] > 50000
+    assert rep["last_loss"] < 0.5 * rep["first_loss"], rep
+    o, d = scenes.cone_rays(262144, 1234, 5.0, 3.0, 10.0)
+    K = 8
+    runs = {}
+    for name, prec, guess in (("plain", C.PREC_FP64, C.GUESS_TRIANGLE), ("learned", C.PREC_FP64, C.GUESS_LEARNED),
+                              ("split", C.PREC_SPLIT, C.GUESS_TRIANGLE), ("both", C.PREC_SPLIT, C.GUESS_LEARNED)):
+        sc.set_modes(prec, guess)
+        runs[name] = sc.trace(o, d, 200, record=K)
+    sc.set_modes(C.PREC_FP64, C.GUESS_TRIANGLE)
+    plain = runs["plain"]
+    for name in ("learned", "split", "both"):
+        agree, err = _compare_traces(plain, runs[name], K)
+        assert agree >= 0.999, (name, agree)
+        assert err <= 1e-10, (name, err)
+    st_p, st_l, st_s, st_b = (runs[k]["stats"] for k in ("plain", "learned", "split", "both"))
+    # the network's start is used for most wavefront solves and rarely abandoned
+    assert st_l["guess_used"] > 0 and st_l["guess_fallback"] < 0.05 * st_l["guess_used"]
+    # the FP32 phase takes over most of the iterations from FP64 ...
+    assert st_s["newton_iters_fp32"] > 0 and st_s["newton_iters"] < 0.9 * st_p["newton_iters"]
+    # ... and starting it from the learned guess saves FP64 iterations again
+    assert st_b["newton_iters"] < st_s["newton_iters"]
