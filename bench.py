@@ -9,14 +9,19 @@ nodes, coarse grid 17 x 17 — lit by 1,048,576 seeded rays from z = 5 over
 [-3,3]^2 in a 10-degree cone about -z, at most 200 bounces, Newton tolerance
 1e-12.  One step = one bbrt_trace call over all rays.
 
-value     bounces of all rays / device time of the trace kernel (inputs already
-          in HBM; CUDA events on the launching stream; L2 flushed before each
-          step outside the timed events).
+value     bounces of all rays / device time of one step of the learned-guess
+          FP32/FP64 tracer (network trained on this GPU beforehand on a
+          separately seeded ray set; inputs already in HBM; CUDA events on the
+          launching stream; L2 flushed before each step outside the timed
+          events).  The plain FP64 form (the reference's arithmetic, stage-1
+          triangle start) and the split form alone are timed the same way and
+          reported under "forms"; "accuracy" compares the learned form with the
+          plain one ray by ray.
 e2e       the same metric through bbrt_trace with pinned host buffers: the
           host->device copy of the rays and the device->host copy of the
           per-ray results are inside the timed region.
-roofline  the trace kernel's dominant pipe (FP64: the path keeps every decision
-          in exact FP64) against the pipe peak measured in this process.
+roofline  the dominant kernel (k_advance: BVH traversal and stage 1, the same
+          in every form) against the pipe peaks measured in this process.
 cpu_baseline  the reference's own OpenMP trace loop (oracle/_ref), or the
           oracle port when the reference was not built, on a bounded sample
           of the same rays on all host cores (rank 0, N = 1 only).
@@ -57,7 +62,14 @@ def parse():
     ap.add_argument("--cull", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=8.0, help="target wall time of the CPU sample")
+    ap.add_argument("--train-rays", type=int, default=1 << 20, help="rays traced to record training samples")
+    ap.add_argument("--train-epochs", type=int, default=20)
+    ap.add_argument("--accuracy-rays", type=int, default=262144)
     return ap.parse_args()
+
+
+# plane height, half extent and cone half-angle of each workload's seeded source
+TRAIN_SOURCE = {"tetra_spheres": (5.0, 3.0, 10.0), "ellipsoids": (8.0, 6.0, 20.0)}
 
 
 def workload_config(name, n_rays, maxb, cn, tol, extra=None):
@@ -249,6 +261,70 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def _trace_form(scene, to, td, n, maxb, outs, stream, flush, steps, warmup, dev, world, clocks=None):
+    """Times `steps` device traces of the scene's current mode (after `warmup`
+    untimed ones); returns (kernel seconds, wall seconds, last stats)."""
+    import torch
+    stats = None
+    for _ in range(warmup):
+        stats = scene.trace_device(to.data_ptr(), td.data_ptr(), n, maxb, outs, stream=stream.cuda_stream,
+                                   want_stats=True)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    if clocks:
+        clocks.start()
+    torch.cuda.synchronize(dev)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    wall0 = time.perf_counter()
+    for k in range(steps):
+        flush.zero_()
+        evs[k][0].record(stream)
+        scene.trace_device(to.data_ptr(), td.data_ptr(), n, maxb, outs, stream=stream.cuda_stream)
+        evs[k][1].record(stream)
+    torch.cuda.synchronize(dev)
+    wall = time.perf_counter() - wall0
+    if world > 1:
+        dist.barrier()
+    return sum(a.elapsed_time(b) for a, b in evs) / 1e3, wall, stats
+
+
+def _max_over_ranks(kern_s, total_b, dev, world):
+    if world == 1:
+        return kern_s, total_b
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([kern_s], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    b = torch.tensor([total_b], dtype=torch.int64, device=dev)
+    dist.all_reduce(b, op=dist.ReduceOp.SUM)
+    return float(t.item()), int(b.item())
+
+
+def _accuracy(scene, o, d, maxb, C, K=8):
+    """The learned FP32/FP64 form against the plain FP64 form (bit-identical to
+    the reference) on the same rays: share of rays with the same status and
+    hit-object sequence, largest hit-point difference over those rays, and
+    Newton failures of each."""
+    outs = ("status", "bounce_count", "hit_object", "hit_point")
+    scene.set_modes(C.PREC_FP64, C.GUESS_TRIANGLE)
+    a = scene.trace(o, d, maxb, record=K, outputs=outs)
+    scene.set_modes(C.PREC_SPLIT, C.GUESS_LEARNED)
+    b = scene.trace(o, d, maxb, record=K, outputs=outs)
+    same = (a["status"] == b["status"]) & (a["bounce_count"] == b["bounce_count"])
+    same &= np.all(a["hit_object"] == b["hit_object"], axis=1)
+    mask = np.arange(K)[None, :] < np.minimum(a["bounce_count"], K)[:, None]
+    diff = np.abs(a["hit_point"] - b["hit_point"]).max(axis=2)
+    err = float(np.max(np.where(mask & same[:, None], diff, 0.0)))
+    newton_fail = lambda r: int(np.isin(r["status"], [C.RAY_NEWTON_SINGULAR, C.RAY_NEWTON_NOCONV,  # noqa: E731
+                                                      C.RAY_NEWTON_DOMAIN]).sum())
+    return {"rays": int(o.shape[0]), "sequence_agreement": float(np.mean(same)), "max_hit_err_agreeing": err,
+            "hit_err_bound": 1e-10, "within_bound": bool(err <= 1e-10),
+            "newton_failures_plain": newton_fail(a), "newton_failures_learned": newton_fail(b),
+            "compared": f"status, hit-object sequence and first {K} hit points vs the plain FP64 form"}
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     from billardballraytracing3d_b200 import _capi as C
@@ -273,6 +349,10 @@ def run_ours(args, rank, world, local_rank):
     C.check(lib, lib.bbrt_measure_pipe_peak(C.PIPE_L2, ctypes.byref(peak)), "bbrt_measure_pipe_peak")
     l2_peak = peak.value
 
+    # the learned guess: trained on this GPU on a separately seeded ray set of the same source
+    train_o, train_d = scenes.cone_rays(args.train_rays, 99 + rank, *TRAIN_SOURCE.get(args.workload, (5.0, 3.0, 10.0)))
+    training = scene.guess_train(train_o, train_d, maxb, epochs=args.train_epochs)
+
     to = torch.from_numpy(np.ascontiguousarray(o)).to(dev)
     td = torch.from_numpy(np.ascontiguousarray(d)).to(dev)
     st_ = torch.empty(n, dtype=torch.int32, device=dev)
@@ -285,41 +365,24 @@ def run_ours(args, rank, world, local_rank):
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
 
-    stats = None
-    for _ in range(args.warmup):
-        stats = scene.trace_device(to.data_ptr(), td.data_ptr(), n, maxb, outs, stream=stream.cuda_stream,
-                                   want_stats=True)
-    torch.cuda.synchronize(dev)
+    # the plain form (FP64, stage-1 triangle start: the reference's arithmetic)
+    scene.set_modes(C.PREC_FP64, C.GUESS_TRIANGLE)
+    p_s, _, p_stats = _trace_form(scene, to, td, n, maxb, outs, stream, flush, args.steps, args.warmup, dev, world)
+    plain_bounces = int(bc.sum().item())
+    p_s, p_b = _max_over_ranks(p_s, plain_bounces * args.steps, dev, world)
+    # the split form alone (FP32 Newton phase, triangle start)
+    scene.set_modes(C.PREC_SPLIT, C.GUESS_TRIANGLE)
+    s_s, _, s_stats = _trace_form(scene, to, td, n, maxb, outs, stream, flush, args.steps, args.warmup, dev, world)
+    s_s, s_b = _max_over_ranks(s_s, int(bc.sum().item()) * args.steps, dev, world)
+    # the headline: the learned-guess FP32/FP64 tracer
+    scene.set_modes(C.PREC_SPLIT, C.GUESS_LEARNED)
+    clocks = ClockSampler(local_rank)
+    kern_s, wall, stats = _trace_form(scene, to, td, n, maxb, outs, stream, flush, args.steps, args.warmup, dev,
+                                      world, clocks)
+    clk = clocks.stop()
     bounces_per_step = int(bc.sum().item())
     assert stats is None or stats["bounces"] == bounces_per_step
-
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
-    clocks = ClockSampler(local_rank)
-    clocks.start()
-    torch.cuda.synchronize(dev)
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    wall0 = time.perf_counter()
-    for k in range(args.steps):
-        flush.zero_()
-        evs[k][0].record(stream)
-        scene.trace_device(to.data_ptr(), td.data_ptr(), n, maxb, outs, stream=stream.cuda_stream)
-        evs[k][1].record(stream)
-    torch.cuda.synchronize(dev)
-    wall = time.perf_counter() - wall0
-    if world > 1:
-        dist.barrier()
-    clk = clocks.stop()
-    step_ms = [a.elapsed_time(b) for a, b in evs]
-    kern_s = sum(step_ms) / 1e3
-    total_b = bounces_per_step * args.steps
-    if world > 1:
-        t = torch.tensor([kern_s], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        b = torch.tensor([total_b], dtype=torch.int64, device=dev)
-        dist.all_reduce(b, op=dist.ReduceOp.SUM)
-        kern_s, total_b = float(t.item()), int(b.item())
+    kern_s, total_b = _max_over_ranks(kern_s, bounces_per_step * args.steps, dev, world)
     value = total_b / kern_s
 
     # e2e: host (pinned) buffers through the same C ABI call, copies inside the timed region
@@ -342,32 +405,40 @@ def run_ours(args, rank, world, local_rank):
                                     0, ctypes.byref(out), None, ctypes.c_void_p(stream.cuda_stream)), "bbrt_trace")
         if k > 0:
             e2e_s += time.perf_counter() - t0
-    e2e_b = int(hb.numpy().sum()) * e2e_steps
-    if world > 1:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        b = torch.tensor([e2e_b], dtype=torch.int64, device=dev)
-        dist.all_reduce(b, op=dist.ReduceOp.SUM)
-        e2e_s, e2e_b = float(t.item()), int(b.item())
+    e2e_s, e2e_b = _max_over_ranks(e2e_s, int(hb.numpy().sum()) * e2e_steps, dev, world)
     e2e = {"value": e2e_b / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(ho.numel() * 8 + hd.numel() * 8),
            "d2h_bytes_per_step": int(hs.numel() * 4 + hb.numel() * 4 + he.numel() * 8),
-           "note": "host wall clock around bbrt_trace with pinned host arrays (copies + kernel + sync)"}
+           "note": "host wall clock around bbrt_trace (learned FP32/FP64 form) with pinned host arrays "
+                   "(copies + kernels + sync)"}
 
     if rank != 0:
         return
+    accuracy = _accuracy(scene, o[:args.accuracy_rays], d[:args.accuracy_rays], maxb, C)
     per_launch_s = kern_s / args.steps
     roofline = advance_roofline(stats, fp64_peak, fp32_peak, l2_peak) if stats else None
+    form = lambda secs, b, st: {"value": b / secs, "unit": UNIT, "ms_per_step": 1e3 * secs / args.steps,  # noqa: E731
+                                "newton_iters_fp64": st["newton_iters"], "newton_iters_fp32": st["newton_iters_fp32"],
+                                "newton_ms": st["newton_ms"], "guess_ms": st["guess_ms"],
+                                "advance_ms": st["advance_ms"], "tail_ms": st["tail_ms"]}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * per_launch_s, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32 (BF16 MLP guess)", "data": "synthetic",
             "config": workload_config(args.workload, n, maxb, cn, tol,
                                       {"parallelism": "replicas" if world > 1 else "single GPU",
                                        "cull": args.cull,
+                                       "precision": "split: FP32 Newton phase to |F|<1e-5, FP64 finish",
+                                       "guess": "learned (BF16 MLP on tcgen05), triangle fallback",
                                        "l2": "flushed before each step (256 MiB write), flush outside the timed events",
                                        "bounces_per_step": bounces_per_step}),
+            "forms": {"plain_fp64_triangle": form(p_s, p_b, p_stats),
+                      "split_triangle": form(s_s, s_b, s_stats),
+                      "learned_split": form(kern_s, total_b, stats),
+                      "learned_over_plain": (total_b / kern_s) / (p_b / p_s)},
+            "accuracy": accuracy,
+            "guess_training": training,
             "e2e": e2e, "gpu_launches": int(stats["launches"]) * args.steps if stats else None,
             "roofline": roofline, "clocks": clk,
-            "kernel_ms_per_step": {k: stats[k] for k in ("order_ms", "advance_ms", "newton_ms", "tail_ms")}
+            "kernel_ms_per_step": {k: stats[k] for k in ("order_ms", "advance_ms", "guess_ms", "newton_ms", "tail_ms")}
             if stats else None,
             "wall_s_timed_region": wall,
             "counters_per_step": {k: v for k, v in (stats or {}).items() if k not in ("kernel_ms", "total_ms")}}
