@@ -34,7 +34,7 @@ namespace bbrt {
 cudaError_t launch_trace(const DScene& S, const TraceArgs& A, cudaStream_t stream, int sm_count);
 size_t wave_workspace_bytes(long long n);
 void wave_layout(void* ws, long long n, WaveArgs& W, NewtonRequest*& req_a, NewtonRequest*& req_b);
-cudaError_t launch_advance(const DScene& S, const TraceArgs& A, const WaveArgs& W, int sm_count,
+cudaError_t launch_advance(const DScene& S, const TraceArgs& A, const WaveArgs& W, int sm_count, int shape,
                            cudaStream_t stream);
 cudaError_t launch_newton(const DScene& S, const TraceArgs& A, const WaveArgs& W, long long n_req,
                           cudaStream_t stream);
@@ -259,8 +259,9 @@ int ensure_uploaded(bbrt_scene* s) {
             nlink[4 * h + 3] = 0;
         }
     }
-    // up to 96 KB of nodes (64 bytes each) in shared memory
-    D.smem_nodes = static_cast<int>(std::min<size_t>(nn, 1536));
+    // up to 3400 nodes (64 bytes each, 217 KB) in shared memory; launch shapes
+    // with several blocks per SM stage fewer
+    D.smem_nodes = static_cast<int>(std::min<size_t>(nn, 3400));
     std::vector<int> dims(2 * static_cast<size_t>(H.n_patches));
     for (int q = 0; q < H.n_patches; ++q) { dims[2 * q] = H.p_imax[q]; dims[2 * q + 1] = H.p_jmax[q]; }
     int rc;
@@ -411,6 +412,7 @@ struct Tuning {
     int order_rays = 1;               // bucket rays by origin / direction before round 0
     int log_rounds = 0;               // print per-round counts and times to stderr
     int warp_tail = 1;                // finish the tail one warp per ray (else one thread per ray)
+    int advance_shape = 3;            // k_advance launch shape (see launch_advance): 512 threads x 1 block per SM
 };
 
 // Launch-shape knobs; defaults tuned on B200, overridable for experiments by
@@ -424,6 +426,7 @@ const Tuning& tuning() {
         if (const char* e = std::getenv("BBRT_ORDER_RAYS")) v.order_rays = std::atoi(e);
         if (const char* e = std::getenv("BBRT_LOG_ROUNDS")) v.log_rounds = std::atoi(e);
         if (const char* e = std::getenv("BBRT_WARP_TAIL")) v.warp_tail = std::atoi(e);
+        if (const char* e = std::getenv("BBRT_ADV_SHAPE")) v.advance_shape = std::atoi(e);
         return v;
     }();
     return t;
@@ -485,7 +488,7 @@ int run_wavefront(bbrt_scene* s, const bbrt::TraceArgs& A, cudaStream_t st) {
         if (T.log_rounds) BBRT_CUDA(cudaEventRecord(s->ev[2], st));
         BBRT_CUDA(cudaMemsetAsync(W.counters, 0, sizeof(unsigned int), st));
         BBRT_CUDA(cudaMemsetAsync(W.counters + 2, 0, sizeof(unsigned int), st));
-        BBRT_CUDA(timed(s, K_ADVANCE, st, [&] { return bbrt::launch_advance(s->dev, A, W, s->sm_count, st); }));
+        BBRT_CUDA(timed(s, K_ADVANCE, st, [&] { return bbrt::launch_advance(s->dev, A, W, s->sm_count, T.advance_shape, st); }));
         ++s->rounds;
         if (T.log_rounds) BBRT_CUDA(cudaEventRecord(s->ev[3], st));
         BBRT_CUDA(cudaMemcpyAsync(s->wave_ctr_host, W.counters, 2 * sizeof(unsigned int), cudaMemcpyDeviceToHost, st));

@@ -563,7 +563,10 @@ __device__ __forceinline__ void stage1_tri(const double* __restrict__ X, const d
 // Advances runnable rays until each needs a Newton solve, overflows its
 // resolved list, or finishes.  Persistent: lanes fetch rays from the
 // runnable set until it is drained.
-__global__ void __launch_bounds__(128) k_advance(DScene S, TraceArgs A, WaveArgs W) {
+// NT threads per block, MINB blocks per SM requested from the register
+// allocator (launch shape variants of the same body).
+template <int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, WaveArgs W) {
     Counters ctr, cray;
     RayTally tally;
     NewtonRequest rq;
@@ -1248,20 +1251,41 @@ void wave_layout(void* ws, long long n, WaveArgs& W, NewtonRequest*& req_a, Newt
 
 size_t wave_workspace_bytes(long long n) { return wave_bytes_per_ray() * n + 16 * 256; }
 
-cudaError_t launch_advance(const DScene& S, const TraceArgs& A, const WaveArgs& W, int sm_count, cudaStream_t stream) {
-    if (W.n_runnable <= 0) return cudaSuccess;
-    const size_t smem = static_cast<size_t>(S.smem_nodes) * (6 * sizeof(double) + 4 * sizeof(int));
-    cudaError_t e = cudaFuncSetAttribute(k_advance, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+template <int NT, int MINB>
+static cudaError_t launch_advance_shape(const DScene& S, const TraceArgs& A, const WaveArgs& W, int sm_count,
+                                        int max_smem_nodes, cudaStream_t stream) {
+    DScene Sl = S;
+    if (Sl.smem_nodes > max_smem_nodes) Sl.smem_nodes = max_smem_nodes;
+    const size_t smem = static_cast<size_t>(Sl.smem_nodes) * (6 * sizeof(double) + 4 * sizeof(int));
+    cudaError_t e = cudaFuncSetAttribute(k_advance<NT, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_advance, 128, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_advance<NT, MINB>, NT, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
     long long blocks = static_cast<long long>(per_sm) * sm_count;
-    const long long need = (W.n_runnable + 127) / 128;
+    const long long need = (W.n_runnable + NT - 1) / NT;
     if (blocks > need) blocks = need;
-    k_advance<<<static_cast<unsigned>(blocks), 128, smem, stream>>>(S, A, W);
+    k_advance<NT, MINB><<<static_cast<unsigned>(blocks), NT, smem, stream>>>(Sl, A, W);
     return cudaGetLastError();
+}
+
+// Launch shapes of k_advance: 0 = 128 threads x 3 blocks per SM,
+// 1 = 256 threads x 2 blocks per SM, 2 = 128 threads x 4 blocks per SM (fewer
+// staged nodes), 3 / 4 / 5 / 6 = 512 / 768 / 1024 / 384 threads x 1 block per SM.
+cudaError_t launch_advance(const DScene& S, const TraceArgs& A, const WaveArgs& W, int sm_count, int shape,
+                           cudaStream_t stream) {
+    if (W.n_runnable <= 0) return cudaSuccess;
+    switch (shape) {
+        case 1: return launch_advance_shape<256, 2>(S, A, W, sm_count, 1536, stream);
+        case 2: return launch_advance_shape<128, 4>(S, A, W, sm_count, 864, stream);
+        case 3: return launch_advance_shape<512, 1>(S, A, W, sm_count, 3400, stream);
+        case 4: return launch_advance_shape<768, 1>(S, A, W, sm_count, 3400, stream);
+        case 5: return launch_advance_shape<1024, 1>(S, A, W, sm_count, 3400, stream);
+        case 6: return launch_advance_shape<384, 1>(S, A, W, sm_count, 3400, stream);
+        default: return launch_advance_shape<128, 3>(S, A, W, sm_count, 1536, stream);
+    }
 }
 
 cudaError_t launch_newton(const DScene& S, const TraceArgs& A, const WaveArgs& W, long long n_req, cudaStream_t stream) {
