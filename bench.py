@@ -64,7 +64,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=8.0, help="target wall time of the CPU sample")
     ap.add_argument("--train-rays", type=int, default=1 << 20, help="rays traced to record training samples")
     ap.add_argument("--train-epochs", type=int, default=20)
-    ap.add_argument("--accuracy-rays", type=int, default=262144)
+    ap.add_argument("--accuracy-rays", type=int, default=262144, help="0 skips the accuracy comparison")
+    ap.add_argument("--forms", default="plain,split,learned",
+                    help="forms to time besides the headline (learned); e.g. 'learned' alone for profiling")
     return ap.parse_args()
 
 
@@ -365,15 +367,20 @@ def run_ours(args, rank, world, local_rank):
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
 
+    forms = set(args.forms.split(","))
+    timed_forms = {}
     # the plain form (FP64, stage-1 triangle start: the reference's arithmetic)
-    scene.set_modes(C.PREC_FP64, C.GUESS_TRIANGLE)
-    p_s, _, p_stats = _trace_form(scene, to, td, n, maxb, outs, stream, flush, args.steps, args.warmup, dev, world)
-    plain_bounces = int(bc.sum().item())
-    p_s, p_b = _max_over_ranks(p_s, plain_bounces * args.steps, dev, world)
+    if "plain" in forms:
+        scene.set_modes(C.PREC_FP64, C.GUESS_TRIANGLE)
+        p_s, _, p_stats = _trace_form(scene, to, td, n, maxb, outs, stream, flush, args.steps, args.warmup, dev, world)
+        p_s, p_b = _max_over_ranks(p_s, int(bc.sum().item()) * args.steps, dev, world)
+        timed_forms["plain_fp64_triangle"] = (p_s, p_b, p_stats)
     # the split form alone (FP32 Newton phase, triangle start)
-    scene.set_modes(C.PREC_SPLIT, C.GUESS_TRIANGLE)
-    s_s, _, s_stats = _trace_form(scene, to, td, n, maxb, outs, stream, flush, args.steps, args.warmup, dev, world)
-    s_s, s_b = _max_over_ranks(s_s, int(bc.sum().item()) * args.steps, dev, world)
+    if "split" in forms:
+        scene.set_modes(C.PREC_SPLIT, C.GUESS_TRIANGLE)
+        s_s, _, s_stats = _trace_form(scene, to, td, n, maxb, outs, stream, flush, args.steps, args.warmup, dev, world)
+        s_s, s_b = _max_over_ranks(s_s, int(bc.sum().item()) * args.steps, dev, world)
+        timed_forms["split_triangle"] = (s_s, s_b, s_stats)
     # the headline: the learned-guess FP32/FP64 tracer
     scene.set_modes(C.PREC_SPLIT, C.GUESS_LEARNED)
     clocks = ClockSampler(local_rank)
@@ -413,7 +420,8 @@ def run_ours(args, rank, world, local_rank):
 
     if rank != 0:
         return
-    accuracy = _accuracy(scene, o[:args.accuracy_rays], d[:args.accuracy_rays], maxb, C)
+    accuracy = _accuracy(scene, o[:args.accuracy_rays], d[:args.accuracy_rays], maxb, C) if args.accuracy_rays > 0 \
+        else None
     per_launch_s = kern_s / args.steps
     roofline = advance_roofline(stats, fp64_peak, fp32_peak, l2_peak) if stats else None
     form = lambda secs, b, st: {"value": b / secs, "unit": UNIT, "ms_per_step": 1e3 * secs / args.steps,  # noqa: E731
@@ -430,10 +438,10 @@ def run_ours(args, rank, world, local_rank):
                                        "guess": "learned (BF16 MLP on tcgen05), triangle fallback",
                                        "l2": "flushed before each step (256 MiB write), flush outside the timed events",
                                        "bounces_per_step": bounces_per_step}),
-            "forms": {"plain_fp64_triangle": form(p_s, p_b, p_stats),
-                      "split_triangle": form(s_s, s_b, s_stats),
-                      "learned_split": form(kern_s, total_b, stats),
-                      "learned_over_plain": (total_b / kern_s) / (p_b / p_s)},
+            "forms": dict({k: form(*v) for k, v in timed_forms.items()}, learned_split=form(kern_s, total_b, stats),
+                          learned_over_plain=(value / (timed_forms["plain_fp64_triangle"][1] /
+                                                       timed_forms["plain_fp64_triangle"][0])
+                                              if "plain_fp64_triangle" in timed_forms else None)),
             "accuracy": accuracy,
             "guess_training": training,
             "e2e": e2e, "gpu_launches": int(stats["launches"]) * args.steps if stats else None,
