@@ -389,7 +389,7 @@ enum { K_ORDER = 0, K_ADVANCE = 1, K_NEWTON = 2, K_TAIL = 3, K_GUESS = 4 };
 // Records a pair of events around one launch when the call collects statistics.
 template <class F>
 cudaError_t timed(bbrt_scene* s, int kind, cudaStream_t st, F&& launch) {
-    s->launches += (kind == K_ORDER) ? 3 : 1;   // ray ordering is three kernels
+    s->launches += (kind == K_ORDER) ? 4 : 1;   // ray ordering is four kernels
     if (!s->timing || s->kev_used + 2 > bbrt_scene::kTimerEvents) return launch();
     const int k = s->kev_used;
     cudaError_t e = cudaEventRecord(s->kev[k], st);

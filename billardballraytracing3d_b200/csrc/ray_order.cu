@@ -3,7 +3,7 @@
 // Rays are bucketed by an 18-bit key — the octant of the direction (3 bits)
 // over a 15-bit Morton code of the origin quantised to 32 cells per axis
 // inside a cube of four scene radii — with a counting sort: histogram,
-// exclusive scan, scatter.  Warps then hold rays that start close together
+// exclusive scan (two passes), scatter.  Warps then hold rays that start close together
 // and head the same way, so their BVH walks and stage-1 patch tests follow
 // the same paths.  Only the order in which rays are processed changes; every
 // ray's result is written to its own index.
@@ -47,28 +47,62 @@ __global__ void k_order_hist(const double* __restrict__ o, const double* __restr
     atomicAdd(hist + k, 1u);
 }
 
-// Exclusive scan of kOrderBuckets counts by one block of 1024 threads.
-__global__ void __launch_bounds__(1024) k_order_scan(unsigned* __restrict__ hist) {
-    constexpr int per = kOrderBuckets / 1024;
-    __shared__ unsigned part[1024];
-    const int t = threadIdx.x;
-    unsigned* h = hist + t * per;
-    unsigned s = 0;
-    for (int k = 0; k < per; ++k) s += h[k];
-    part[t] = s;
+// Exclusive scan of the kOrderBuckets counts in two passes of
+// kOrderBuckets / 1024 blocks: each block scans its 1024 counts in place and
+// records their total; then each block adds the totals of the blocks before it.
+constexpr int kScanBlock = 1024;
+constexpr int kScanBlocks = kOrderBuckets / kScanBlock;
+
+// Block-wide exclusive scan of one value per thread (1024 threads); *total
+// receives the block's sum.
+__device__ __forceinline__ unsigned block_exclusive_scan(unsigned v, unsigned* warp_sums, unsigned* total) {
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    unsigned x = v;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const unsigned y = __shfl_up_sync(0xffffffffu, x, off);
+        if (lane >= off) x += y;
+    }
+    if (lane == 31) warp_sums[w] = x;
     __syncthreads();
-    for (int off = 1; off < 1024; off <<= 1) {
-        const unsigned v = (t >= off) ? part[t - off] : 0u;
-        __syncthreads();
-        part[t] += v;
-        __syncthreads();
+    if (w == 0) {
+        unsigned s = warp_sums[lane];
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const unsigned y = __shfl_up_sync(0xffffffffu, s, off);
+            if (lane >= off) s += y;
+        }
+        warp_sums[lane] = s;   // inclusive prefix of the warp totals
     }
-    unsigned run = part[t] - s;
-    for (int k = 0; k < per; ++k) {
-        const unsigned c = h[k];
-        h[k] = run;
-        run += c;
-    }
+    __syncthreads();
+    if (total) *total = warp_sums[31];
+    return x - v + (w > 0 ? warp_sums[w - 1] : 0u);
+}
+
+__global__ void __launch_bounds__(kScanBlock) k_order_scan_local(unsigned* __restrict__ hist,
+                                                                 unsigned* __restrict__ block_sums) {
+    __shared__ unsigned ws[32];
+    __shared__ unsigned total;
+    unsigned* h = hist + blockIdx.x * kScanBlock;
+    const unsigned v = h[threadIdx.x];
+    const unsigned ex = block_exclusive_scan(v, ws, &total);
+    h[threadIdx.x] = ex;
+    if (threadIdx.x == 0) block_sums[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kScanBlock) k_order_scan_add(unsigned* __restrict__ hist,
+                                                               const unsigned* __restrict__ block_sums) {
+    __shared__ unsigned part[32];
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    // sum of the totals of blocks [0, blockIdx.x)
+    unsigned v = (t < static_cast<int>(blockIdx.x)) ? block_sums[t] : 0u;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    if (lane == 0) part[w] = v;
+    __syncthreads();
+    unsigned base = 0;
+    for (int k = 0; k < 32; ++k) base += part[k];
+    hist[blockIdx.x * kScanBlock + t] += base;
 }
 
 __global__ void k_order_scatter(const unsigned* __restrict__ keys, long long n, unsigned* __restrict__ cursor,
@@ -80,7 +114,7 @@ __global__ void k_order_scatter(const unsigned* __restrict__ keys, long long n, 
 }
 
 size_t ray_order_workspace_bytes(long long n) {
-    return sizeof(unsigned) * (static_cast<size_t>(n) + kOrderBuckets) + 512;
+    return sizeof(unsigned) * (static_cast<size_t>(n) + kOrderBuckets + kScanBlocks) + 512;
 }
 
 // order[n] receives the processing order.  `ws` holds ray_order_workspace_bytes(n).
@@ -88,13 +122,15 @@ cudaError_t ray_order(const double* o, const double* d, long long n, const doubl
                       void* ws, int* order, cudaStream_t stream) {
     if (n <= 0) return cudaSuccess;
     unsigned* hist = static_cast<unsigned*>(ws);
-    unsigned* keys = hist + kOrderBuckets;
+    unsigned* block_sums = hist + kOrderBuckets;
+    unsigned* keys = block_sums + kScanBlocks;
     cudaError_t e = cudaMemsetAsync(hist, 0, sizeof(unsigned) * kOrderBuckets, stream);
     if (e != cudaSuccess) return e;
     const double inv_span = radius > 0.0 ? 1.0 / (4.0 * radius) : 1.0;
     const unsigned blocks = static_cast<unsigned>((n + 255) / 256);
     k_order_hist<<<blocks, 256, 0, stream>>>(o, d, n, center[0], center[1], center[2], inv_span, keys, hist);
-    k_order_scan<<<1, 1024, 0, stream>>>(hist);
+    k_order_scan_local<<<kScanBlocks, kScanBlock, 0, stream>>>(hist, block_sums);
+    k_order_scan_add<<<kScanBlocks, kScanBlock, 0, stream>>>(hist, block_sums);
     k_order_scatter<<<blocks, 256, 0, stream>>>(keys, n, hist, order);
     return cudaGetLastError();
 }
