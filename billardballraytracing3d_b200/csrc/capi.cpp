@@ -413,6 +413,7 @@ struct Tuning {
     int log_rounds = 0;               // print per-round counts and times to stderr
     int warp_tail = 1;                // finish the tail one warp per ray (else one thread per ray)
     int advance_shape = 3;            // k_advance launch shape (see launch_advance): 512 threads x 1 block per SM
+    int warp_stage1 = 1;              // k_advance runs each patch's stage 1 with the whole warp
 };
 
 // Launch-shape knobs; defaults tuned on B200, overridable for experiments by
@@ -427,6 +428,7 @@ const Tuning& tuning() {
         if (const char* e = std::getenv("BBRT_LOG_ROUNDS")) v.log_rounds = std::atoi(e);
         if (const char* e = std::getenv("BBRT_WARP_TAIL")) v.warp_tail = std::atoi(e);
         if (const char* e = std::getenv("BBRT_ADV_SHAPE")) v.advance_shape = std::atoi(e);
+        if (const char* e = std::getenv("BBRT_WARP_S1")) v.warp_stage1 = std::atoi(e);
         return v;
     }();
     return t;
@@ -467,6 +469,7 @@ int run_wavefront(bbrt_scene* s, const bbrt::TraceArgs& A, cudaStream_t st) {
     bbrt::NewtonRequest *req_a = nullptr, *req_b = nullptr;
     bbrt::wave_layout(s->wave.p, n, W, req_a, req_b);
     W.counters = static_cast<unsigned int*>(s->wave_ctr.p);
+    W.warp_stage1 = T.warp_stage1;
     W.runnable = nullptr;
     W.n_runnable = n;
     W.req = req_a;

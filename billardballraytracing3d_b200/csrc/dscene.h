@@ -140,6 +140,7 @@ struct WaveArgs {
     const double* frame = nullptr;             // per-patch frames (size L at [12] of each 16)
     double guess_min_logit = 0.0;              // confidence needed to start Newton from the guess
     double guess_t_window = 0.5;               // accepted |t - t_stage1| in units of L
+    int warp_stage1 = 1;                       // stage 1 of k_advance by the whole warp (else per lane)
 };
 
 struct QueryArgs {

@@ -474,6 +474,105 @@ __device__ __forceinline__ void record_sample(const TraceArgs& A, int label, con
     s->label = label;
 }
 
+// One of the six Moller-Trumbore tests of cell (i, j): step = 2 * sign + triangle,
+// sign order 0, +1, -1 of the sagitta along the cell normal, triangles
+// (q00,q10,q11) then (q00,q11,q01) — the order and arithmetic of stage1_cell.
+__device__ __forceinline__ void stage1_tri(const double* __restrict__ X, const double* __restrict__ CC, int n, int i,
+                                           int j, int step, const V3& o, const V3& d, Stage1& best) {
+    const int nc = n - 1;
+    const double* r0 = X + static_cast<long long>(i * n + j) * 3;
+    const double* r1 = r0 + 3 * n;
+    const double* c = CC + static_cast<long long>(i * nc + j) * 4;
+    const V3 cn = v3(c[0], c[1], c[2]);
+    const int k = step >> 1;
+    const double sg = (k == 0) ? 0.0 : ((k == 1) ? 1.0 : -1.0);
+    const double dd = sg * c[3];
+    const V3 p00 = load3(r0), p11 = load3(r1 + 3);
+    const V3 pm = (step & 1) ? load3(r0 + 3) : load3(r1);   // p01 for the second triangle, p10 for the first
+    const V3 q00 = v3(p00.x + cn.x * dd, p00.y + cn.y * dd, p00.z + cn.z * dd);
+    const V3 q11 = v3(p11.x + cn.x * dd, p11.y + cn.y * dd, p11.z + cn.z * dd);
+    const V3 qm = v3(pm.x + cn.x * dd, pm.y + cn.y * dd, pm.z + cn.z * dd);
+    double t;
+    const bool hit = (step & 1) ? mt_exact(o, d, q00, q11, qm, t) : mt_exact(o, d, q00, qm, q11, t);
+    if (hit) best.consider(t, (i * nc + j) * 6 + step);
+}
+
+// ---- warp-cooperative stage 1 (used by k_advance and the warp-per-ray tail) ----
+
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ void warp_min_stage1(Stage1& s) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const int oh = __shfl_xor_sync(kFull, s.have ? 1 : 0, off);
+        const double ot = __shfl_xor_sync(kFull, s.t, off);
+        const int ok = __shfl_xor_sync(kFull, s.key, off);
+        if (oh) s.consider(ot, ok);
+    }
+}
+
+// Lane `lane` runs the `k`-th of the six triangle tests of each passing cell in
+// `cm` (cells enumerated by the set bits of cm, offsets into (ci0, cj0) grid of
+// width w), 32 tests at a time.
+__device__ __forceinline__ void warp_cell_tris(const double* X, const double* CC, int n, unsigned cm, int base_i,
+                                               int base_j, int w, int c0, const V3& o, const V3& d, int lane,
+                                               Stage1& best) {
+    const int total = __popc(cm) * 6;
+    for (int p0 = 0; p0 < total; p0 += 32) {
+        const int p = p0 + lane;
+        if (p < total) {
+            const int bit = __fns(cm, 0, p / 6 + 1);
+            const int c = c0 + bit;
+            stage1_tri(X, CC, n, base_i + c / w, base_j + c % w, p % 6, o, d, best);
+        }
+    }
+}
+
+__device__ Stage1 warp_patch_stage1(const DScene& S, int pidx, const V3& o, const V3& d, bool use_cull,
+                                    const CullRay& cr, int lane, Counters& ctr) {
+    const int n = S.coarse_n, nc = n - 1;
+    const double* X = S.c_xyz + static_cast<long long>(pidx) * n * n * 3;
+    const double* CC = S.c_cell + static_cast<long long>(pidx) * nc * nc * 4;
+    Stage1 best;
+    if (lane == 0) ++ctr.patch_tests;
+    if (!(finite3(o) && finite3(d))) {
+        // ordered loop on every lane (same result everywhere)
+        Counters dummy;
+        best = patch_stage1(S, pidx, o, d, false, cr, dummy);
+        if (lane == 0) ctr.tri_tests += 6LL * nc * nc;
+        return best;
+    }
+    if (use_cull) {
+        const int B = S.block_cells, NB = S.n_blocks_side, NB2 = NB * NB;
+        const float* BB = S.c_block_box + static_cast<long long>(pidx) * NB2 * 6;
+        const float* CB = S.c_cell_box + static_cast<long long>(pidx) * nc * nc * 6;
+        for (int b0 = 0; b0 < NB2; b0 += 32) {
+            const int b = b0 + lane;
+            unsigned bm = __ballot_sync(kFull, b < NB2 && cull_box(BB + b * 6, cr));
+            if (lane == 0) ctr.cell_tests += min(32, NB2 - b0);
+            while (bm) {
+                const int bl = __ffs(bm) - 1;
+                bm &= bm - 1;
+                const int bi = (b0 + bl) / NB, bj = (b0 + bl) % NB;
+                const int i0 = bi * B, j0 = bj * B;
+                const int h = min(nc, i0 + B) - i0, w = min(nc, j0 + B) - j0;
+                for (int c0 = 0; c0 < h * w; c0 += 32) {
+                    const int c = c0 + lane;
+                    const unsigned cm = __ballot_sync(kFull, c < h * w && cull_box(CB + ((i0 + c / w) * nc + j0 + c % w) * 6, cr));
+                    if (lane == 0) { ctr.cell_tests += min(32, h * w - c0); ctr.tri_tests += 6 * __popc(cm); }
+                    warp_cell_tris(X, CC, n, cm, i0, j0, w, c0, o, d, lane, best);
+                }
+            }
+        }
+    } else {
+        const int total = nc * nc * 6;
+        for (int p = lane; p < total; p += 32) stage1_tri(X, CC, n, (p / 6) / nc, (p / 6) % nc, p % 6, o, d, best);
+        if (lane == 0) ctr.tri_tests += total;
+    }
+    warp_min_stage1(best);
+    return best;
+}
+
 // Advance-kernel modes.  The kernel is persistent: each lane owns one ray at
 // a time and the body is one flat loop in which every iteration does one
 // small unit of work for the lane's ray (one BVH node test, one leaf object,
@@ -489,12 +588,13 @@ enum AdvMode {
     M_CELL_ALL = 4,  // next cell, culling off
     M_TRI = 5,       // next of the six triangle tests of a cell
     M_S1_DONE = 6,   // stage 1 of the current patch finished
-    M_RESOLVE = 7,   // query finished: bounce, escape or error
-    M_FINISH = 8,    // ray finished
-    M_SUSPEND = 9,   // waiting for a Newton solve
-    M_OVERFLOW = 10, // more solves than the resolved list holds
-    M_IDLE = 11,     // lane has no ray
-    M_DRAINED = 12   // no runnable ray left
+    M_S1_WARP = 7,   // stage 1 of the current patch waits for the whole warp
+    M_RESOLVE = 8,   // query finished: bounce, escape or error
+    M_FINISH = 9,    // ray finished
+    M_SUSPEND = 10,  // waiting for a Newton solve
+    M_OVERFLOW = 11, // more solves than the resolved list holds
+    M_IDLE = 12,     // lane has no ray
+    M_DRAINED = 13   // no runnable ray left
 };
 
 struct AdvState {
@@ -537,29 +637,6 @@ __device__ __forceinline__ void adv_start_query(const DScene& S, const TraceArgs
     stack[q.sp++] = 0;
 }
 
-// One of the six Moller-Trumbore tests of cell (i, j): step = 2 * sign + triangle,
-// sign order 0, +1, -1 of the sagitta along the cell normal, triangles
-// (q00,q10,q11) then (q00,q11,q01) — the order and arithmetic of stage1_cell.
-__device__ __forceinline__ void stage1_tri(const double* __restrict__ X, const double* __restrict__ CC, int n, int i,
-                                           int j, int step, const V3& o, const V3& d, Stage1& best) {
-    const int nc = n - 1;
-    const double* r0 = X + static_cast<long long>(i * n + j) * 3;
-    const double* r1 = r0 + 3 * n;
-    const double* c = CC + static_cast<long long>(i * nc + j) * 4;
-    const V3 cn = v3(c[0], c[1], c[2]);
-    const int k = step >> 1;
-    const double sg = (k == 0) ? 0.0 : ((k == 1) ? 1.0 : -1.0);
-    const double dd = sg * c[3];
-    const V3 p00 = load3(r0), p11 = load3(r1 + 3);
-    const V3 pm = (step & 1) ? load3(r0 + 3) : load3(r1);   // p01 for the second triangle, p10 for the first
-    const V3 q00 = v3(p00.x + cn.x * dd, p00.y + cn.y * dd, p00.z + cn.z * dd);
-    const V3 q11 = v3(p11.x + cn.x * dd, p11.y + cn.y * dd, p11.z + cn.z * dd);
-    const V3 qm = v3(pm.x + cn.x * dd, pm.y + cn.y * dd, pm.z + cn.z * dd);
-    double t;
-    const bool hit = (step & 1) ? mt_exact(o, d, q00, q11, qm, t) : mt_exact(o, d, q00, qm, q11, t);
-    if (hit) best.consider(t, (i * nc + j) * 6 + step);
-}
-
 // Advances runnable rays until each needs a Newton solve, overflows its
 // resolved list, or finishes.  Persistent: lanes fetch rays from the
 // runnable set until it is drained.
@@ -578,6 +655,7 @@ __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, Wav
     AdvState q;
     int stack[64];
     const int n = S.coarse_n, nc = n - 1, NB = S.n_blocks_side, B = S.block_cells;
+    const int lane = threadIdx.x & 31;
     // The first S.smem_nodes BVH nodes (breadth-first order: the top levels)
     // are staged in shared memory for the whole launch.
     extern __shared__ double smem_bvh[];
@@ -651,6 +729,10 @@ __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, Wav
                             }
                             ++q.leaf_k;
                         }
+                    } else if (W.warp_stage1) {
+                        q.obj = obj;
+                        q.pidx = S.obj_sub[obj];
+                        mode = M_S1_WARP;
                     } else {
                         q.obj = obj;
                         q.pidx = S.obj_sub[obj];
@@ -767,6 +849,46 @@ __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, Wav
             } else {
                 adv_start_query(S, A, r, q, stack);
                 mode = M_NODE;
+            }
+        }
+        // Stage 1 of every lane that reached a patch, one patch at a time with
+        // all 32 lanes: the block, cell and triangle tests of the patch are
+        // split over the lanes and the (t, key) minimum is taken over the warp
+        // (the same winner as the lane's own ordered loop).
+        if (W.warp_stage1) {
+            unsigned pend = __ballot_sync(kFull, mode == M_S1_WARP);
+            while (pend) {
+                const int src = __ffs(pend) - 1;
+                pend &= pend - 1;
+                V3 so, sd;
+                so.x = __shfl_sync(kFull, r.o.x, src);
+                so.y = __shfl_sync(kFull, r.o.y, src);
+                so.z = __shfl_sync(kFull, r.o.z, src);
+                sd.x = __shfl_sync(kFull, r.d.x, src);
+                sd.y = __shfl_sync(kFull, r.d.y, src);
+                sd.z = __shfl_sync(kFull, r.d.z, src);
+                const int spidx = __shfl_sync(kFull, q.pidx, src);
+                const bool scull = __shfl_sync(kFull, q.use_cull ? 1 : 0, src) != 0;
+                CullRay scr;
+                scr.ox = __shfl_sync(kFull, q.cr.ox, src);
+                scr.oy = __shfl_sync(kFull, q.cr.oy, src);
+                scr.oz = __shfl_sync(kFull, q.cr.oz, src);
+                scr.ix = __shfl_sync(kFull, q.cr.ix, src);
+                scr.iy = __shfl_sync(kFull, q.cr.iy, src);
+                scr.iz = __shfl_sync(kFull, q.cr.iz, src);
+                scr.delta = __shfl_sync(kFull, q.cr.delta, src);
+                Counters c2;
+                const Stage1 res = warp_patch_stage1(S, spidx, so, sd, scull, scr, lane, c2);
+                const long long pt = __shfl_sync(kFull, c2.patch_tests, 0);
+                const long long ct = __shfl_sync(kFull, c2.cell_tests, 0);
+                const long long tt = __shfl_sync(kFull, c2.tri_tests, 0);
+                if (lane == src) {
+                    q.s1 = res;
+                    cray.patch_tests += pt;
+                    cray.cell_tests += ct;
+                    cray.tri_tests += tt;
+                    mode = M_S1_DONE;
+                }
             }
         }
         // Only when some lane's ray left its working modes (one vote in the
@@ -917,80 +1039,6 @@ __global__ void __launch_bounds__(128) k_resume(DScene S, TraceArgs A, WaveArgs 
 // triangle tests of a patch are split over the lanes and the winner is the
 // (t, key) minimum over the warp, which is what the reference's ordered loop
 // keeps for finite t.  Non-finite rays take the ordered per-lane loop.
-
-constexpr unsigned kFull = 0xffffffffu;
-
-__device__ __forceinline__ void warp_min_stage1(Stage1& s) {
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-        const int oh = __shfl_xor_sync(kFull, s.have ? 1 : 0, off);
-        const double ot = __shfl_xor_sync(kFull, s.t, off);
-        const int ok = __shfl_xor_sync(kFull, s.key, off);
-        if (oh) s.consider(ot, ok);
-    }
-}
-
-// Lane `lane` runs the `k`-th of the six triangle tests of each passing cell in
-// `cm` (cells enumerated by the set bits of cm, offsets into (ci0, cj0) grid of
-// width w), 32 tests at a time.
-__device__ __forceinline__ void warp_cell_tris(const double* X, const double* CC, int n, unsigned cm, int base_i,
-                                               int base_j, int w, int c0, const V3& o, const V3& d, int lane,
-                                               Stage1& best) {
-    const int total = __popc(cm) * 6;
-    for (int p0 = 0; p0 < total; p0 += 32) {
-        const int p = p0 + lane;
-        if (p < total) {
-            const int bit = __fns(cm, 0, p / 6 + 1);
-            const int c = c0 + bit;
-            stage1_tri(X, CC, n, base_i + c / w, base_j + c % w, p % 6, o, d, best);
-        }
-    }
-}
-
-__device__ Stage1 warp_patch_stage1(const DScene& S, int pidx, const V3& o, const V3& d, bool use_cull,
-                                    const CullRay& cr, int lane, Counters& ctr) {
-    const int n = S.coarse_n, nc = n - 1;
-    const double* X = S.c_xyz + static_cast<long long>(pidx) * n * n * 3;
-    const double* CC = S.c_cell + static_cast<long long>(pidx) * nc * nc * 4;
-    Stage1 best;
-    if (lane == 0) ++ctr.patch_tests;
-    if (!(finite3(o) && finite3(d))) {
-        // ordered loop on every lane (same result everywhere)
-        Counters dummy;
-        best = patch_stage1(S, pidx, o, d, false, cr, dummy);
-        if (lane == 0) ctr.tri_tests += 6LL * nc * nc;
-        return best;
-    }
-    if (use_cull) {
-        const int B = S.block_cells, NB = S.n_blocks_side, NB2 = NB * NB;
-        const float* BB = S.c_block_box + static_cast<long long>(pidx) * NB2 * 6;
-        const float* CB = S.c_cell_box + static_cast<long long>(pidx) * nc * nc * 6;
-        for (int b0 = 0; b0 < NB2; b0 += 32) {
-            const int b = b0 + lane;
-            unsigned bm = __ballot_sync(kFull, b < NB2 && cull_box(BB + b * 6, cr));
-            if (lane == 0) ctr.cell_tests += min(32, NB2 - b0);
-            while (bm) {
-                const int bl = __ffs(bm) - 1;
-                bm &= bm - 1;
-                const int bi = (b0 + bl) / NB, bj = (b0 + bl) % NB;
-                const int i0 = bi * B, j0 = bj * B;
-                const int h = min(nc, i0 + B) - i0, w = min(nc, j0 + B) - j0;
-                for (int c0 = 0; c0 < h * w; c0 += 32) {
-                    const int c = c0 + lane;
-                    const unsigned cm = __ballot_sync(kFull, c < h * w && cull_box(CB + ((i0 + c / w) * nc + j0 + c % w) * 6, cr));
-                    if (lane == 0) { ctr.cell_tests += min(32, h * w - c0); ctr.tri_tests += 6 * __popc(cm); }
-                    warp_cell_tris(X, CC, n, cm, i0, j0, w, c0, o, d, lane, best);
-                }
-            }
-        }
-    } else {
-        const int total = nc * nc * 6;
-        for (int p = lane; p < total; p += 32) stage1_tri(X, CC, n, (p / 6) / nc, (p / 6) % nc, p % 6, o, d, best);
-        if (lane == 0) ctr.tri_tests += total;
-    }
-    warp_min_stage1(best);
-    return best;
-}
 
 // BVH::intersect for one ray with a whole warp (every lane returns the same result).
 __device__ QHit warp_bvh_query(const DScene& S, const V3& o, const V3& d, int cull_flag, int lane, Counters& ctr) {
