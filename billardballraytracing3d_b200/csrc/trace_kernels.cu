@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 #include <math_constants.h>
 
+#include <algorithm>
 #include <mutex>
 
 #include "../../include/bbrt.h"
@@ -1312,10 +1313,16 @@ static cudaError_t launch_advance_shape(const DScene& S, const TraceArgs& A, con
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_advance<NT, MINB>, NT, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
+    // A small round (the late ones) is spread over every SM with smaller
+    // blocks rather than packed into the first few SMs with full ones.
+    int threads = NT;
+    const long long per_block = (W.n_runnable + static_cast<long long>(per_sm) * sm_count - 1) /
+                                (static_cast<long long>(per_sm) * sm_count);
+    if (per_block < NT) threads = static_cast<int>(std::max<long long>(32, (per_block + 31) / 32 * 32));
     long long blocks = static_cast<long long>(per_sm) * sm_count;
-    const long long need = (W.n_runnable + NT - 1) / NT;
+    const long long need = (W.n_runnable + threads - 1) / threads;
     if (blocks > need) blocks = need;
-    k_advance<NT, MINB><<<static_cast<unsigned>(blocks), NT, smem, stream>>>(Sl, A, W);
+    k_advance<NT, MINB><<<static_cast<unsigned>(blocks), threads, smem, stream>>>(Sl, A, W);
     return cudaGetLastError();
 }
 
