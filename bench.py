@@ -65,6 +65,7 @@ def parse():
     ap.add_argument("--train-rays", type=int, default=1 << 20, help="rays traced to record training samples")
     ap.add_argument("--train-epochs", type=int, default=20)
     ap.add_argument("--accuracy-rays", type=int, default=262144, help="0 skips the accuracy comparison")
+    ap.add_argument("--autotune", type=int, default=1, help="pick the launch schedule on the workload first")
     ap.add_argument("--forms", default="plain,split,learned",
                     help="forms to time besides the headline (learned); e.g. 'learned' alone for profiling")
     return ap.parse_args()
@@ -351,6 +352,8 @@ def run_ours(args, rank, world, local_rank):
     C.check(lib, lib.bbrt_measure_pipe_peak(C.PIPE_L2, ctypes.byref(peak)), "bbrt_measure_pipe_peak")
     l2_peak = peak.value
 
+    # launch schedule picked on the workload itself (plain form; results do not depend on it)
+    tuned = scene.autotune(o, d, maxb, trials=2) if args.autotune else scene.tuning()
     # the learned guess: trained on this GPU on a separately seeded ray set of the same source
     train_o, train_d = scenes.cone_rays(args.train_rays, 99 + rank, *TRAIN_SOURCE.get(args.workload, (5.0, 3.0, 10.0)))
     training = scene.guess_train(train_o, train_d, maxb, epochs=args.train_epochs)
@@ -436,6 +439,7 @@ def run_ours(args, rank, world, local_rank):
                                        "cull": args.cull,
                                        "precision": "split: FP32 Newton phase to |F|<1e-5, FP64 finish",
                                        "guess": "learned (BF16 MLP on tcgen05), triangle fallback",
+                                       "schedule": tuned,
                                        "l2": "flushed before each step (256 MiB write), flush outside the timed events",
                                        "bounces_per_step": bounces_per_step}),
             "forms": dict({k: form(*v) for k, v in timed_forms.items()}, learned_split=form(kern_s, total_b, stats),

@@ -174,6 +174,16 @@ class TraceStats(ctypes.Structure):
         return d
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [
+        ("advance_shape", ctypes.c_int), ("warp_stage1", ctypes.c_int), ("order_rays", ctypes.c_int),
+        ("warp_tail", ctypes.c_int), ("wave_tail", ctypes.c_longlong), ("wave_min_rays", ctypes.c_longlong),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class GuessTrainConfig(ctypes.Structure):
     _fields_ = [
         ("epochs", ctypes.c_int), ("batch", ctypes.c_int), ("lr", ctypes.c_float),
@@ -279,6 +289,9 @@ def _declare(lib):
     lib.bbrt_umma_check.argtypes = [ctypes.POINTER(ctypes.c_ushort), ctypes.POINTER(ctypes.c_ushort),
                                     ctypes.POINTER(ctypes.c_float)]
     lib.bbrt_scene_set_modes.argtypes = [V, I, I]
+    lib.bbrt_scene_get_tuning.argtypes = [V, ctypes.POINTER(Tuning)]
+    lib.bbrt_scene_set_tuning.argtypes = [V, ctypes.POINTER(Tuning)]
+    lib.bbrt_scene_autotune.argtypes = [V, c_double_p, c_double_p, LL, I, I, ctypes.POINTER(Tuning), c_double_p, V]
     lib.bbrt_guess_train_config_init.argtypes = [ctypes.POINTER(GuessTrainConfig)]
     lib.bbrt_guess_train_config_init.restype = None
     lib.bbrt_guess_train.argtypes = [V, c_double_p, c_double_p, LL, I, ctypes.POINTER(GuessTrainConfig),

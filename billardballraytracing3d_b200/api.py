@@ -174,6 +174,29 @@ class Scene:
         """Arithmetic mode (PREC_FP64 / PREC_SPLIT) and Newton start (GUESS_TRIANGLE / GUESS_LEARNED)."""
         C.check(self.lib, self.lib.bbrt_scene_set_modes(self.h, int(precision), int(guess)), "bbrt_scene_set_modes")
 
+    def tuning(self, **set_fields) -> Dict:
+        """The scene's launch schedule; keyword arguments change fields of it first."""
+        t = C.Tuning()
+        C.check(self.lib, self.lib.bbrt_scene_get_tuning(self.h, ctypes.byref(t)), "bbrt_scene_get_tuning")
+        if set_fields:
+            for k, v in set_fields.items():
+                if not hasattr(t, k):
+                    raise KeyError(k)
+                setattr(t, k, v)
+            C.check(self.lib, self.lib.bbrt_scene_set_tuning(self.h, ctypes.byref(t)), "bbrt_scene_set_tuning")
+        return t.as_dict()
+
+    def autotune(self, origins, dirs, max_bounces: int, trials: int = 2) -> Dict:
+        """Picks the fastest launch schedule on these rays; returns it with its time."""
+        o = np.ascontiguousarray(origins, dtype=np.float64)
+        d = np.ascontiguousarray(dirs, dtype=np.float64)
+        t = C.Tuning()
+        ms = ctypes.c_double()
+        C.check(self.lib, self.lib.bbrt_scene_autotune(self.h, C.ptr(o), C.ptr(d), o.shape[0], int(max_bounces),
+                                                       int(trials), ctypes.byref(t), ctypes.byref(ms), None),
+                "bbrt_scene_autotune")
+        return dict(t.as_dict(), ms=ms.value)
+
     def guess_train(self, origins, dirs, max_bounces: int, **kw) -> Dict:
         """Records training samples from a plain trace of these rays and trains
         the learned-guess network on the GPU; returns the training report."""

@@ -49,6 +49,10 @@ cudaError_t launch_query(const DScene& S, const QueryArgs& Q, cudaStream_t strea
 cudaError_t launch_trace_noalloc(const DScene& S, TraceArgs A, bool count_hits, long long* hit_counts_out,
                                  long long* host_stats, cudaStream_t stream, int sm_count);
 int launch_umma_check(const uint16_t* A, const uint16_t* B, float* D, int* err, cudaStream_t st);
+cudaError_t launch_bounce_rays(const double* frames, const double* trig, int theta_n, int phi_n, long long n,
+                               double* org, double* dir, cudaStream_t st);
+cudaError_t launch_bounce_reduce(const int* status, const int* bounces, long long points, int dirs_per, int* max_out,
+                                 int* err_out, int* best_out, cudaStream_t st);
 }  // namespace bbrt
 
 namespace {
@@ -121,6 +125,9 @@ struct bbrt_scene {
         long long steps = 0;
         double min_logit = 0.0, t_window = 0.5;
     } guess;
+    // Launch schedule of this scene (library defaults until set or autotuned).
+    bool tune_set = false;
+    bbrt_tuning tune{};
     // Training-sample recording, set only inside bbrt_guess_train.
     bbrt::GuessSample* rec_samples = nullptr;
     unsigned long long* rec_count = nullptr;
@@ -453,15 +460,30 @@ bbrt::MlpNet guess_net(bbrt_scene* s) {
 // set, and rays whose query needed more solves than the resolved list holds,
 // are finished by k_resume.
 // Finishes the rays of `reqs` (or `rays`) from their saved state.
+// The scene's schedule: its own once set or autotuned, else the library defaults.
+bbrt_tuning scene_tuning(const bbrt_scene* s) {
+    if (s->tune_set) return s->tune;
+    const Tuning& T = tuning();
+    bbrt_tuning t;
+    t.advance_shape = T.advance_shape;
+    t.warp_stage1 = T.warp_stage1;
+    t.order_rays = T.order_rays;
+    t.warp_tail = T.warp_tail;
+    t.wave_tail = T.wave_tail;
+    t.wave_min_rays = T.wave_min_rays;
+    return t;
+}
+
 cudaError_t run_tail(bbrt_scene* s, const bbrt::TraceArgs& A, const bbrt::WaveArgs& W,
                      const bbrt::NewtonRequest* reqs, const int* rays, long long n, cudaStream_t st) {
-    if (tuning().warp_tail) return bbrt::launch_resume_warp(s->dev, A, W, reqs, rays, n, s->sm_count, st);
+    if (scene_tuning(s).warp_tail) return bbrt::launch_resume_warp(s->dev, A, W, reqs, rays, n, s->sm_count, st);
     return bbrt::launch_resume(s->dev, A, W, reqs, rays, n, st);
 }
 
 int run_wavefront(bbrt_scene* s, const bbrt::TraceArgs& A, cudaStream_t st) {
     const long long n = A.n;
-    const Tuning& T = tuning();
+    const bbrt_tuning T = scene_tuning(s);
+    const int log_rounds = tuning().log_rounds;
     BBRT_CUDA(s->wave.ensure(bbrt::wave_workspace_bytes(n)));
     BBRT_CUDA(s->wave_ctr.ensure(3 * sizeof(unsigned int)));
     if (!s->wave_ctr_host) BBRT_CUDA(cudaMallocHost(&s->wave_ctr_host, 2 * sizeof(unsigned int)));
@@ -488,17 +510,17 @@ int run_wavefront(bbrt_scene* s, const bbrt::TraceArgs& A, cudaStream_t st) {
     const long long max_rounds = 4 + static_cast<long long>(A.max_bounces + 1) * (s->host.n_objects + 1);
     long long overflowed = 0;
     for (long long round = 0; round < max_rounds; ++round) {
-        if (T.log_rounds) BBRT_CUDA(cudaEventRecord(s->ev[2], st));
+        if (log_rounds) BBRT_CUDA(cudaEventRecord(s->ev[2], st));
         BBRT_CUDA(cudaMemsetAsync(W.counters, 0, sizeof(unsigned int), st));
         BBRT_CUDA(cudaMemsetAsync(W.counters + 2, 0, sizeof(unsigned int), st));
         BBRT_CUDA(timed(s, K_ADVANCE, st, [&] { return bbrt::launch_advance(s->dev, A, W, s->sm_count, T.advance_shape, st); }));
         ++s->rounds;
-        if (T.log_rounds) BBRT_CUDA(cudaEventRecord(s->ev[3], st));
+        if (log_rounds) BBRT_CUDA(cudaEventRecord(s->ev[3], st));
         BBRT_CUDA(cudaMemcpyAsync(s->wave_ctr_host, W.counters, 2 * sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
         BBRT_CUDA(cudaStreamSynchronize(st));
         const long long n_req = s->wave_ctr_host[0];
         overflowed = s->wave_ctr_host[1];
-        if (T.log_rounds) {
+        if (log_rounds) {
             float ms = 0.0f;
             cudaEventElapsedTime(&ms, s->ev[2], s->ev[3]);
             std::fprintf(stderr, "bbrt round %lld: runnable %lld advance %.3f ms -> requests %lld overflow %lld\n",
@@ -509,7 +531,7 @@ int run_wavefront(bbrt_scene* s, const bbrt::TraceArgs& A, cudaStream_t st) {
             BBRT_CUDA(timed(s, K_TAIL, st, [&] { return run_tail(s, A, W, W.req, nullptr, n_req, st); }));
             break;
         }
-        if (T.log_rounds) BBRT_CUDA(cudaEventRecord(s->ev[2], st));
+        if (log_rounds) BBRT_CUDA(cudaEventRecord(s->ev[2], st));
         W.guess = nullptr;
         if (s->host.cfg.guess == BBRT_GUESS_LEARNED && s->guess.trained) {
             BBRT_CUDA(s->guess.out.ensure(sizeof(double) * 4 * static_cast<size_t>(n_req)));
@@ -524,7 +546,7 @@ int run_wavefront(bbrt_scene* s, const bbrt::TraceArgs& A, cudaStream_t st) {
             W.guess_t_window = s->guess.t_window;
         }
         BBRT_CUDA(timed(s, K_NEWTON, st, [&] { return bbrt::launch_newton(s->dev, A, W, n_req, st); }));
-        if (T.log_rounds) {
+        if (log_rounds) {
             BBRT_CUDA(cudaEventRecord(s->ev[3], st));
             BBRT_CUDA(cudaEventSynchronize(s->ev[3]));
             float ms = 0.0f;
@@ -582,7 +604,7 @@ int run_trace_device(bbrt_scene* s, const double* d_o, const double* d_d, long l
     s->rounds = 0;
     s->launches = 0;
     BBRT_CUDA(cudaEventRecord(s->ev[0], st));
-    if (n < tuning().wave_min_rays) {
+    if (n < scene_tuning(s).wave_min_rays) {
         BBRT_CUDA(timed(s, K_TAIL, st, [&] { return bbrt::launch_trace(s->dev, A, st, s->sm_count); }));
     } else {
         const int rc = run_wavefront(s, A, st);
@@ -951,13 +973,16 @@ static int check_bounce_map_args(int grid_n, int theta_n, int phi_n, double cone
 // point k, polar index ti and azimuth index pj.  With idx == NULL all rays
 // are written in that order (n must be their count); otherwise ray idx[i]
 // goes to slot i.
-static void gen_bounce_rays(const bbrt_scene* s, const bbrt_patch_desc* samples, int n_sample, int grid_n, int theta_n,
-                            int phi_n, double cone_angle_deg, const long long* idx, long long n, double* org,
-                            double* dir) {
+// Direction tables of the sweep: mu[theta_n], sin(theta)[theta_n],
+// cos(phi)[phi_n], sin(phi)[phi_n], in that order (host libm, as the reference).
+static std::vector<double> bounce_trig(int theta_n, int phi_n, double cone_angle_deg) {
     const double kTwoPi = 6.283185307179586476925286766559;
     const double cos_max = std::cos(cone_angle_deg / 2.0 * kTwoPi / 360.0);
-    const long long per = static_cast<long long>(grid_n) * grid_n, dirs_per = static_cast<long long>(theta_n) * phi_n;
-    std::vector<double> cphi(phi_n), sphi(phi_n), mu(theta_n), sth(theta_n);
+    std::vector<double> tab(2 * static_cast<size_t>(theta_n) + 2 * static_cast<size_t>(phi_n));
+    double* mu = tab.data();
+    double* sth = mu + theta_n;
+    double* cphi = sth + theta_n;
+    double* sphi = cphi + phi_n;
     for (int ti = 0; ti < theta_n; ++ti) {
         mu[ti] = cos_max + (static_cast<double>(ti) + 0.5) / static_cast<double>(theta_n) * (1.0 - cos_max);
         sth[ti] = std::sqrt(std::max(0.0, 1.0 - mu[ti] * mu[ti]));
@@ -967,52 +992,78 @@ static void gen_bounce_rays(const bbrt_scene* s, const bbrt_patch_desc* samples,
         cphi[pj] = std::cos(phi);
         sphi[pj] = std::sin(phi);
     }
-    // Per sample patch, built on first use: launch origin and frame
-    // (origin, t1, t2, n) of every grid point.
+    return tab;
+}
+
+// Launch origin and frame (origin, t1, t2, n: 12 doubles) of every grid point
+// of one sample patch, written to f[12 * per].
+static void bounce_frame(const bbrt_scene* s, const bbrt_patch_desc& sample, int grid_n, double* f) {
+    const long long per = static_cast<long long>(grid_n) * grid_n;
+    bbrt::HostScene one;
+    bbrt_object_desc od{};
+    od.kind = BBRT_OBJ_PATCH;
+    od.patch = &sample;
+    bbrt::build_host_scene(&od, 1, s->host.cfg, one);
+    const double a = s->host.cfg.self_intersect_eps_factor * s->host.scene_diagonal;
+    const double b = s->host.cfg.sagitta_clearance_factor * one.padding[0];
+    const double eps = (a < b) ? b : a;
+    std::vector<double> xyz(3 * per), nrm(3 * per), du(3 * per);
+    bbrt::sample_grid(sample, grid_n, xyz.data(), nrm.data(), du.data());
+    for (long long k = 0; k < per; ++k) {
+        const double* P = &xyz[3 * k];
+        double n0 = nrm[3 * k], n1 = nrm[3 * k + 1], n2 = nrm[3 * k + 2];
+        const double nl = std::sqrt(n0 * n0 + n1 * n1 + n2 * n2);
+        n0 /= nl; n1 /= nl; n2 /= nl;
+        const double d0 = du[3 * k], d1 = du[3 * k + 1], d2 = du[3 * k + 2];
+        const double du2 = d0 * d0 + d1 * d1 + d2 * d2, dn = d0 * n0 + d1 * n1 + d2 * n2;
+        const double q0 = d0 - dn * n0, q1 = d1 - dn * n1, q2 = d2 - dn * n2;
+        const double qq = q0 * q0 + q1 * q1 + q2 * q2;
+        double* F = f + 12 * k;
+        double* t1 = F + 3;
+        double* t2 = F + 6;
+        if (qq > 1e-6 * 1e-6 * du2) {
+            const double l = std::sqrt(q0 * q0 + q1 * q1 + q2 * q2);
+            t1[0] = q0 / l; t1[1] = q1 / l; t1[2] = q2 / l;
+        } else {
+            double ax[3] = { 0, 0, 0 };
+            if (std::fabs(n0) <= std::fabs(n1) && std::fabs(n0) <= std::fabs(n2)) ax[0] = 1.0;
+            else if (std::fabs(n1) <= std::fabs(n2)) ax[1] = 1.0;
+            else ax[2] = 1.0;
+            const double c0v = n1 * ax[2] - n2 * ax[1], c1v = n2 * ax[0] - n0 * ax[2], c2v = n0 * ax[1] - n1 * ax[0];
+            const double l = std::sqrt(c0v * c0v + c1v * c1v + c2v * c2v);
+            t1[0] = c0v / l; t1[1] = c1v / l; t1[2] = c2v / l;
+        }
+        t2[0] = n1 * t1[2] - n2 * t1[1];
+        t2[1] = n2 * t1[0] - n0 * t1[2];
+        t2[2] = n0 * t1[1] - n1 * t1[0];
+        F[0] = P[0] + n0 * eps; F[1] = P[1] + n1 * eps; F[2] = P[2] + n2 * eps;
+        F[9] = n0; F[10] = n1; F[11] = n2;
+    }
+}
+
+// Bounce-map launch rays on the host, in the reference's arithmetic
+// (BounceMapDriver.hpp:119-237, build_tangent_frame :499-519).  Ray r is
+// ((p * grid_n^2 + k) * theta_n + ti) * phi_n + pj for sample patch p, grid
+// point k, polar index ti and azimuth index pj.  With idx == NULL all rays
+// are written in that order (n must be their count); otherwise ray idx[i]
+// goes to slot i.  (bbrt_bounce_map itself builds the rays on the device
+// from the same frames and tables, k_bounce_rays.)
+static void gen_bounce_rays(const bbrt_scene* s, const bbrt_patch_desc* samples, int n_sample, int grid_n, int theta_n,
+                            int phi_n, double cone_angle_deg, const long long* idx, long long n, double* org,
+                            double* dir) {
+    const long long per = static_cast<long long>(grid_n) * grid_n, dirs_per = static_cast<long long>(theta_n) * phi_n;
+    const std::vector<double> tab = bounce_trig(theta_n, phi_n, cone_angle_deg);
+    const double* mu = tab.data();
+    const double* sth = mu + theta_n;
+    const double* cphi = sth + theta_n;
+    const double* sphi = cphi + phi_n;
+    // per sample patch, built on first use
     std::vector<std::vector<double>> frames(n_sample);
     auto frame_of = [&](int p) -> const std::vector<double>& {
         std::vector<double>& f = frames[p];
-        if (!f.empty()) return f;
-        bbrt::HostScene one;
-        bbrt_object_desc od{};
-        od.kind = BBRT_OBJ_PATCH;
-        od.patch = &samples[p];
-        bbrt::build_host_scene(&od, 1, s->host.cfg, one);
-        const double a = s->host.cfg.self_intersect_eps_factor * s->host.scene_diagonal;
-        const double b = s->host.cfg.sagitta_clearance_factor * one.padding[0];
-        const double eps = (a < b) ? b : a;
-        std::vector<double> xyz(3 * per), nrm(3 * per), du(3 * per);
-        bbrt::sample_grid(samples[p], grid_n, xyz.data(), nrm.data(), du.data());
-        f.resize(12 * per);
-        for (long long k = 0; k < per; ++k) {
-            const double* P = &xyz[3 * k];
-            double n0 = nrm[3 * k], n1 = nrm[3 * k + 1], n2 = nrm[3 * k + 2];
-            const double nl = std::sqrt(n0 * n0 + n1 * n1 + n2 * n2);
-            n0 /= nl; n1 /= nl; n2 /= nl;
-            const double d0 = du[3 * k], d1 = du[3 * k + 1], d2 = du[3 * k + 2];
-            const double du2 = d0 * d0 + d1 * d1 + d2 * d2, dn = d0 * n0 + d1 * n1 + d2 * n2;
-            const double q0 = d0 - dn * n0, q1 = d1 - dn * n1, q2 = d2 - dn * n2;
-            const double qq = q0 * q0 + q1 * q1 + q2 * q2;
-            double* F = &f[12 * k];
-            double* t1 = F + 3;
-            double* t2 = F + 6;
-            if (qq > 1e-6 * 1e-6 * du2) {
-                const double l = std::sqrt(q0 * q0 + q1 * q1 + q2 * q2);
-                t1[0] = q0 / l; t1[1] = q1 / l; t1[2] = q2 / l;
-            } else {
-                double ax[3] = { 0, 0, 0 };
-                if (std::fabs(n0) <= std::fabs(n1) && std::fabs(n0) <= std::fabs(n2)) ax[0] = 1.0;
-                else if (std::fabs(n1) <= std::fabs(n2)) ax[1] = 1.0;
-                else ax[2] = 1.0;
-                const double c0v = n1 * ax[2] - n2 * ax[1], c1v = n2 * ax[0] - n0 * ax[2], c2v = n0 * ax[1] - n1 * ax[0];
-                const double l = std::sqrt(c0v * c0v + c1v * c1v + c2v * c2v);
-                t1[0] = c0v / l; t1[1] = c1v / l; t1[2] = c2v / l;
-            }
-            t2[0] = n1 * t1[2] - n2 * t1[1];
-            t2[1] = n2 * t1[0] - n0 * t1[2];
-            t2[2] = n0 * t1[1] - n1 * t1[0];
-            F[0] = P[0] + n0 * eps; F[1] = P[1] + n1 * eps; F[2] = P[2] + n2 * eps;
-            F[9] = n0; F[10] = n1; F[11] = n2;
+        if (f.empty()) {
+            f.resize(12 * per);
+            bounce_frame(s, samples[p], grid_n, f.data());
         }
         return f;
     };
@@ -1063,35 +1114,56 @@ BBRT_API int bbrt_bounce_map(bbrt_scene_t s, const bbrt_patch_desc* samples, int
     int rc0 = check_bounce_map_args(grid_n, theta_n, phi_n, cone_angle_deg);
     if (rc0) return rc0;
     if (n_sample < 1) return fail(BBRT_ERR_ARG, "bbrt_bounce_map: no sample patches");
+    if (max_bounces < 0) return fail(BBRT_ERR_ARG, "bbrt_bounce_map: max_bounces < 0");
     const long long per = static_cast<long long>(grid_n) * grid_n, dirs_per = static_cast<long long>(theta_n) * phi_n;
-    const long long N = static_cast<long long>(n_sample) * per * dirs_per;
-    std::vector<double> org(3 * N), dir(3 * N);
+    const long long points = static_cast<long long>(n_sample) * per;
+    const long long N = points * dirs_per;
+    // Host: the grid frames of the sample patches and the direction tables
+    // (libm sin / cos, as the reference); device: every launch ray, the
+    // trace, and the per-point reduction.
+    std::vector<double> frames(12 * static_cast<size_t>(points));
+    std::vector<double> tab;
     try {
-        gen_bounce_rays(s, samples, n_sample, grid_n, theta_n, phi_n, cone_angle_deg, nullptr, N, org.data(),
-                        dir.data());
+        for (int p = 0; p < n_sample; ++p) bounce_frame(s, samples[p], grid_n, frames.data() + 12 * p * per);
+        tab = bounce_trig(theta_n, phi_n, cone_angle_deg);
     } catch (const std::exception& e) {
         return fail(BBRT_ERR_ARG, e.what());
     }
-    std::vector<int> status(N), bounces(N);
-    bbrt_trace_out o{};
-    o.status = status.data();
-    o.bounce_count = bounces.data();
-    const int rc = bbrt_trace(s, org.data(), dir.data(), N, max_bounces, 0, &o, stats, stream);
+    std::lock_guard<std::mutex> g(s->mu);
+    int rc = ensure_uploaded(s);
     if (rc) return rc;
-    // per point: max over non-Error directions, Error count, first maximum
-    for (long long q = 0; q < static_cast<long long>(n_sample) * per; ++q) {
-        int best = 0, nerr = 0, bdir = -1;
-        for (long long k = 0; k < dirs_per; ++k) {
-            const long long r = q * dirs_per + k;
-            const int stt = status[r];
-            if (stt != BBRT_RAY_ESCAPED && stt != BBRT_RAY_MAX_BOUNCES) { ++nerr; continue; }
-            if (bdir < 0 || bounces[r] > best) bdir = static_cast<int>(k);
-            best = std::max(best, bounces[r]);
-        }
-        max_out[q] = best;
-        err_out[q] = nerr;
-        if (best_out) best_out[q] = bdir;
-    }
+    cudaStream_t st = pick_stream(s, stream);
+    const size_t fb = sizeof(double) * frames.size(), tb = sizeof(double) * tab.size();
+    BBRT_CUDA(s->in_o.ensure(sizeof(double) * 3 * N));
+    BBRT_CUDA(s->in_d.ensure(sizeof(double) * 3 * N));
+    BBRT_CUDA(s->o_status.ensure(sizeof(int) * N));
+    BBRT_CUDA(s->o_bounce.ensure(sizeof(int) * N));
+    BBRT_CUDA(s->hits.ensure(fb + tb + 3 * sizeof(int) * static_cast<size_t>(points)));
+    double* dframes = static_cast<double*>(s->hits.p);
+    double* dtab = dframes + frames.size();
+    int* dmax = reinterpret_cast<int*>(dtab + tab.size());
+    int* derr = dmax + points;
+    int* dbest = derr + points;
+    BBRT_CUDA(cudaMemcpyAsync(dframes, frames.data(), fb, cudaMemcpyHostToDevice, st));
+    BBRT_CUDA(cudaMemcpyAsync(dtab, tab.data(), tb, cudaMemcpyHostToDevice, st));
+    double* dorg = static_cast<double*>(s->in_o.p);
+    double* ddir = static_cast<double*>(s->in_d.p);
+    BBRT_CUDA(bbrt::launch_bounce_rays(dframes, dtab, theta_n, phi_n, N, dorg, ddir, st));
+    bbrt_trace_out o{};
+    o.status = static_cast<int*>(s->o_status.p);
+    o.bounce_count = static_cast<int*>(s->o_bounce.p);
+    long long hs[bbrt::ST_COUNT] = { 0 };
+    float kms = 0.0f;
+    rc = run_trace_device(s, dorg, ddir, N, max_bounces, &o, nullptr, 1, st, stats != nullptr, hs,
+                          stats ? &kms : nullptr);
+    if (rc) return rc;
+    BBRT_CUDA(bbrt::launch_bounce_reduce(o.status, o.bounce_count, points, static_cast<int>(dirs_per), dmax, derr,
+                                         dbest, st));
+    BBRT_CUDA(cudaMemcpyAsync(max_out, dmax, sizeof(int) * points, cudaMemcpyDeviceToHost, st));
+    BBRT_CUDA(cudaMemcpyAsync(err_out, derr, sizeof(int) * points, cudaMemcpyDeviceToHost, st));
+    if (best_out) BBRT_CUDA(cudaMemcpyAsync(best_out, dbest, sizeof(int) * points, cudaMemcpyDeviceToHost, st));
+    BBRT_CUDA(cudaStreamSynchronize(st));
+    if (stats) fill_stats(s, hs, N, kms, kms, stats);
     return BBRT_OK;
 }
 
@@ -1539,5 +1611,92 @@ BBRT_API int bbrt_mlp_infer_check(const float* params, int n_patches, const floa
     BBRT_CUDA(cudaMemcpy(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost));
     if (herr) return fail(BBRT_ERR_KERNEL, "bbrt_mlp_infer_check: a tensor-core completion wait timed out");
     BBRT_CUDA(cudaMemcpy(out, dout, sizeof(double) * 4 * rows, cudaMemcpyDeviceToHost));
+    return BBRT_OK;
+}
+
+// ---- launch schedule and its autotuner -------------------------------------
+
+BBRT_API int bbrt_scene_get_tuning(bbrt_scene_t s, bbrt_tuning* out) {
+    if (!s || !out) return fail(BBRT_ERR_ARG, "bbrt_scene_get_tuning: NULL argument");
+    std::lock_guard<std::mutex> g(s->mu);
+    *out = scene_tuning(s);
+    return BBRT_OK;
+}
+
+BBRT_API int bbrt_scene_set_tuning(bbrt_scene_t s, const bbrt_tuning* t) {
+    if (!s || !t) return fail(BBRT_ERR_ARG, "bbrt_scene_set_tuning: NULL argument");
+    if (t->advance_shape < 0 || t->advance_shape > 6) return fail(BBRT_ERR_ARG, "bbrt_scene_set_tuning: advance_shape must be 0..6");
+    if (t->wave_tail < 0 || t->wave_min_rays < 0) return fail(BBRT_ERR_ARG, "bbrt_scene_set_tuning: negative size");
+    std::lock_guard<std::mutex> g(s->mu);
+    s->tune = *t;
+    s->tune_set = true;
+    return BBRT_OK;
+}
+
+BBRT_API int bbrt_scene_autotune(bbrt_scene_t s, const double* origins, const double* dirs, long long n, int max_bounces,
+                                 int trials, bbrt_tuning* best, double* best_ms, void* stream) {
+    if (!s || !origins || !dirs) return fail(BBRT_ERR_ARG, "bbrt_scene_autotune: NULL argument");
+    if (n <= 0 || max_bounces < 0 || trials < 1) return fail(BBRT_ERR_ARG, "bbrt_scene_autotune: bad size");
+    std::lock_guard<std::mutex> g(s->mu);
+    int rc = ensure_uploaded(s);
+    if (rc) return rc;
+    cudaStream_t st = pick_stream(s, stream);
+    BBRT_CUDA(s->in_o.ensure(sizeof(double) * 3 * n));
+    BBRT_CUDA(s->in_d.ensure(sizeof(double) * 3 * n));
+    BBRT_CUDA(cudaMemcpyAsync(s->in_o.p, origins, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, st));
+    BBRT_CUDA(cudaMemcpyAsync(s->in_d.p, dirs, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, st));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    BBRT_CUDA(cudaEventCreate(&e0));
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return fail(BBRT_ERR_CUDA, "bbrt_scene_autotune: cudaEventCreate failed");
+    }
+    auto time_one = [&](const bbrt_tuning& t, double& ms) -> int {
+        s->tune = t;
+        s->tune_set = true;
+        double total = 0.0;
+        for (int k = 0; k <= trials; ++k) {
+            BBRT_CUDA(cudaEventRecord(e0, st));
+            const int r = run_trace_device(s, static_cast<const double*>(s->in_o.p), static_cast<const double*>(s->in_d.p),
+                                           n, max_bounces, nullptr, nullptr, 1, st, false, nullptr, nullptr);
+            if (r) return r;
+            BBRT_CUDA(cudaEventRecord(e1, st));
+            BBRT_CUDA(cudaEventSynchronize(e1));
+            float el = 0.0f;
+            BBRT_CUDA(cudaEventElapsedTime(&el, e0, e1));
+            if (k > 0) total += el;
+        }
+        ms = total / trials;
+        return BBRT_OK;
+    };
+    bbrt_tuning cur = scene_tuning(s);
+    double cur_ms = 0.0;
+    rc = time_one(cur, cur_ms);
+    // coordinate descent: launch shape, then tail size
+    const int shapes[] = { 3, 6, 1, 0 };
+    for (int sh : shapes) {
+        if (rc || sh == cur.advance_shape) continue;
+        bbrt_tuning c = cur;
+        c.advance_shape = sh;
+        double ms = 0.0;
+        rc = time_one(c, ms);
+        if (!rc && ms < cur_ms) { cur = c; cur_ms = ms; }
+    }
+    const long long tails[] = { 8192, 16384, 32768 };
+    for (long long tl : tails) {
+        if (rc || tl == cur.wave_tail) continue;
+        bbrt_tuning c = cur;
+        c.wave_tail = tl;
+        double ms = 0.0;
+        rc = time_one(c, ms);
+        if (!rc && ms < cur_ms) { cur = c; cur_ms = ms; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    s->tune = cur;
+    s->tune_set = true;
+    if (rc) return rc;
+    if (best) *best = cur;
+    if (best_ms) *best_ms = cur_ms;
     return BBRT_OK;
 }

@@ -1370,6 +1370,66 @@ cudaError_t launch_resume_warp(const DScene& S, const TraceArgs& A, const WaveAr
     return cudaGetLastError();
 }
 
+// ---- BounceMapDriver::run on the device ------------------------------------
+
+// Launch ray r = (point q, direction ti * phi_n + pj) of the sweep
+// (BounceMapDriver.hpp:195-237): the point's frame (origin, t1, t2, n) and
+// the direction tables come from the host; the expression and its rounding
+// (no fused multiply-add in this file) are the reference's.
+__global__ void k_bounce_rays(const double* __restrict__ frames, const double* __restrict__ trig, int theta_n,
+                              int phi_n, long long n, double* __restrict__ org, double* __restrict__ dir) {
+    const long long r = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (r >= n) return;
+    const long long dirs_per = static_cast<long long>(theta_n) * phi_n;
+    const long long q = r / dirs_per, dk = r % dirs_per;
+    const int ti = static_cast<int>(dk / phi_n), pj = static_cast<int>(dk % phi_n);
+    const double* F = frames + 12 * q;
+    const double m = trig[ti], st_ = trig[theta_n + ti], cp = trig[2 * theta_n + pj], sp = trig[2 * theta_n + phi_n + pj];
+    org[3 * r] = F[0];
+    org[3 * r + 1] = F[1];
+    org[3 * r + 2] = F[2];
+    dir[3 * r] = F[3] * st_ * cp + F[6] * st_ * sp + F[9] * m;
+    dir[3 * r + 1] = F[4] * st_ * cp + F[7] * st_ * sp + F[10] * m;
+    dir[3 * r + 2] = F[5] * st_ * cp + F[8] * st_ * sp + F[11] * m;
+}
+
+// Per grid point: the largest bounce count over non-Error directions, the
+// number of Error directions, and the first direction reaching the maximum
+// (BounceMapDriver.hpp:199-240).
+__global__ void k_bounce_reduce(const int* __restrict__ status, const int* __restrict__ bounces, long long points,
+                                int dirs_per, int* __restrict__ max_out, int* __restrict__ err_out,
+                                int* __restrict__ best_out) {
+    const long long q = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (q >= points) return;
+    int best = 0, nerr = 0, bdir = -1;
+    for (int k = 0; k < dirs_per; ++k) {
+        const long long r = q * dirs_per + k;
+        const int s = status[r];
+        if (s != BBRT_RAY_ESCAPED && s != BBRT_RAY_MAX_BOUNCES) { ++nerr; continue; }
+        const int b = bounces[r];
+        if (bdir < 0 || b > best) bdir = k;
+        best = b > best ? b : best;
+    }
+    max_out[q] = best;
+    err_out[q] = nerr;
+    best_out[q] = bdir;
+}
+
+cudaError_t launch_bounce_rays(const double* frames, const double* trig, int theta_n, int phi_n, long long n,
+                               double* org, double* dir, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    k_bounce_rays<<<static_cast<unsigned>((n + 255) / 256), 256, 0, st>>>(frames, trig, theta_n, phi_n, n, org, dir);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bounce_reduce(const int* status, const int* bounces, long long points, int dirs_per, int* max_out,
+                                 int* err_out, int* best_out, cudaStream_t st) {
+    if (points <= 0) return cudaSuccess;
+    k_bounce_reduce<<<static_cast<unsigned>((points + 127) / 128), 128, 0, st>>>(status, bounces, points, dirs_per,
+                                                                              max_out, err_out, best_out);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_query(const DScene& S, const QueryArgs& Q, cudaStream_t stream) {
     if (Q.n <= 0) return cudaSuccess;
     const long long blocks = (Q.n + 127) / 128;

@@ -368,6 +368,34 @@ BBRT_API int  bbrt_mlp_check(const float* params, int n_patches, const float* fe
 BBRT_API int  bbrt_mlp_infer_check(const float* params, int n_patches, const float* feat, const int* patch,
                                    int rows, double* out);
 
+/* ---- launch schedule and its autotuner (no reference counterpart) --------
+ *
+ * The schedule changes only the order and grouping of work, never a result
+ * (every schedule gives the same bits; GPU-tested).  A scene starts with the
+ * library defaults (environment overrides BBRT_ADV_SHAPE, BBRT_WARP_S1,
+ * BBRT_ORDER_RAYS, BBRT_WARP_TAIL, BBRT_WAVE_TAIL, BBRT_WAVE_MIN are read
+ * once per process). */
+typedef struct bbrt_tuning {
+    int advance_shape;        /* k_advance launch shape, threads x blocks per SM: 0 = 128x3, 1 = 256x2,
+                                 2 = 128x4, 3 = 512x1 (default), 4 = 768x1, 5 = 1024x1, 6 = 384x1 */
+    int warp_stage1;          /* 1 (default): each patch's stage 1 by the whole warp */
+    int order_rays;           /* 1 (default): bucket rays by direction and origin before round 0 */
+    int warp_tail;            /* 1 (default): the tail one warp per ray, else one thread per ray */
+    long long wave_tail;      /* rays still waiting when the tail takes over (16384) */
+    long long wave_min_rays;  /* smaller batches run the fused per-thread kernel (8192) */
+} bbrt_tuning;
+
+BBRT_API int bbrt_scene_get_tuning(bbrt_scene_t scene, bbrt_tuning* out);
+BBRT_API int bbrt_scene_set_tuning(bbrt_scene_t scene, const bbrt_tuning* tuning);
+/* Times candidate schedules on the given rays (host arrays; the scene's
+ * current precision and guess modes), by coordinate descent over the launch
+ * shape, then the tail size, `trials` timed traces each after one untimed
+ * one; keeps the fastest in the scene and returns it with its mean device
+ * time per trace. */
+BBRT_API int bbrt_scene_autotune(bbrt_scene_t scene, const double* origins, const double* dirs, long long n,
+                                 int max_bounces, int trials, bbrt_tuning* best, double* best_ms,
+                                 void* stream);
+
 /* ---- diagnostics ------------------------------------------------------ */
 enum {
     BBRT_PIPE_FP64 = 0,   /* FP64 FMA throughput, TFLOP/s (2 FLOP per FMA) */

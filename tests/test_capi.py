@@ -171,3 +171,13 @@ def test_bounce_map_rays_equal_oracle(built):
         sc.bounce_map_rays(samples, 3, 2, 5, 180.0, ray_index=[3 * 9 * 10])
     with pytest.raises(RuntimeError, match="position_grid_n must be >= 2"):
         sc.bounce_map_rays(samples, 1, 2, 5, 180.0)
+
+
+def test_scene_tuning_roundtrip_and_validation(built):
+    sc = api.Scene(scenes.scene_two_spheres(), config=C.default_config(coarse_grid_n=9))
+    t = sc.tuning()
+    assert t["advance_shape"] == 3 and t["warp_stage1"] == 1 and t["wave_tail"] == 16384
+    t2 = sc.tuning(advance_shape=6, wave_tail=8192)
+    assert t2["advance_shape"] == 6 and t2["wave_tail"] == 8192 and sc.tuning() == t2
+    with pytest.raises(RuntimeError, match="advance_shape"):
+        sc.tuning(advance_shape=9)

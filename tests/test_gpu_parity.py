@@ -249,3 +249,17 @@ def test_launch_shape_knobs_do_not_change_results(built, workloads, tmp_path, en
     r = oracle.Oracle(patches, config=C.default_config(coarse_grid_n=cn, newton_tol=tol)).trace(o, d, maxb, K=4)
     for k in g.files:
         assert np.array_equal(g[k], r[k]), (env, k)
+
+
+def test_autotune_keeps_results(built, workloads):
+    """The autotuner only picks a launch schedule: the trace under the chosen
+    schedule equals the trace under the defaults, bit for bit."""
+    patches, o, d, maxb, cn, tol = workloads("tetra_spheres", 131072)
+    sc = api.Scene(patches, config=C.default_config(coarse_grid_n=cn, newton_tol=tol))
+    base = sc.trace(o, d, maxb, record=4, outputs=("status", "bounce_count", "hit_object", "hit_point", "exit_dir"))
+    best = sc.autotune(o, d, maxb, trials=1)
+    assert best["ms"] > 0 and 0 <= best["advance_shape"] <= 6
+    assert sc.tuning()["advance_shape"] == best["advance_shape"]
+    tuned = sc.trace(o, d, maxb, record=4, outputs=("status", "bounce_count", "hit_object", "hit_point", "exit_dir"))
+    for k in ("status", "bounce_count", "hit_object", "hit_point", "exit_dir"):
+        assert np.array_equal(base[k], tuned[k]), k
