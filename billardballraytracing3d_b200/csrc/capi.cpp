@@ -421,6 +421,7 @@ struct Tuning {
     int warp_tail = 1;                // finish the tail one warp per ray (else one thread per ray)
     int advance_shape = 3;            // k_advance launch shape (see launch_advance): 512 threads x 1 block per SM
     int warp_stage1 = 1;              // k_advance runs each patch's stage 1 with the whole warp
+    int resume_queries = 1;           // suspended queries resume where they stopped (else replay from the root)
 };
 
 // Launch-shape knobs; defaults tuned on B200, overridable for experiments by
@@ -436,6 +437,7 @@ const Tuning& tuning() {
         if (const char* e = std::getenv("BBRT_WARP_TAIL")) v.warp_tail = std::atoi(e);
         if (const char* e = std::getenv("BBRT_ADV_SHAPE")) v.advance_shape = std::atoi(e);
         if (const char* e = std::getenv("BBRT_WARP_S1")) v.warp_stage1 = std::atoi(e);
+        if (const char* e = std::getenv("BBRT_RESUME")) v.resume_queries = std::atoi(e);
         return v;
     }();
     return t;
@@ -492,6 +494,7 @@ int run_wavefront(bbrt_scene* s, const bbrt::TraceArgs& A, cudaStream_t st) {
     bbrt::wave_layout(s->wave.p, n, W, req_a, req_b);
     W.counters = static_cast<unsigned int*>(s->wave_ctr.p);
     W.warp_stage1 = T.warp_stage1;
+    W.resume_queries = tuning().resume_queries;
     W.runnable = nullptr;
     W.n_runnable = n;
     W.req = req_a;

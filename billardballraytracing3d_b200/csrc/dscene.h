@@ -141,7 +141,19 @@ struct WaveArgs {
     double guess_min_logit = 0.0;              // confidence needed to start Newton from the guess
     double guess_t_window = 0.5;               // accepted |t - t_stage1| in units of L
     int warp_stage1 = 1;                       // stage 1 of k_advance by the whole warp (else per lane)
+    // Traversal state of a query suspended for a Newton solve, so that the
+    // next round resumes it instead of replaying it from the root:
+    // qs_int[ray][kQsInt] = stack depth (-1: none saved), leaf start, leaf
+    // count, position in the leaf, best object, best resolved entry;
+    // qs_dbl[ray][3] = best t, triangle u, v; qs_stack[ray][kSaveStack].
+    int* qs_int = nullptr;
+    double* qs_dbl = nullptr;
+    int* qs_stack = nullptr;
+    int resume_queries = 1;
 };
+
+constexpr int kQsInt = 6;
+constexpr int kSaveStack = 24;
 
 struct QueryArgs {
     const double* origins = nullptr;

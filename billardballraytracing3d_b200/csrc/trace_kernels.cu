@@ -638,6 +638,53 @@ __device__ __forceinline__ void adv_start_query(const DScene& S, const TraceArgs
     stack[q.sp++] = 0;
 }
 
+// Keeps the traversal state of a query that suspends for a Newton solve
+// (the lane stands at the leaf position of the patch being solved).
+__device__ __forceinline__ void save_query(const WaveArgs& W, long long i, const AdvState& q, const int* stack) {
+    int* qi = W.qs_int + i * kQsInt;
+    if (!W.resume_queries || q.sp > kSaveStack) {
+        qi[0] = -1;
+        return;
+    }
+    qi[0] = q.sp;
+    qi[1] = q.leaf_start;
+    qi[2] = q.leaf_count;
+    qi[3] = q.leaf_k;
+    qi[4] = q.best_obj;
+    qi[5] = q.best_e;
+    double* qd = W.qs_dbl + i * 3;
+    qd[0] = q.best_t;
+    qd[1] = q.tri_u;
+    qd[2] = q.tri_v;
+    int* st = W.qs_stack + i * kSaveStack;
+    for (int k = 0; k < q.sp; ++k) st[k] = stack[k];
+}
+
+// Resumes a suspended query where it stopped (false when none was saved).
+// The visit sequence is the one a replay from the root would produce, whose
+// already-solved patches come from the resolved list.
+__device__ __forceinline__ bool resume_query(const DScene& S, const TraceArgs& A, const WaveArgs& W, long long i,
+                                             const RayCtx& r, AdvState& q, int* stack) {
+    if (!W.resume_queries) return false;
+    const int* qi = W.qs_int + i * kQsInt;
+    const int sp = qi[0];
+    if (sp < 0) return false;
+    adv_start_query(S, A, r, q, stack);
+    q.sp = sp;
+    q.leaf_start = qi[1];
+    q.leaf_count = qi[2];
+    q.leaf_k = qi[3];
+    q.best_obj = qi[4];
+    q.best_e = qi[5];
+    const double* qd = W.qs_dbl + i * 3;
+    q.best_t = qd[0];
+    q.tri_u = qd[1];
+    q.tri_v = qd[2];
+    const int* st = W.qs_stack + i * kSaveStack;
+    for (int k = 0; k < sp; ++k) stack[k] = st[k];
+    return true;
+}
+
 // Advances runnable rays until each needs a Newton solve, overflows its
 // resolved list, or finishes.  Persistent: lanes fetch rays from the
 // runnable set until it is drained.
@@ -908,6 +955,7 @@ __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, Wav
             ctr.tri_tests += cray.tri_tests;
             if (mode == M_SUSPEND) {
                 save_ray(W, i, r, nres + 1);
+                save_query(W, i, q, stack);
             } else if (mode == M_OVERFLOW) {
                 save_ray(W, i, r, nres);
             } else {
@@ -933,7 +981,9 @@ __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, Wav
                 }
                 mode = M_FINISH;
                 if (r.status < 0) {
-                    if (r.bounces >= A.max_bounces) {
+                    if (W.runnable != nullptr && resume_query(S, A, W, i, r, q, stack)) {
+                        mode = M_LEAF;
+                    } else if (r.bounces >= A.max_bounces) {
                         r.status = BBRT_RAY_MAX_BOUNCES;
                     } else {
                         adv_start_query(S, A, r, q, stack);
@@ -1278,7 +1328,7 @@ cudaError_t launch_trace_noalloc(const DScene& S, TraceArgs A, bool count_hits, 
 
 size_t wave_bytes_per_ray() {
     return sizeof(double) * 9 + sizeof(int) * 2 + sizeof(int) * 2 * kResolved + sizeof(double) * kResolved * kResData +
-           2 * sizeof(NewtonRequest) + sizeof(int);
+           2 * sizeof(NewtonRequest) + sizeof(int) + sizeof(int) * (kQsInt + kSaveStack) + sizeof(double) * 3;
 }
 
 // Carves the wavefront workspace for n rays out of `ws` (wave_bytes_per_ray() * n bytes).
@@ -1296,9 +1346,12 @@ void wave_layout(void* ws, long long n, WaveArgs& W, NewtonRequest*& req_a, Newt
     req_a = reinterpret_cast<NewtonRequest*>(take(sizeof(NewtonRequest) * n));
     req_b = reinterpret_cast<NewtonRequest*>(take(sizeof(NewtonRequest) * n));
     W.overflow = reinterpret_cast<int*>(take(sizeof(int) * n));
+    W.qs_int = reinterpret_cast<int*>(take(sizeof(int) * kQsInt * n));
+    W.qs_dbl = reinterpret_cast<double*>(take(sizeof(double) * 3 * n));
+    W.qs_stack = reinterpret_cast<int*>(take(sizeof(int) * kSaveStack * n));
 }
 
-size_t wave_workspace_bytes(long long n) { return wave_bytes_per_ray() * n + 16 * 256; }
+size_t wave_workspace_bytes(long long n) { return wave_bytes_per_ray() * n + 20 * 256; }
 
 template <int NT, int MINB>
 static cudaError_t launch_advance_shape(const DScene& S, const TraceArgs& A, const WaveArgs& W, int sm_count,
