@@ -39,7 +39,7 @@ cudaError_t launch_advance(const DScene& S, const TraceArgs& A, const WaveArgs& 
 cudaError_t launch_newton(const DScene& S, const TraceArgs& A, const WaveArgs& W, long long n_req,
                           cudaStream_t stream);
 cudaError_t launch_resume_warp(const DScene& S, const TraceArgs& A, const WaveArgs& W, const NewtonRequest* reqs,
-                               const int* rays, long long n, int sm_count, cudaStream_t stream);
+                               const int* rays, long long n, int sm_count, int shape, cudaStream_t stream);
 cudaError_t launch_resume(const DScene& S, const TraceArgs& A, const WaveArgs& W, const NewtonRequest* reqs,
                           const int* rays, long long n, cudaStream_t stream);
 size_t ray_order_workspace_bytes(long long n);
@@ -422,6 +422,7 @@ struct Tuning {
     int advance_shape = 3;            // k_advance launch shape (see launch_advance): 512 threads x 1 block per SM
     int warp_stage1 = 1;              // k_advance runs each patch's stage 1 with the whole warp
     int resume_queries = 1;           // suspended queries resume where they stopped (else replay from the root)
+    int tail_shape = 0;               // k_resume_warp launch shape (see launch_resume_warp)
 };
 
 // Launch-shape knobs; defaults tuned on B200, overridable for experiments by
@@ -438,6 +439,7 @@ const Tuning& tuning() {
         if (const char* e = std::getenv("BBRT_ADV_SHAPE")) v.advance_shape = std::atoi(e);
         if (const char* e = std::getenv("BBRT_WARP_S1")) v.warp_stage1 = std::atoi(e);
         if (const char* e = std::getenv("BBRT_RESUME")) v.resume_queries = std::atoi(e);
+        if (const char* e = std::getenv("BBRT_TAIL_SHAPE")) v.tail_shape = std::atoi(e);
         return v;
     }();
     return t;
@@ -478,7 +480,8 @@ bbrt_tuning scene_tuning(const bbrt_scene* s) {
 
 cudaError_t run_tail(bbrt_scene* s, const bbrt::TraceArgs& A, const bbrt::WaveArgs& W,
                      const bbrt::NewtonRequest* reqs, const int* rays, long long n, cudaStream_t st) {
-    if (scene_tuning(s).warp_tail) return bbrt::launch_resume_warp(s->dev, A, W, reqs, rays, n, s->sm_count, st);
+    if (scene_tuning(s).warp_tail)
+        return bbrt::launch_resume_warp(s->dev, A, W, reqs, rays, n, s->sm_count, tuning().tail_shape, st);
     return bbrt::launch_resume(s->dev, A, W, reqs, rays, n, st);
 }
 

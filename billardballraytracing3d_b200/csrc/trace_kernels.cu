@@ -1092,7 +1092,9 @@ __global__ void __launch_bounds__(128) k_resume(DScene S, TraceArgs A, WaveArgs 
 // keeps for finite t.  Non-finite rays take the ordered per-lane loop.
 
 // BVH::intersect for one ray with a whole warp (every lane returns the same result).
-__device__ QHit warp_bvh_query(const DScene& S, const V3& o, const V3& d, int cull_flag, int lane, Counters& ctr) {
+// Nodes [0, staged) are read from the shared-memory copy (sbox, slink).
+__device__ QHit warp_bvh_query(const DScene& S, const V3& o, const V3& d, int cull_flag, int lane, Counters& ctr,
+                               const double* sbox, const int* slink, int staged) {
     QHit best;
     best.obj = -1;
     best.err = 0;
@@ -1109,8 +1111,9 @@ __device__ QHit warp_bvh_query(const DScene& S, const V3& o, const V3& d, int cu
     while (sp > 0) {
         const int idx = stack[--sp];
         if (lane == 0) ++ctr.node_tests;
-        if (!ray_box_exact(o, inv, S.node_box + 6LL * idx, best_t)) continue;
-        const int* link = S.node_link + 4LL * idx;
+        const bool in_smem = idx < staged;
+        if (!ray_box_exact(o, inv, in_smem ? sbox + 6 * idx : S.node_box + 6LL * idx, best_t)) continue;
+        const int* link = in_smem ? slink + 4 * idx : S.node_link + 4LL * idx;
         if (link[1] < 0) {
             const int start = link[0], count = link[2];
             for (int k = 0; k < count; ++k) {
@@ -1158,8 +1161,17 @@ __device__ QHit warp_bvh_query(const DScene& S, const V3& o, const V3& d, int cu
 }
 
 // Finishes rays from their saved state, one warp per ray.
-__global__ void __launch_bounds__(128) k_resume_warp(DScene S, TraceArgs A, WaveArgs W, const NewtonRequest* reqs,
-                                                     const int* rays, long long n) {
+// MINB blocks of 128 threads per SM requested from the register allocator;
+// the first S.smem_nodes BVH nodes are staged in shared memory.
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB) k_resume_warp(DScene S, TraceArgs A, WaveArgs W,
+                                                           const NewtonRequest* reqs, const int* rays, long long n) {
+    extern __shared__ double smem_tail[];
+    double* sbox = smem_tail;
+    int* slink = reinterpret_cast<int*>(smem_tail + 6 * S.smem_nodes);
+    for (int k = threadIdx.x; k < 6 * S.smem_nodes; k += blockDim.x) sbox[k] = S.node_box[k];
+    for (int k = threadIdx.x; k < 4 * S.smem_nodes; k += blockDim.x) slink[k] = S.node_link[k];
+    __syncthreads();
     const int lane = threadIdx.x & 31;
     const long long warp = (blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x) >> 5;
     const long long n_warps = (static_cast<long long>(gridDim.x) * blockDim.x) >> 5;
@@ -1173,7 +1185,7 @@ __global__ void __launch_bounds__(128) k_resume_warp(DScene S, TraceArgs A, Wave
         while (r.status < 0) {
             if (r.bounces >= A.max_bounces) { r.status = BBRT_RAY_MAX_BOUNCES; break; }
             if (lane == 0) ++tally.queries;
-            const QHit h = warp_bvh_query(S, r.o, r.d, A.cull, lane, c1);
+            const QHit h = warp_bvh_query(S, r.o, r.d, A.cull, lane, c1, sbox, slink, S.smem_nodes);
             if (!step_ray(S, A, i, r, h, lane == 0)) break;
         }
         if (lane == 0) {
@@ -1409,18 +1421,39 @@ cudaError_t launch_resume(const DScene& S, const TraceArgs& A, const WaveArgs& W
     return cudaGetLastError();
 }
 
-cudaError_t launch_resume_warp(const DScene& S, const TraceArgs& A, const WaveArgs& W, const NewtonRequest* reqs,
-                               const int* rays, long long n, int sm_count, cudaStream_t stream) {
-    if (n <= 0) return cudaSuccess;
+template <int MINB>
+static cudaError_t launch_resume_warp_shape(const DScene& S, const TraceArgs& A, const WaveArgs& W,
+                                            const NewtonRequest* reqs, const int* rays, long long n, int sm_count,
+                                            int max_smem_nodes, cudaStream_t stream) {
+    DScene Sl = S;
+    if (Sl.smem_nodes > max_smem_nodes) Sl.smem_nodes = max_smem_nodes;
+    const size_t smem = static_cast<size_t>(Sl.smem_nodes) * (6 * sizeof(double) + 4 * sizeof(int));
+    cudaError_t e = cudaFuncSetAttribute(k_resume_warp<MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
     int per_sm = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_resume_warp, 128, 0);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_resume_warp<MINB>, 128, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
     long long blocks = static_cast<long long>(per_sm) * sm_count;
     const long long need = (n + 3) / 4;   // four warps (rays) per block
     if (blocks > need) blocks = need;
-    k_resume_warp<<<static_cast<unsigned>(blocks), 128, 0, stream>>>(S, A, W, reqs, rays, n);
+    k_resume_warp<MINB><<<static_cast<unsigned>(blocks), 128, smem, stream>>>(Sl, A, W, reqs, rays, n);
     return cudaGetLastError();
+}
+
+// Tail launch shapes (blocks of 128 threads per SM, BVH nodes staged in
+// shared memory): 0 = 3 blocks, none staged; 1 = 4 blocks, 768 nodes;
+// 2 = 3 blocks, 1024 nodes; 3 = 2 blocks, 1536 nodes.
+cudaError_t launch_resume_warp(const DScene& S, const TraceArgs& A, const WaveArgs& W, const NewtonRequest* reqs,
+                               const int* rays, long long n, int sm_count, int shape, cudaStream_t stream) {
+    if (n <= 0) return cudaSuccess;
+    switch (shape) {
+        case 1: return launch_resume_warp_shape<4>(S, A, W, reqs, rays, n, sm_count, 768, stream);
+        case 2: return launch_resume_warp_shape<3>(S, A, W, reqs, rays, n, sm_count, 1024, stream);
+        case 3: return launch_resume_warp_shape<2>(S, A, W, reqs, rays, n, sm_count, 1536, stream);
+        default: return launch_resume_warp_shape<3>(S, A, W, reqs, rays, n, sm_count, 0, stream);
+    }
 }
 
 // ---- BounceMapDriver::run on the device ------------------------------------
