@@ -66,6 +66,8 @@ def parse():
     ap.add_argument("--train-epochs", type=int, default=20)
     ap.add_argument("--accuracy-rays", type=int, default=262144, help="0 skips the accuracy comparison")
     ap.add_argument("--autotune", type=int, default=1, help="pick the launch schedule on the workload first")
+    ap.add_argument("--multi-scene", type=int, default=0,
+                    help="also time K uneven scenes traced together (bbrt_trace_batch) vs one after another")
     ap.add_argument("--forms", default="plain,split,learned",
                     help="forms to time besides the headline (learned); e.g. 'learned' alone for profiling")
     return ap.parse_args()
@@ -454,9 +456,49 @@ def run_ours(args, rank, world, local_rank):
             if stats else None,
             "wall_s_timed_region": wall,
             "counters_per_step": {k: v for k, v in (stats or {}).items() if k not in ("kernel_ms", "total_ms")}}
+    if args.multi_scene > 0:
+        line["multi_scene"] = multi_scene(args.multi_scene, args.steps, dev)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(patches, o, d, maxb, cn, tol, args.cpu_seconds)
     print(json.dumps(line), flush=True)
+
+
+def multi_scene(k, steps, dev):
+    """k independent scenes of uneven size (scenes.multi_scene_workload:
+    1-32 obstacles of 96 or 384 patches at degree 4 or 6, 16k-1M rays each,
+    <= 100 bounces, plain FP64): device time of tracing them together in one
+    bbrt_trace_batch call vs one after another (the same call with one scene
+    at a time), best of `steps`."""
+    import torch
+    from billardballraytracing3d_b200 import _capi as C
+    from billardballraytracing3d_b200 import api, scenes
+    work = scenes.multi_scene_workload(k)
+    scs, tens = [], []
+    for patches, o, d, maxb, cn, tol in work:
+        sc = api.Scene(patches, config=C.default_config(coarse_grid_n=cn, newton_tol=tol))
+        sc.upload()
+        n = o.shape[0]
+        scs.append(sc)
+        tens.append(dict(o=torch.from_numpy(o).to(dev), d=torch.from_numpy(d).to(dev),
+                         status=torch.zeros(n, dtype=torch.int32, device=dev),
+                         bounce_count=torch.zeros(n, dtype=torch.int32, device=dev)))
+    ns = [w[1].shape[0] for w in work]
+    optr = [t["o"].data_ptr() for t in tens]
+    dptr = [t["d"].data_ptr() for t in tens]
+    outs = [dict(status=t["status"].data_ptr(), bounce_count=t["bounce_count"].data_ptr()) for t in tens]
+    st, _ = api.trace_batch_device(scs, optr, dptr, ns, 100, outs)   # warm-up
+    bounces = st["bounces"]
+    batch = min(api.trace_batch_device(scs, optr, dptr, ns, 100, outs, want_stats=False)[1] for _ in range(steps))
+    for j in range(k):   # warm-up one at a time
+        api.trace_batch_device([scs[j]], [optr[j]], [dptr[j]], [ns[j]], 100, [outs[j]], want_stats=False)
+    seq = min(sum(api.trace_batch_device([scs[j]], [optr[j]], [dptr[j]], [ns[j]], 100, [outs[j]],
+                                         want_stats=False)[1] for j in range(k)) for _ in range(steps))
+    return {"scenes": k, "rays": int(sum(ns)), "patches": int(sum(len(w[0]) for w in work)),
+            "bounces": int(bounces), "batched_ms": batch, "sequential_ms": seq,
+            "batched_value": bounces / (batch / 1e3), "sequential_value": bounces / (seq / 1e3),
+            "unit": UNIT, "speedup": seq / batch,
+            "note": "device time of one bbrt_trace_batch call over all scenes vs the sum over one-scene calls; "
+                    "plain FP64 form, default schedule"}
 
 
 def main():

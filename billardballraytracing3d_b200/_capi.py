@@ -289,6 +289,8 @@ def _declare(lib):
     lib.bbrt_umma_check.argtypes = [ctypes.POINTER(ctypes.c_ushort), ctypes.POINTER(ctypes.c_ushort),
                                     ctypes.POINTER(ctypes.c_float)]
     lib.bbrt_scene_set_modes.argtypes = [V, I, I]
+    lib.bbrt_trace_batch.argtypes = [ctypes.POINTER(V), I, ctypes.POINTER(V), ctypes.POINTER(V), c_ll_p, I,
+                                     ctypes.POINTER(TraceOut), ctypes.POINTER(TraceStats), c_double_p]
     lib.bbrt_scene_get_tuning.argtypes = [V, ctypes.POINTER(Tuning)]
     lib.bbrt_scene_set_tuning.argtypes = [V, ctypes.POINTER(Tuning)]
     lib.bbrt_scene_autotune.argtypes = [V, c_double_p, c_double_p, LL, I, I, ctypes.POINTER(Tuning), c_double_p, V]

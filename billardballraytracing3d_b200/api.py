@@ -245,6 +245,37 @@ class Scene:
         return o, d
 
 
+def trace_batch_device(scenes: Sequence["Scene"], origin_ptrs, dir_ptrs, ns, max_bounces: int, outs=None,
+                       want_stats: bool = True):
+    """bbrt_trace_batch: every scene's rays (device pointers, e.g. torch
+    tensors' data_ptr()) traced with all scenes in flight together.
+    outs: per scene a dict of device pointers (status, bounce_count, exit_dir,
+    hit_object, hit_point with 'record'), or None.  Returns (stats, batch_ms)."""
+    lib = C.load_library()
+    k = len(scenes)
+    hs = (ctypes.c_void_p * k)(*[s.h for s in scenes])
+    op = (ctypes.c_void_p * k)(*[ctypes.c_void_p(p) for p in origin_ptrs])
+    dp = (ctypes.c_void_p * k)(*[ctypes.c_void_p(p) for p in dir_ptrs])
+    nn = (ctypes.c_longlong * k)(*[int(v) for v in ns])
+    to = None
+    if outs is not None:
+        to = (C.TraceOut * k)()
+        for j, od in enumerate(outs):
+            if not od:
+                continue
+            to[j].record_bounces = int(od.get("record", 0))
+            for key, v in od.items():
+                if key == "record":
+                    continue
+                ct = ctypes.c_int if key in ("status", "bounce_count", "hit_object", "err_object") else ctypes.c_double
+                setattr(to[j], key, ctypes.cast(ctypes.c_void_p(v), ctypes.POINTER(ct)))
+    st = C.TraceStats()
+    ms = ctypes.c_double()
+    C.check(lib, lib.bbrt_trace_batch(hs, k, op, dp, nn, int(max_bounces), to, ctypes.byref(st) if want_stats else None,
+                                      ctypes.byref(ms)), "bbrt_trace_batch")
+    return (st.as_dict() if want_stats else None), ms.value
+
+
 def sample_grid(patch, n: int):
     """SurfacePatch::sample_grid(n) through the C ABI: (xyz, normal, dX/du)."""
     lib = C.load_library()

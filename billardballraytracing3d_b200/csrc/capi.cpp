@@ -485,45 +485,69 @@ cudaError_t run_tail(bbrt_scene* s, const bbrt::TraceArgs& A, const bbrt::WaveAr
     return bbrt::launch_resume(s->dev, A, W, reqs, rays, n, st);
 }
 
-int run_wavefront(bbrt_scene* s, const bbrt::TraceArgs& A, cudaStream_t st) {
-    const long long n = A.n;
-    const bbrt_tuning T = scene_tuning(s);
-    const int log_rounds = tuning().log_rounds;
-    BBRT_CUDA(s->wave.ensure(bbrt::wave_workspace_bytes(n)));
-    BBRT_CUDA(s->wave_ctr.ensure(3 * sizeof(unsigned int)));
-    if (!s->wave_ctr_host) BBRT_CUDA(cudaMallocHost(&s->wave_ctr_host, 2 * sizeof(unsigned int)));
+// One scene's wavefront trace as a resumable sequence, so that several
+// scenes can advance round by round together (bbrt_trace_batch): begin()
+// queues the ordering and round 0 and the readback of its counters; after
+// that readback has completed, step() queues the next round (or the tail)
+// until done; finish() runs the tail of rays that overflowed the resolved
+// list.  run_wavefront() is the one-scene loop over the same steps.
+struct WaveRun {
+    bbrt_scene* s = nullptr;
+    bbrt::TraceArgs A;
+    cudaStream_t st = nullptr;
+    bbrt_tuning T{};
+    int log_rounds = 0;
     bbrt::WaveArgs W;
     bbrt::NewtonRequest *req_a = nullptr, *req_b = nullptr;
-    bbrt::wave_layout(s->wave.p, n, W, req_a, req_b);
-    W.counters = static_cast<unsigned int*>(s->wave_ctr.p);
-    W.warp_stage1 = T.warp_stage1;
-    W.resume_queries = tuning().resume_queries;
-    W.runnable = nullptr;
-    W.n_runnable = n;
-    W.req = req_a;
-    if (T.order_rays) {
-        BBRT_CUDA(s->order_ws.ensure(bbrt::ray_order_workspace_bytes(n)));
-        BBRT_CUDA(s->order.ensure(sizeof(int) * static_cast<size_t>(n)));
-        const double radius = s->cull.radius > 0.0 ? s->cull.radius : s->host.scene_diagonal;
-        BBRT_CUDA(timed(s, K_ORDER, st, [&] {
-            return bbrt::ray_order(A.origins, A.dirs, n, s->cull.center, radius, s->order_ws.p,
-                                   static_cast<int*>(s->order.p), st);
-        }));
-        W.order = static_cast<const int*>(s->order.p);
+    long long round = 0, max_rounds = 0, overflowed = 0;
+    bool done = false;
+
+    int begin(bbrt_scene* s_, const bbrt::TraceArgs& A_, cudaStream_t st_) {
+        s = s_;
+        A = A_;
+        st = st_;
+        const long long n = A.n;
+        T = scene_tuning(s);
+        log_rounds = tuning().log_rounds;
+        BBRT_CUDA(s->wave.ensure(bbrt::wave_workspace_bytes(n)));
+        BBRT_CUDA(s->wave_ctr.ensure(3 * sizeof(unsigned int)));
+        if (!s->wave_ctr_host) BBRT_CUDA(cudaMallocHost(&s->wave_ctr_host, 2 * sizeof(unsigned int)));
+        bbrt::wave_layout(s->wave.p, n, W, req_a, req_b);
+        W.counters = static_cast<unsigned int*>(s->wave_ctr.p);
+        W.warp_stage1 = T.warp_stage1;
+        W.resume_queries = tuning().resume_queries;
+        W.runnable = nullptr;
+        W.n_runnable = n;
+        W.req = req_a;
+        if (T.order_rays) {
+            BBRT_CUDA(s->order_ws.ensure(bbrt::ray_order_workspace_bytes(n)));
+            BBRT_CUDA(s->order.ensure(sizeof(int) * static_cast<size_t>(n)));
+            const double radius = s->cull.radius > 0.0 ? s->cull.radius : s->host.scene_diagonal;
+            BBRT_CUDA(timed(s, K_ORDER, st, [&] {
+                return bbrt::ray_order(A.origins, A.dirs, n, s->cull.center, radius, s->order_ws.p,
+                                       static_cast<int*>(s->order.p), st);
+            }));
+            W.order = static_cast<const int*>(s->order.p);
+        }
+        BBRT_CUDA(cudaMemsetAsync(W.counters, 0, 3 * sizeof(unsigned int), st));
+        // every round finishes at least one query or one Newton solve of each runnable ray
+        max_rounds = 4 + static_cast<long long>(A.max_bounces + 1) * (s->host.n_objects + 1);
+        return launch_round();
     }
-    BBRT_CUDA(cudaMemsetAsync(W.counters, 0, 3 * sizeof(unsigned int), st));
-    // every round finishes at least one query or one Newton solve of each runnable ray
-    const long long max_rounds = 4 + static_cast<long long>(A.max_bounces + 1) * (s->host.n_objects + 1);
-    long long overflowed = 0;
-    for (long long round = 0; round < max_rounds; ++round) {
+
+    int launch_round() {
         if (log_rounds) BBRT_CUDA(cudaEventRecord(s->ev[2], st));
         BBRT_CUDA(cudaMemsetAsync(W.counters, 0, sizeof(unsigned int), st));
         BBRT_CUDA(cudaMemsetAsync(W.counters + 2, 0, sizeof(unsigned int), st));
-        BBRT_CUDA(timed(s, K_ADVANCE, st, [&] { return bbrt::launch_advance(s->dev, A, W, s->sm_count, T.advance_shape, st); }));
+        BBRT_CUDA(timed(s, K_ADVANCE, st,
+                        [&] { return bbrt::launch_advance(s->dev, A, W, s->sm_count, T.advance_shape, st); }));
         ++s->rounds;
         if (log_rounds) BBRT_CUDA(cudaEventRecord(s->ev[3], st));
         BBRT_CUDA(cudaMemcpyAsync(s->wave_ctr_host, W.counters, 2 * sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
-        BBRT_CUDA(cudaStreamSynchronize(st));
+        return BBRT_OK;
+    }
+
+    int step() {
         const long long n_req = s->wave_ctr_host[0];
         overflowed = s->wave_ctr_host[1];
         if (log_rounds) {
@@ -532,10 +556,14 @@ int run_wavefront(bbrt_scene* s, const bbrt::TraceArgs& A, cudaStream_t st) {
             std::fprintf(stderr, "bbrt round %lld: runnable %lld advance %.3f ms -> requests %lld overflow %lld\n",
                          round, W.n_runnable, ms, n_req, overflowed);
         }
-        if (n_req == 0) break;
+        if (n_req == 0) {
+            done = true;
+            return BBRT_OK;
+        }
         if (n_req <= T.wave_tail) {
             BBRT_CUDA(timed(s, K_TAIL, st, [&] { return run_tail(s, A, W, W.req, nullptr, n_req, st); }));
-            break;
+            done = true;
+            return BBRT_OK;
         }
         if (log_rounds) BBRT_CUDA(cudaEventRecord(s->ev[2], st));
         W.guess = nullptr;
@@ -562,19 +590,36 @@ int run_wavefront(bbrt_scene* s, const bbrt::TraceArgs& A, cudaStream_t st) {
         W.runnable = W.req;
         W.n_runnable = n_req;
         W.req = (W.req == req_a) ? req_b : req_a;
-        if (round + 1 == max_rounds) return fail(BBRT_ERR_KERNEL, "bbrt_trace: wavefront round bound reached");
+        if (++round == max_rounds) return fail(BBRT_ERR_KERNEL, "bbrt_trace: wavefront round bound reached");
+        return launch_round();
     }
-    if (overflowed > 0)
-        BBRT_CUDA(timed(s, K_TAIL, st, [&] { return run_tail(s, A, W, nullptr, W.overflow, overflowed, st); }));
-    return BBRT_OK;
+
+    int finish() {
+        if (overflowed > 0)
+            BBRT_CUDA(timed(s, K_TAIL, st, [&] { return run_tail(s, A, W, nullptr, W.overflow, overflowed, st); }));
+        return BBRT_OK;
+    }
+};
+
+int run_wavefront(bbrt_scene* s, const bbrt::TraceArgs& A, cudaStream_t st) {
+    WaveRun w;
+    int rc = w.begin(s, A, st);
+    while (!rc && !w.done) {
+        BBRT_CUDA(cudaStreamSynchronize(st));
+        rc = w.step();
+    }
+    if (rc) return rc;
+    return w.finish();
 }
 
 // Launches the trace kernel on device arrays.  hit_counts (device, may be
 // null) receives per-object counts for bounces with index >= count_from.
-int run_trace_device(bbrt_scene* s, const double* d_o, const double* d_d, long long n, int max_bounces,
-                     const bbrt_trace_out* out_dev, unsigned long long* hit_counts, int count_from,
-                     cudaStream_t st, bool want_stats, long long* host_stats, float* kernel_ms) {
-    bbrt::TraceArgs A;
+// Trace arguments of one call and the per-call resets (statistics, ray
+// counter, per-kernel timing); records the call's start event.
+int prepare_trace(bbrt_scene* s, const double* d_o, const double* d_d, long long n, int max_bounces,
+                  const bbrt_trace_out* out_dev, unsigned long long* hit_counts, int count_from, cudaStream_t st,
+                  bool want_stats, bbrt::TraceArgs& A) {
+    A = bbrt::TraceArgs();
     A.origins = d_o;
     A.dirs = d_d;
     A.n = n;
@@ -610,12 +655,11 @@ int run_trace_device(bbrt_scene* s, const double* d_o, const double* d_d, long l
     s->rounds = 0;
     s->launches = 0;
     BBRT_CUDA(cudaEventRecord(s->ev[0], st));
-    if (n < scene_tuning(s).wave_min_rays) {
-        BBRT_CUDA(timed(s, K_TAIL, st, [&] { return bbrt::launch_trace(s->dev, A, st, s->sm_count); }));
-    } else {
-        const int rc = run_wavefront(s, A, st);
-        if (rc) return rc;
-    }
+    return BBRT_OK;
+}
+
+// Records the call's end event and queues the statistics readback.
+int complete_trace(bbrt_scene* s, cudaStream_t st, bool want_stats, long long* host_stats, float* kernel_ms) {
     BBRT_CUDA(cudaEventRecord(s->ev[1], st));
     if (want_stats) {
         BBRT_CUDA(cudaMemcpyAsync(host_stats, s->stats.p, sizeof(long long) * bbrt::ST_COUNT,
@@ -626,6 +670,23 @@ int run_trace_device(bbrt_scene* s, const double* d_o, const double* d_d, long l
         BBRT_CUDA(cudaEventElapsedTime(kernel_ms, s->ev[0], s->ev[1]));
     }
     return BBRT_OK;
+}
+
+// Launches the trace kernel on device arrays.  hit_counts (device, may be
+// null) receives per-object counts for bounces with index >= count_from.
+int run_trace_device(bbrt_scene* s, const double* d_o, const double* d_d, long long n, int max_bounces,
+                     const bbrt_trace_out* out_dev, unsigned long long* hit_counts, int count_from,
+                     cudaStream_t st, bool want_stats, long long* host_stats, float* kernel_ms) {
+    bbrt::TraceArgs A;
+    int rc = prepare_trace(s, d_o, d_d, n, max_bounces, out_dev, hit_counts, count_from, st, want_stats, A);
+    if (rc) return rc;
+    if (n < scene_tuning(s).wave_min_rays) {
+        BBRT_CUDA(timed(s, K_TAIL, st, [&] { return bbrt::launch_trace(s->dev, A, st, s->sm_count); }));
+    } else {
+        rc = run_wavefront(s, A, st);
+        if (rc) return rc;
+    }
+    return complete_trace(s, st, want_stats, host_stats, kernel_ms);
 }
 
 }  // namespace
@@ -1705,4 +1766,123 @@ BBRT_API int bbrt_scene_autotune(bbrt_scene_t s, const double* origins, const do
     if (best) *best = cur;
     if (best_ms) *best_ms = cur_ms;
     return BBRT_OK;
+}
+
+// ---- several scenes together -----------------------------------------------
+
+BBRT_API int bbrt_trace_batch(const bbrt_scene_t* scenes, int n_scenes, const double* const* origins,
+                              const double* const* dirs, const long long* n, int max_bounces,
+                              const bbrt_trace_out* outs, bbrt_trace_stats* stats, double* batch_ms) {
+    if (!scenes || !origins || !dirs || !n || n_scenes < 1) return fail(BBRT_ERR_ARG, "bbrt_trace_batch: bad argument");
+    if (max_bounces < 0) return fail(BBRT_ERR_ARG, "bbrt_trace_batch: max_bounces < 0");
+    std::vector<bbrt_scene*> order;
+    for (int k = 0; k < n_scenes; ++k) {
+        if (!scenes[k]) return fail(BBRT_ERR_ARG, "bbrt_trace_batch: NULL scene");
+        if (n[k] < 0 || (n[k] > 0 && (!origins[k] || !dirs[k])))
+            return fail(BBRT_ERR_ARG, "bbrt_trace_batch: bad rays of scene " + std::to_string(k));
+        order.push_back(scenes[k]);
+    }
+    std::sort(order.begin(), order.end());
+    if (std::adjacent_find(order.begin(), order.end()) != order.end())
+        return fail(BBRT_ERR_ARG, "bbrt_trace_batch: a scene appears twice in the batch");
+    std::vector<std::unique_lock<std::mutex>> locks;
+    for (bbrt_scene* sc : order) locks.emplace_back(sc->mu);   // address order: no lock cycles
+    for (int k = 0; k < n_scenes; ++k) {
+        const int rc = ensure_uploaded(scenes[k]);
+        if (rc) return rc;
+    }
+    // One device timeline for the whole batch: every scene's stream waits on
+    // a start event, and the end event waits on every scene's stream.
+    cudaStream_t bs = scenes[0]->stream;
+    cudaEvent_t start = nullptr, end = nullptr;
+    BBRT_CUDA(cudaEventCreate(&start));
+    if (cudaEventCreate(&end) != cudaSuccess) {
+        cudaEventDestroy(start);
+        return fail(BBRT_ERR_CUDA, "bbrt_trace_batch: cudaEventCreate failed");
+    }
+    auto cleanup = [&]() { cudaEventDestroy(start); cudaEventDestroy(end); };
+    const bool want = stats != nullptr;
+    std::vector<WaveRun> runs(n_scenes);
+    std::vector<std::vector<long long>> hs(n_scenes, std::vector<long long>(bbrt::ST_COUNT, 0));
+    int rc = BBRT_OK;
+    if (cudaEventRecord(start, bs) != cudaSuccess) rc = fail(BBRT_ERR_CUDA, "bbrt_trace_batch: cudaEventRecord failed");
+    for (int k = 0; k < n_scenes && !rc; ++k) {
+        bbrt_scene* s = scenes[k];
+        if (s->stream != bs && cudaStreamWaitEvent(s->stream, start, 0) != cudaSuccess) {
+            rc = fail(BBRT_ERR_CUDA, "bbrt_trace_batch: cudaStreamWaitEvent failed");
+            break;
+        }
+        bbrt::TraceArgs A;
+        rc = prepare_trace(s, origins[k], dirs[k], n[k], max_bounces, outs ? &outs[k] : nullptr, nullptr, 1, s->stream,
+                           want, A);
+        if (rc) break;
+        if (n[k] < scene_tuning(s).wave_min_rays) {
+            if (n[k] > 0) {
+                const cudaError_t e = timed(s, K_TAIL, s->stream, [&] { return bbrt::launch_trace(s->dev, A, s->stream, s->sm_count); });
+                if (e != cudaSuccess) rc = fail(BBRT_ERR_CUDA, std::string("bbrt_trace_batch: ") + cudaGetErrorString(e));
+            }
+            runs[k].s = s;
+            runs[k].done = true;
+        } else {
+            rc = runs[k].begin(s, A, s->stream);
+        }
+    }
+    // rounds of all scenes together: one wait per round for the whole batch
+    bool active = true;
+    while (!rc && active) {
+        active = false;
+        for (int k = 0; k < n_scenes && !rc; ++k) {
+            if (runs[k].done) continue;
+            if (cudaStreamSynchronize(scenes[k]->stream) != cudaSuccess) {
+                rc = fail(BBRT_ERR_CUDA, "bbrt_trace_batch: stream synchronisation failed");
+                break;
+            }
+            rc = runs[k].step();
+            if (!runs[k].done) active = true;
+        }
+    }
+    for (int k = 0; k < n_scenes && !rc; ++k) {
+        if (runs[k].s && n[k] >= scene_tuning(scenes[k]).wave_min_rays) rc = runs[k].finish();
+        if (!rc) rc = complete_trace(scenes[k], scenes[k]->stream, want, hs[k].data(), nullptr);
+        if (!rc && scenes[k]->stream != bs) {
+            cudaEvent_t e = scenes[k]->ev[1];
+            if (cudaStreamWaitEvent(bs, e, 0) != cudaSuccess) rc = fail(BBRT_ERR_CUDA, "bbrt_trace_batch: cudaStreamWaitEvent failed");
+        }
+    }
+    if (!rc && cudaEventRecord(end, bs) != cudaSuccess) rc = fail(BBRT_ERR_CUDA, "bbrt_trace_batch: cudaEventRecord failed");
+    if (!rc && cudaEventSynchronize(end) != cudaSuccess) rc = fail(BBRT_ERR_CUDA, "bbrt_trace_batch: synchronisation failed");
+    for (int k = 0; k < n_scenes && !rc; ++k)
+        if (cudaStreamSynchronize(scenes[k]->stream) != cudaSuccess) rc = fail(BBRT_ERR_CUDA, "bbrt_trace_batch: synchronisation failed");
+    if (!rc && batch_ms) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, start, end);
+        *batch_ms = ms;
+    }
+    if (!rc && stats) {
+        std::memset(stats, 0, sizeof *stats);
+        for (int k = 0; k < n_scenes; ++k) {
+            bbrt_trace_stats one;
+            float kms = 0.0f;
+            cudaEventElapsedTime(&kms, scenes[k]->ev[0], scenes[k]->ev[1]);
+            fill_stats(scenes[k], hs[k].data(), n[k], kms, kms, &one);
+            stats->rays += one.rays;
+            stats->bounces += one.bounces;
+            stats->queries += one.queries;
+            stats->node_tests += one.node_tests;
+            stats->patch_tests += one.patch_tests;
+            stats->cell_tests += one.cell_tests;
+            stats->tri_tests += one.tri_tests;
+            stats->newton_iters += one.newton_iters;
+            stats->newton_iters_fp32 += one.newton_iters_fp32;
+            for (int q = 0; q < BBRT_RAY_STATUS_COUNT; ++q) stats->status_hist[q] += one.status_hist[q];
+            stats->rounds += one.rounds;
+            stats->launches += one.launches;
+            stats->tail_rays += one.tail_rays;
+            stats->guess_used += one.guess_used;
+            stats->guess_fallback += one.guess_fallback;
+        }
+        if (batch_ms) stats->kernel_ms = stats->total_ms = *batch_ms;
+    }
+    cleanup();
+    return rc;
 }

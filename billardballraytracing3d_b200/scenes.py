@@ -397,6 +397,35 @@ def cone_rays(n: int, seed: int, plane_z: float, half_extent: float, cone_half_d
 # ---------------------------------------------------------------------------
 # named workloads
 # ---------------------------------------------------------------------------
+def multi_scene_workload(n_scenes: int, seed: int = 77, max_obstacles: int = 32, min_rays: int = 16384,
+                         max_rays: int = 1 << 20):
+    """Independent scenes of uneven size (the batched multi-scene case): each
+    has a seeded count of 1..max_obstacles spheres or ellipsoids (semi-axes
+    U[0.2,1.2], random rotations, centres in [-6,6]^3 with gap >= 0.2), each
+    obstacle 6*4*4 = 96 or 6*8*8 = 384 patches of degree 4 (5x5 nodes) or 6
+    (7x7), coarse grid 17x17, and a log-uniform count of rays in
+    [min_rays, max_rays] from z = 8 over [-6,6]^2 in a 20-degree cone, <= 100
+    bounces, Newton tolerance 1e-12.  Returns a list of
+    (patches, origins, dirs, max_bounces, coarse_n, newton_tol)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for k in range(n_scenes):
+        count = int(rng.integers(1, max_obstacles + 1))
+        objs = random_ellipsoids(rng, count)
+        patches = []
+        for j, (cen, axes, rot) in enumerate(objs):
+            if rng.random() < 0.5:   # sphere
+                r = axes[0]
+                axes, rot = (r, r, r), None
+            m = 4 if rng.random() < 0.5 else 8
+            nn = 5 if rng.random() < 0.5 else 7
+            patches += obstacle_patches(j, cen, axes, rot, m=m, n_nodes=nn)
+        n_rays = int(round(np.exp(rng.uniform(np.log(min_rays), np.log(max_rays)))))
+        o, d = cone_rays(n_rays, int(rng.integers(1, 1 << 30)), 8.0, 6.0, 20.0)
+        out.append((patches, o, d, 100, 17, 1e-12))
+    return out
+
+
 def workload(name: str, n_rays: int = None):
     """(patches, origins, dirs, max_bounces, coarse_n, newton_tol) of a named workload.
 

@@ -368,6 +368,20 @@ BBRT_API int  bbrt_mlp_check(const float* params, int n_patches, const float* fe
 BBRT_API int  bbrt_mlp_infer_check(const float* params, int n_patches, const float* feat, const int* patch,
                                    int rows, double* out);
 
+/* ---- several scenes together (no reference counterpart) ----------------
+ *
+ * Traces the ray batch of each scene (device arrays, as with BBRT_DEVICE_PTRS;
+ * scenes distinct) with all scenes in flight together: each scene's trace
+ * runs on its own stream and the wavefront rounds of all scenes interleave,
+ * with one host wait per round for the whole batch, so small scenes run
+ * alongside large ones instead of one after the other.  Each scene's results
+ * are those of bbrt_trace on it alone.  stats (optional) sums the counters of
+ * all scenes; batch_ms (optional) is the device time from the batch's first
+ * launch to its last. */
+BBRT_API int bbrt_trace_batch(const bbrt_scene_t* scenes, int n_scenes, const double* const* origins,
+                              const double* const* dirs, const long long* n, int max_bounces,
+                              const bbrt_trace_out* outs, bbrt_trace_stats* stats, double* batch_ms);
+
 /* ---- launch schedule and its autotuner (no reference counterpart) --------
  *
  * The schedule changes only the order and grouping of work, never a result

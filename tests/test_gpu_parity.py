@@ -263,3 +263,36 @@ def test_autotune_keeps_results(built, workloads):
     tuned = sc.trace(o, d, maxb, record=4, outputs=("status", "bounce_count", "hit_object", "hit_point", "exit_dir"))
     for k in ("status", "bounce_count", "hit_object", "hit_point", "exit_dir"):
         assert np.array_equal(base[k], tuned[k]), k
+
+
+def test_trace_batch_equals_single_scene_traces(built):
+    """bbrt_trace_batch traces uneven scenes together; each scene's results are
+    bit-identical to tracing it alone (wavefront and fused-kernel sizes mixed)."""
+    import torch
+    work = scenes.multi_scene_workload(4, seed=5, max_obstacles=6, min_rays=4000, max_rays=60000)
+    scs, tens, outs, refs = [], [], [], []
+    K = 4
+    for patches, o, d, maxb, cn, tol in work:
+        sc = api.Scene(patches, config=C.default_config(coarse_grid_n=cn, newton_tol=tol))
+        refs.append(sc.trace(o, d, maxb, record=K, outputs=("status", "bounce_count", "exit_dir", "hit_object",
+                                                             "hit_point")))
+        n = o.shape[0]
+        t = dict(o=torch.from_numpy(o).cuda(), d=torch.from_numpy(d).cuda(),
+                 status=torch.zeros(n, dtype=torch.int32, device="cuda"),
+                 bounce_count=torch.zeros(n, dtype=torch.int32, device="cuda"),
+                 exit_dir=torch.zeros((n, 3), dtype=torch.float64, device="cuda"),
+                 hit_object=torch.zeros((n, K), dtype=torch.int32, device="cuda"),
+                 hit_point=torch.zeros((n, K, 3), dtype=torch.float64, device="cuda"))
+        scs.append(sc)
+        tens.append(t)
+        outs.append(dict(record=K, **{k: t[k].data_ptr() for k in ("status", "bounce_count", "exit_dir", "hit_object",
+                                                                     "hit_point")}))
+    assert min(o.shape[0] for _, o, _, _, _, _ in work) < 8192 <= max(o.shape[0] for _, o, _, _, _, _ in work)
+    st, ms = api.trace_batch_device(scs, [t["o"].data_ptr() for t in tens], [t["d"].data_ptr() for t in tens],
+                                    [w[1].shape[0] for w in work], 100, outs)
+    torch.cuda.synchronize()
+    assert ms > 0 and st["rays"] == sum(w[1].shape[0] for w in work)
+    for ref, t in zip(refs, tens):
+        for k in ("status", "bounce_count", "exit_dir", "hit_object", "hit_point"):
+            assert np.array_equal(ref[k], t[k].cpu().numpy()), k
+    assert st["bounces"] == sum(int(r["bounce_count"].sum()) for r in refs)
