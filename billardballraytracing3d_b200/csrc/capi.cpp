@@ -270,7 +270,11 @@ int ensure_uploaded(bbrt_scene* s) {
     // with several blocks per SM stage fewer
     D.smem_nodes = static_cast<int>(std::min<size_t>(nn, 3400));
     std::vector<int> dims(2 * static_cast<size_t>(H.n_patches));
-    for (int q = 0; q < H.n_patches; ++q) { dims[2 * q] = H.p_imax[q]; dims[2 * q + 1] = H.p_jmax[q]; }
+    for (int q = 0; q < H.n_patches; ++q) {
+        dims[2 * q] = H.p_imax[q];
+        dims[2 * q + 1] = H.p_jmax[q];
+        D.max_nodes = std::max(D.max_nodes, std::max(H.p_imax[q], H.p_jmax[q]));
+    }
     int rc;
     if ((rc = s->upload(nbox, D.node_box))) return rc;
     if ((rc = s->upload(nlink, D.node_link))) return rc;
@@ -423,6 +427,7 @@ struct Tuning {
     int warp_stage1 = 1;              // k_advance runs each patch's stage 1 with the whole warp
     int resume_queries = 1;           // suspended queries resume where they stopped (else replay from the root)
     int tail_shape = 0;               // k_resume_warp launch shape (see launch_resume_warp)
+    int group_newton = 0;             // k_newton by 8-lane groups (exact, measured slower: off)
 };
 
 // Launch-shape knobs; defaults tuned on B200, overridable for experiments by
@@ -440,6 +445,7 @@ const Tuning& tuning() {
         if (const char* e = std::getenv("BBRT_WARP_S1")) v.warp_stage1 = std::atoi(e);
         if (const char* e = std::getenv("BBRT_RESUME")) v.resume_queries = std::atoi(e);
         if (const char* e = std::getenv("BBRT_TAIL_SHAPE")) v.tail_shape = std::atoi(e);
+        if (const char* e = std::getenv("BBRT_GROUP_NEWTON")) v.group_newton = std::atoi(e);
         return v;
     }();
     return t;
@@ -516,6 +522,7 @@ struct WaveRun {
         W.counters = static_cast<unsigned int*>(s->wave_ctr.p);
         W.warp_stage1 = T.warp_stage1;
         W.resume_queries = tuning().resume_queries;
+        W.group_newton = tuning().group_newton;
         W.runnable = nullptr;
         W.n_runnable = n;
         W.req = req_a;

@@ -43,6 +43,7 @@ struct DScene {
     const float* p_nodes32 = nullptr;      // FP32 copies (same offsets) for the FP32 Newton phase
     const float* p_fields32 = nullptr;
     int precision = 0;                     // BBRT_PREC_*
+    int max_nodes = 0;                     // largest node count per axis over the patches
     const double* coarse_uv = nullptr;     // [coarse_n]
     const double* c_xyz = nullptr;         // [n_patches][coarse_n^2][3]
     const double* c_cell = nullptr;        // [n_patches][(coarse_n-1)^2][4] normal xyz, sagitta
@@ -150,6 +151,7 @@ struct WaveArgs {
     double* qs_dbl = nullptr;
     int* qs_stack = nullptr;
     int resume_queries = 1;
+    int group_newton = 0;                      // Newton solves by 8-lane groups when the patches allow it
 };
 
 constexpr int kQsInt = 6;

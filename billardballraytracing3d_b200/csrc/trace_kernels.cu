@@ -22,6 +22,7 @@
 #include "../../include/bbrt.h"
 #include "exact.cuh"
 #include "guess.h"
+#include "newton_group.cuh"
 
 namespace bbrt {
 
@@ -1060,6 +1061,63 @@ __global__ void __launch_bounds__(128) k_newton(DScene S, TraceArgs A, WaveArgs 
     }
 }
 
+// k_newton with 8 lanes per request (patches of at most 8 nodes per axis):
+// the same starts, fallbacks and results, bit for bit.
+__global__ void __launch_bounds__(128) k_newton_grp(DScene S, TraceArgs A, WaveArgs W, long long n_req) {
+    const Grp G = make_grp();
+    const long long j = (blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x) / kGroup;
+    long long iters = 0, iters32 = 0, used = 0, fallback = 0;
+    if (j < n_req) {   // uniform over the group
+        const NewtonRequest q = W.req[j];
+        const V3 o = load3(W.o + 3LL * q.ray);
+        const V3 d = load3(W.d + 3LL * q.ray);
+        const int pidx = S.obj_sub[q.obj];
+        QHit h;
+        h.err = 0;
+        h.ev0 = h.ev1 = 0.0;
+        h.t = 0.0;
+        h.p = h.n = v3(0.0, 0.0, 0.0);
+        h.u = h.v = 0.0;
+        bool done = false;
+        if (W.guess) {
+            const double* g = W.guess + 4 * j;
+            const double win = W.guess_t_window * W.frame[16LL * pidx + 12];
+            if (g[3] > W.guess_min_logit && isfinite(g[0]) && isfinite(g[1]) && fabs(g[2] - q.t0) <= win) {
+                used = 1;
+                QHit hg = h;
+                if (grp_newton_mode(S, pidx, o, d, g[0], g[1], g[2], hg, iters, iters32, G) &&
+                    fabs(hg.t - q.t0) <= win) {
+                    h = hg;
+                    done = true;
+                } else {
+                    fallback = 1;
+                }
+            }
+        }
+        if (!done) {
+            double u0, v0;
+            key_to_uv(S, q.key, u0, v0);
+            grp_newton_mode(S, pidx, o, d, u0, v0, q.t0, h, iters, iters32, G);
+        }
+        if (G.g == 0) {
+            if (A.samples && h.err == 0) record_sample(A, 1, o, d, pidx, h.u, h.v, h.t);
+            const long long e = static_cast<long long>(q.ray) * kResolved + q.entry;
+            double* rd = W.res_data + e * kResData;
+            rd[0] = h.t; rd[1] = h.p.x; rd[2] = h.p.y; rd[3] = h.p.z;
+            rd[4] = h.n.x; rd[5] = h.n.y; rd[6] = h.n.z; rd[7] = h.u; rd[8] = h.v; rd[9] = h.ev0; rd[10] = h.ev1;
+            W.res_err[e] = h.err;
+            if (A.ray_work) A.ray_work[4LL * q.ray + 3] += iters + iters32;
+        }
+    }
+    if (G.g != 0) iters = iters32 = used = fallback = 0;
+    if (A.stats) {
+        warp_add(A.stats + ST_NEWTON_ITERS, iters);
+        warp_add(A.stats + ST_NEWTON_ITERS_FP32, iters32);
+        warp_add(A.stats + ST_GUESS_USED, used);
+        warp_add(A.stats + ST_GUESS_FALLBACK, fallback);
+    }
+}
+
 // Finishes rays from their saved state with inline queries (the tail of a
 // wavefront trace, and rays whose query overflowed the resolved list).  The
 // current bounce's query restarts from the root, so the result is the same.
@@ -1410,7 +1468,12 @@ cudaError_t launch_advance(const DScene& S, const TraceArgs& A, const WaveArgs& 
 
 cudaError_t launch_newton(const DScene& S, const TraceArgs& A, const WaveArgs& W, long long n_req, cudaStream_t stream) {
     if (n_req <= 0) return cudaSuccess;
-    k_newton<<<static_cast<unsigned>((n_req + 127) / 128), 128, 0, stream>>>(S, A, W, n_req);
+    if (S.max_nodes <= kGroup && W.group_newton) {
+        const long long threads = n_req * kGroup;
+        k_newton_grp<<<static_cast<unsigned>((threads + 127) / 128), 128, 0, stream>>>(S, A, W, n_req);
+    } else {
+        k_newton<<<static_cast<unsigned>((n_req + 127) / 128), 128, 0, stream>>>(S, A, W, n_req);
+    }
     return cudaGetLastError();
 }
 
