@@ -516,8 +516,8 @@ struct WaveRun {
         T = scene_tuning(s);
         log_rounds = tuning().log_rounds;
         BBRT_CUDA(s->wave.ensure(bbrt::wave_workspace_bytes(n)));
-        BBRT_CUDA(s->wave_ctr.ensure(3 * sizeof(unsigned int)));
-        if (!s->wave_ctr_host) BBRT_CUDA(cudaMallocHost(&s->wave_ctr_host, 2 * sizeof(unsigned int)));
+        BBRT_CUDA(s->wave_ctr.ensure(4 * sizeof(unsigned int)));
+        if (!s->wave_ctr_host) BBRT_CUDA(cudaMallocHost(&s->wave_ctr_host, 4 * sizeof(unsigned int)));
         bbrt::wave_layout(s->wave.p, n, W, req_a, req_b);
         W.counters = static_cast<unsigned int*>(s->wave_ctr.p);
         W.warp_stage1 = T.warp_stage1;
@@ -536,7 +536,7 @@ struct WaveRun {
             }));
             W.order = static_cast<const int*>(s->order.p);
         }
-        BBRT_CUDA(cudaMemsetAsync(W.counters, 0, 3 * sizeof(unsigned int), st));
+        BBRT_CUDA(cudaMemsetAsync(W.counters, 0, 4 * sizeof(unsigned int), st));
         // every round finishes at least one query or one Newton solve of each runnable ray
         max_rounds = 4 + static_cast<long long>(A.max_bounces + 1) * (s->host.n_objects + 1);
         return launch_round();
@@ -550,11 +550,13 @@ struct WaveRun {
                         [&] { return bbrt::launch_advance(s->dev, A, W, s->sm_count, T.advance_shape, st); }));
         ++s->rounds;
         if (log_rounds) BBRT_CUDA(cudaEventRecord(s->ev[3], st));
-        BBRT_CUDA(cudaMemcpyAsync(s->wave_ctr_host, W.counters, 2 * sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
+        BBRT_CUDA(cudaMemcpyAsync(s->wave_ctr_host, W.counters, 4 * sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
         return BBRT_OK;
     }
 
     int step() {
+        if (s->wave_ctr_host[3])
+            return fail(BBRT_ERR_KERNEL, "bbrt_trace: a wavefront round ran past its watchdog and was stopped");
         const long long n_req = s->wave_ctr_host[0];
         overflowed = s->wave_ctr_host[1];
         if (log_rounds) {

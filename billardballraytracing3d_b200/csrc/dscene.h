@@ -134,7 +134,7 @@ struct WaveArgs {
     long long n_runnable = 0;
     NewtonRequest* req = nullptr;              // this round's requests
     unsigned int* counters = nullptr;          // [0] requests of the round, [1] overflowed rays (cumulative),
-                                               // [2] runnable rays fetched this round
+                                               // [2] runnable rays fetched this round, [3] watchdog tripped
     int* overflow = nullptr;                   // rays whose query needs more than kResolved solves
     // Learned guess of this round's requests: guess[r] = (u, v, t, logit), or null.
     const double* guess = nullptr;

@@ -689,6 +689,8 @@ __device__ __forceinline__ bool resume_query(const DScene& S, const TraceArgs& A
 // Advances runnable rays until each needs a Newton solve, overflows its
 // resolved list, or finishes.  Persistent: lanes fetch rays from the
 // runnable set until it is drained.
+constexpr long long kAdvanceWatchdog = 1LL << 35;   // SM cycles
+
 // NT threads per block, MINB blocks per SM requested from the register
 // allocator (launch shape variants of the same body).
 template <int NT, int MINB>
@@ -713,7 +715,15 @@ __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, Wav
     for (int k = threadIdx.x; k < 6 * S.smem_nodes; k += blockDim.x) sbox[k] = S.node_box[k];
     for (int k = threadIdx.x; k < 4 * S.smem_nodes; k += blockDim.x) slink[k] = S.node_link[k];
     __syncthreads();
+    // Watchdog: a launch that runs far past any real trace (about 17 s of SM
+    // clock) records an error and ends instead of holding the GPU.
+    const long long t_start = clock64();
+    unsigned int iter = 0;
     while (true) {
+        if ((++iter & 1023u) == 0u && __any_sync(0xffffffffu, clock64() - t_start > kAdvanceWatchdog)) {
+            if ((threadIdx.x & 31) == 0) atomicOr(&W.counters[3], 1u);
+            break;
+        }
         // ---- one unit of work
         if (mode == M_NODE) {
             if (q.sp == 0) {
