@@ -295,7 +295,18 @@ def _trace_form(scene, to, td, n, maxb, outs, stream, flush, steps, warmup, dev,
     return sum(a.elapsed_time(b) for a, b in evs) / 1e3, wall, stats
 
 
+def replica_rays(workload, o, d, rank):
+    """Replicas (weak scaling): rank 0 traces the workload's own rays, every
+    other rank as many rays of the same source with its own seed (the
+    plane-grid workload has no seed: every rank traces the same grid)."""
+    if rank == 0 or workload not in TRAIN_SOURCE:
+        return o, d
+    from billardballraytracing3d_b200 import scenes
+    return scenes.cone_rays(o.shape[0], 1234 + rank, *TRAIN_SOURCE[workload])
+
+
 def _max_over_ranks(kern_s, total_b, dev, world):
+    """The job's time (max over ranks) and work (sum over ranks)."""
     if world == 1:
         return kern_s, total_b
     import torch
@@ -338,8 +349,7 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     patches, o, d, maxb, cn, tol = scenes.workload(args.workload, args.rays)
-    if rank > 0 and args.workload != "two_spheres":   # replicas: every rank its own seeded rays
-        o, d = scenes.cone_rays(o.shape[0], 1234 + rank, 5.0, 3.0, 10.0)
+    o, d = replica_rays(args.workload, o, d, rank)
     n = o.shape[0]
     cfg = C.default_config(coarse_grid_n=cn, newton_tol=tol, cull=args.cull)
     scene = api.Scene(patches, config=cfg)
