@@ -1035,22 +1035,28 @@ __global__ void __launch_bounds__(128) k_newton(DScene S, TraceArgs A, WaveArgs 
         h.t = 0.0;
         h.p = h.n = v3(0.0, 0.0, 0.0);
         h.u = h.v = 0.0;
-        bool done = false;
+        // One solve for every request, from the guess where it is confident
+        // (one call site, so requests of both kinds in a warp run together);
+        // a second solve from the triangle only for abandoned guesses.
+        double su, sv, st;
+        key_to_uv(S, q.key, su, sv);
+        st = q.t0;
+        double win = 0.0;
         if (W.guess) {
             const double* g = W.guess + 4 * j;
-            const double win = W.guess_t_window * W.frame[16LL * pidx + 12];
+            win = W.guess_t_window * W.frame[16LL * pidx + 12];
             if (g[3] > W.guess_min_logit && isfinite(g[0]) && isfinite(g[1]) && fabs(g[2] - q.t0) <= win) {
                 used = 1;
-                QHit hg = h;
-                if (newton_mode(S, pidx, o, d, g[0], g[1], g[2], hg, iters, iters32) && fabs(hg.t - q.t0) <= win) {
-                    h = hg;
-                    done = true;
-                } else {
-                    fallback = 1;
-                }
+                su = g[0];
+                sv = g[1];
+                st = g[2];
             }
         }
-        if (!done) {
+        const QHit h0 = h;
+        const int ok = newton_mode(S, pidx, o, d, su, sv, st, h, iters, iters32);
+        if (used && !(ok && fabs(h.t - q.t0) <= win)) {
+            fallback = 1;
+            h = h0;
             double u0, v0;
             key_to_uv(S, q.key, u0, v0);
             newton_mode(S, pidx, o, d, u0, v0, q.t0, h, iters, iters32);
