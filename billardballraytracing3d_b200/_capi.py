@@ -178,6 +178,7 @@ class Tuning(ctypes.Structure):
     _fields_ = [
         ("advance_shape", ctypes.c_int), ("warp_stage1", ctypes.c_int), ("order_rays", ctypes.c_int),
         ("warp_tail", ctypes.c_int), ("wave_tail", ctypes.c_longlong), ("wave_min_rays", ctypes.c_longlong),
+        ("graph_rounds", ctypes.c_int),
     ]
 
     def as_dict(self):

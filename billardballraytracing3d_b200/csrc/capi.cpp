@@ -16,6 +16,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <filesystem>
+#include <initializer_list>
 #include <memory>
 #include <mutex>
 #include <numeric>
@@ -38,6 +39,8 @@ cudaError_t launch_advance(const DScene& S, const TraceArgs& A, const WaveArgs& 
                            cudaStream_t stream);
 cudaError_t launch_newton(const DScene& S, const TraceArgs& A, const WaveArgs& W, long long n_req,
                           cudaStream_t stream);
+cudaError_t launch_wave_decide(unsigned int* counters, long long wave_tail, long long max_rounds,
+                               cudaGraphConditionalHandle loop, cudaStream_t stream);
 cudaError_t launch_resume_warp(const DScene& S, const TraceArgs& A, const WaveArgs& W, const NewtonRequest* reqs,
                                const int* rays, long long n, int sm_count, int shape, cudaStream_t stream);
 cudaError_t launch_resume(const DScene& S, const TraceArgs& A, const WaveArgs& W, const NewtonRequest* reqs,
@@ -115,6 +118,17 @@ struct bbrt_scene {
     long long rounds = 0, launches = 0;
     std::vector<std::pair<int, int>> kspans;   // (kernel kind, first event)
     std::mutex mu;
+    // Graph-launched wavefront traces: instantiated graphs of recent argument
+    // sets (most recent last), and the streams they are captured on.
+    struct WaveGraph {
+        std::vector<long long> key;
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        long long launches_fixed = 0, launches_round = 0;   // kernels outside / inside the round loop
+    };
+    static constexpr size_t kWaveGraphs = 4;
+    std::vector<WaveGraph> wgraphs;
+    cudaStream_t cap[2] = { nullptr, nullptr };
 
     // Learned Newton guess: network (FP32 master, BF16 image, Adam moments),
     // per-patch frames, per-request outputs of the current round.
@@ -141,6 +155,12 @@ struct bbrt_scene {
                            &guess.out, &guess.rows })
             b->release();
         if (wave_ctr_host) cudaFreeHost(wave_ctr_host);
+        for (WaveGraph& g : wgraphs) {
+            if (g.exec) cudaGraphExecDestroy(g.exec);
+            if (g.graph) cudaGraphDestroy(g.graph);
+        }
+        for (auto& c : cap)
+            if (c) cudaStreamDestroy(c);
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
         for (auto& e : kev)
@@ -428,6 +448,7 @@ struct Tuning {
     int resume_queries = 1;           // suspended queries resume where they stopped (else replay from the root)
     int tail_shape = 0;               // k_resume_warp launch shape (see launch_resume_warp)
     int group_newton = 0;             // k_newton by 8-lane groups (exact, measured slower: off)
+    int graph_rounds = 1;             // the rounds as one CUDA graph with a device-side loop
 };
 
 // Launch-shape knobs; defaults tuned on B200, overridable for experiments by
@@ -446,6 +467,7 @@ const Tuning& tuning() {
         if (const char* e = std::getenv("BBRT_RESUME")) v.resume_queries = std::atoi(e);
         if (const char* e = std::getenv("BBRT_TAIL_SHAPE")) v.tail_shape = std::atoi(e);
         if (const char* e = std::getenv("BBRT_GROUP_NEWTON")) v.group_newton = std::atoi(e);
+        if (const char* e = std::getenv("BBRT_GRAPH")) v.graph_rounds = std::atoi(e);
         return v;
     }();
     return t;
@@ -481,6 +503,7 @@ bbrt_tuning scene_tuning(const bbrt_scene* s) {
     t.warp_tail = T.warp_tail;
     t.wave_tail = T.wave_tail;
     t.wave_min_rays = T.wave_min_rays;
+    t.graph_rounds = T.graph_rounds;
     return t;
 }
 
@@ -489,6 +512,212 @@ cudaError_t run_tail(bbrt_scene* s, const bbrt::TraceArgs& A, const bbrt::WaveAr
     if (scene_tuning(s).warp_tail)
         return bbrt::launch_resume_warp(s->dev, A, W, reqs, rays, n, s->sm_count, tuning().tail_shape, st);
     return bbrt::launch_resume(s->dev, A, W, reqs, rays, n, st);
+}
+
+// ---- the wavefront trace as one CUDA graph ------------------------------------
+
+// Values a captured graph depends on, flattened (pointers and integers by
+// value, doubles by bit pattern): a graph is reused only for an equal key.
+struct GraphKey {
+    std::vector<long long> v;
+    template <class T>
+    void put(T x) {
+        if constexpr (std::is_pointer<T>::value) {
+            v.push_back(static_cast<long long>(reinterpret_cast<intptr_t>(x)));
+        } else if constexpr (std::is_floating_point<T>::value) {
+            const double d = static_cast<double>(x);
+            long long b = 0;
+            std::memcpy(&b, &d, sizeof b);
+            v.push_back(b);
+        } else {
+            v.push_back(static_cast<long long>(x));
+        }
+    }
+};
+
+// A launched graph-run of the wavefront: its kernel counts outside and inside the round loop.
+struct GraphLaunch {
+    bool on = false;
+    long long fixed = 0, per_round = 0;
+};
+
+// Whether a graph-launched trace stopped on a device-side bound; sets the
+// call's round and launch counts.  After the graph's work has completed.
+int check_wave_graph(bbrt_scene* s, const GraphLaunch& g) {
+    const unsigned int* c = s->wave_ctr_host;
+    if (c[3]) return fail(BBRT_ERR_KERNEL, "bbrt_trace: a wavefront round ran past its watchdog and was stopped");
+    if (c[bbrt::kWcBound]) return fail(BBRT_ERR_KERNEL, "bbrt_trace: wavefront round bound reached");
+    s->rounds = 1 + static_cast<long long>(c[bbrt::kWcRounds]);
+    s->launches = g.fixed + static_cast<long long>(c[bbrt::kWcRounds]) * g.per_round;
+    return BBRT_OK;
+}
+
+// The wavefront trace captured as one graph:
+//   [ray order] -> zero counters -> round 0 -> WHILE(loop) { round } -> tail -> overflow tail -> counters to host
+// where a round is k_advance -> k_wave_decide -> [k_mlp_infer] -> k_newton.
+// k_wave_decide takes the host loop's decision on the device (continue,
+// hand the last small round to the tail, or stop) and sets the loop's
+// condition, so no round waits for the host.  Every launch after round 0
+// reads its item count from the counters; requests are written to req_a by
+// k_advance and copied to req_b (the next round's runnable set) by k_newton.
+int build_wave_graph(bbrt_scene* s, const bbrt::TraceArgs& A, const bbrt_tuning& T, bool learned,
+                     long long max_rounds, bbrt_scene::WaveGraph& out) {
+    for (auto& c : s->cap)
+        if (!c) BBRT_CUDA(cudaStreamCreateWithFlags(&c, cudaStreamNonBlocking));
+    const long long n = A.n;
+    bbrt::WaveArgs W;
+    bbrt::NewtonRequest *req_a = nullptr, *req_b = nullptr;
+    bbrt::wave_layout(s->wave.p, n, W, req_a, req_b);
+    unsigned int* c = static_cast<unsigned int*>(s->wave_ctr.p);
+    W.counters = c;
+    W.warp_stage1 = T.warp_stage1;
+    W.resume_queries = tuning().resume_queries;
+    W.group_newton = tuning().group_newton;
+    W.n_runnable = n;   // sizes the persistent grid; later rounds read their count
+    if (T.order_rays) W.order = static_cast<const int*>(s->order.p);
+    bbrt::WaveArgs W0 = W, Wr = W, Wn = W, Wt = W, Wo = W;
+    W0.req = req_a;                        // round 0: every ray
+    Wr.runnable = req_b;                   // later rounds: last round's requests
+    Wr.req = req_a;
+    Wr.count_dev = c + bbrt::kWcNext;
+    Wn.req = req_a;
+    Wn.next_req = req_b;
+    Wn.count_dev = c + bbrt::kWcNext;
+    double* gout = static_cast<double*>(s->guess.out.p);
+    if (learned) {
+        Wn.guess = gout;
+        Wn.frame = s->guess.frame;
+        Wn.guess_min_logit = s->guess.min_logit;
+        Wn.guess_t_window = s->guess.t_window;
+    }
+    Wt.count_dev = c + bbrt::kWcTail;      // the last, small round's requests
+    Wo.count_dev = c + 1;                  // rays that overflowed the resolved list
+    const bbrt::MlpNet net = learned ? guess_net(s) : bbrt::MlpNet();
+    auto round = [&](cudaStream_t q, const bbrt::WaveArgs& Wa, cudaGraphConditionalHandle loop) -> cudaError_t {
+        cudaError_t e = bbrt::launch_advance(s->dev, A, Wa, s->sm_count, T.advance_shape, q);
+        if (e == cudaSuccess) e = bbrt::launch_wave_decide(c, T.wave_tail, max_rounds, loop, q);
+        if (e == cudaSuccess && learned)
+            e = bbrt::mlp_infer_requests(req_a, n, W.o, W.d, s->dev.obj_sub, s->guess.frame, net, gout, q,
+                                         c + bbrt::kWcNext);
+        if (e == cudaSuccess) e = bbrt::launch_newton(s->dev, A, Wn, n, q);
+        return e;
+    };
+    cudaStream_t cs = s->cap[0], cb = s->cap[1];
+    BBRT_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed));
+    cudaStreamCaptureStatus cst;
+    cudaGraph_t cg = nullptr;
+    cudaGraphConditionalHandle loop = 0;
+    cudaError_t e = cudaStreamGetCaptureInfo(cs, &cst, nullptr, &cg, nullptr, nullptr);
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&loop, cg, 0, cudaGraphCondAssignDefault);
+    if (e == cudaSuccess && T.order_rays) {
+        const double radius = s->cull.radius > 0.0 ? s->cull.radius : s->host.scene_diagonal;
+        e = bbrt::ray_order(A.origins, A.dirs, n, s->cull.center, radius, s->order_ws.p,
+                            static_cast<int*>(s->order.p), cs);
+    }
+    if (e == cudaSuccess) e = cudaMemsetAsync(c, 0, bbrt::kWaveCounters * sizeof(unsigned int), cs);
+    if (e == cudaSuccess) e = round(cs, W0, loop);
+    if (e == cudaSuccess) {
+        const cudaGraphNode_t* deps = nullptr;
+        size_t n_deps = 0;
+        e = cudaStreamGetCaptureInfo(cs, &cst, nullptr, &cg, &deps, &n_deps);
+        cudaGraphNodeParams cp = {};   // reserved fields zero
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = loop;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t cond = nullptr;
+        if (e == cudaSuccess) e = cudaGraphAddNode(&cond, cg, deps, n_deps, &cp);
+        if (e == cudaSuccess) e = cudaStreamUpdateCaptureDependencies(cs, &cond, 1, cudaStreamSetCaptureDependencies);
+        if (e == cudaSuccess) {
+            e = cudaStreamBeginCaptureToGraph(cb, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                              cudaStreamCaptureModeRelaxed);
+            if (e == cudaSuccess) {
+                cudaError_t eb = cudaMemsetAsync(c, 0, sizeof(unsigned int), cb);
+                if (eb == cudaSuccess) eb = cudaMemsetAsync(c + 2, 0, sizeof(unsigned int), cb);
+                if (eb == cudaSuccess) eb = round(cb, Wr, loop);
+                cudaGraph_t body = nullptr;
+                e = cudaStreamEndCapture(cb, &body);
+                if (e == cudaSuccess) e = eb;
+            }
+        }
+    }
+    if (e == cudaSuccess) e = run_tail(s, A, Wt, req_a, nullptr, n, cs);
+    if (e == cudaSuccess) e = run_tail(s, A, Wo, nullptr, W.overflow, n, cs);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(s->wave_ctr_host, c, bbrt::kWaveCounters * sizeof(unsigned int), cudaMemcpyDeviceToHost, cs);
+    cudaGraph_t g = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(cs, &g);
+    if (e == cudaSuccess) e = ee;
+    cudaGraphExec_t x = nullptr;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&x, g, 0);
+    if (e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return fail(BBRT_ERR_CUDA, std::string("bbrt_trace: wavefront graph: ") + cudaGetErrorString(e));
+    }
+    out.graph = g;
+    out.exec = x;
+    const long long per_round = 3 + (learned ? 1 : 0);   // advance, decide, [infer], Newton
+    out.launches_round = per_round;
+    out.launches_fixed = (T.order_rays ? 4 : 0) + per_round + 2;
+    return BBRT_OK;
+}
+
+// Launches the scene's graph for these arguments (captured on first use).
+int launch_wave_graph(bbrt_scene* s, const bbrt::TraceArgs& A, const bbrt_tuning& T, cudaStream_t st,
+                      GraphLaunch& used) {
+    const long long n = A.n;
+    const bool learned = s->host.cfg.guess == BBRT_GUESS_LEARNED && s->guess.trained;
+    if (T.order_rays) {
+        BBRT_CUDA(s->order_ws.ensure(bbrt::ray_order_workspace_bytes(n)));
+        BBRT_CUDA(s->order.ensure(sizeof(int) * static_cast<size_t>(n)));
+    }
+    if (learned) BBRT_CUDA(s->guess.out.ensure(sizeof(double) * 4 * static_cast<size_t>(n)));
+    const long long max_rounds = 4 + static_cast<long long>(A.max_bounces + 1) * (s->host.n_objects + 1);
+    GraphKey k;
+    for (const void* p : std::initializer_list<const void*>{ static_cast<const void*>(A.origins), static_cast<const void*>(A.dirs),
+                           static_cast<const void*>(A.status), static_cast<const void*>(A.bounce_count),
+                           static_cast<const void*>(A.exit_dir), static_cast<const void*>(A.end_point),
+                           static_cast<const void*>(A.hit_object), static_cast<const void*>(A.hit_point),
+                           static_cast<const void*>(A.hit_uv), static_cast<const void*>(A.err_object),
+                           static_cast<const void*>(A.err_value), static_cast<const void*>(A.ray_work),
+                           static_cast<const void*>(A.hit_counts), static_cast<const void*>(A.stats),
+                           static_cast<const void*>(A.work_counter), static_cast<const void*>(A.samples),
+                           static_cast<const void*>(A.sample_count), s->wave.p, s->wave_ctr.p,
+                           static_cast<const void*>(s->wave_ctr_host), s->order.p, s->order_ws.p, s->guess.out.p,
+                           static_cast<const void*>(s->guess.frame), s->guess.image.p, s->guess.P.p,
+                           s->guess.err.p })
+        k.put(p);
+    for (long long x : std::initializer_list<long long>{ A.n, static_cast<long long>(A.max_bounces), static_cast<long long>(A.record),
+                         static_cast<long long>(A.cull), static_cast<long long>(A.count_from), A.sample_cap_pos,
+                         A.sample_cap_neg, static_cast<long long>(s->dev.precision), static_cast<long long>(learned),
+                         static_cast<long long>(T.advance_shape), static_cast<long long>(T.warp_stage1),
+                         static_cast<long long>(T.order_rays), static_cast<long long>(T.warp_tail), T.wave_tail,
+                         static_cast<long long>(tuning().resume_queries), static_cast<long long>(tuning().group_newton),
+                         static_cast<long long>(tuning().tail_shape), max_rounds })
+        k.put(x);
+    k.put(s->guess.min_logit);
+    k.put(s->guess.t_window);
+    auto& gs = s->wgraphs;
+    auto it = std::find_if(gs.begin(), gs.end(), [&](const bbrt_scene::WaveGraph& g) { return g.key == k.v; });
+    if (it == gs.end()) {
+        if (gs.size() == bbrt_scene::kWaveGraphs) {
+            if (gs.front().exec) cudaGraphExecDestroy(gs.front().exec);
+            if (gs.front().graph) cudaGraphDestroy(gs.front().graph);
+            gs.erase(gs.begin());
+        }
+        bbrt_scene::WaveGraph g;
+        const int rc = build_wave_graph(s, A, T, learned, max_rounds, g);
+        if (rc) return rc;
+        g.key = std::move(k.v);
+        gs.push_back(std::move(g));
+    } else if (it + 1 != gs.end()) {
+        std::rotate(it, it + 1, gs.end());   // most recent last
+    }
+    used.on = true;
+    used.fixed = gs.back().launches_fixed;
+    used.per_round = gs.back().launches_round;
+    BBRT_CUDA(cudaGraphLaunch(gs.back().exec, st));
+    return BBRT_OK;
 }
 
 // One scene's wavefront trace as a resumable sequence, so that several
@@ -507,6 +736,7 @@ struct WaveRun {
     bbrt::NewtonRequest *req_a = nullptr, *req_b = nullptr;
     long long round = 0, max_rounds = 0, overflowed = 0;
     bool done = false;
+    GraphLaunch graph;   // graph-launched: check_wave_graph() after completion
 
     int begin(bbrt_scene* s_, const bbrt::TraceArgs& A_, cudaStream_t st_) {
         s = s_;
@@ -516,8 +746,13 @@ struct WaveRun {
         T = scene_tuning(s);
         log_rounds = tuning().log_rounds;
         BBRT_CUDA(s->wave.ensure(bbrt::wave_workspace_bytes(n)));
-        BBRT_CUDA(s->wave_ctr.ensure(4 * sizeof(unsigned int)));
-        if (!s->wave_ctr_host) BBRT_CUDA(cudaMallocHost(&s->wave_ctr_host, 4 * sizeof(unsigned int)));
+        BBRT_CUDA(s->wave_ctr.ensure(bbrt::kWaveCounters * sizeof(unsigned int)));
+        if (!s->wave_ctr_host)
+            BBRT_CUDA(cudaMallocHost(&s->wave_ctr_host, bbrt::kWaveCounters * sizeof(unsigned int)));
+        if (T.graph_rounds) {
+            done = true;
+            return launch_wave_graph(s, A, T, st, graph);
+        }
         bbrt::wave_layout(s->wave.p, n, W, req_a, req_b);
         W.counters = static_cast<unsigned int*>(s->wave_ctr.p);
         W.warp_stage1 = T.warp_stage1;
@@ -604,13 +839,16 @@ struct WaveRun {
     }
 
     int finish() {
+        if (graph.on) return BBRT_OK;   // the overflow tail is part of the graph
         if (overflowed > 0)
             BBRT_CUDA(timed(s, K_TAIL, st, [&] { return run_tail(s, A, W, nullptr, W.overflow, overflowed, st); }));
         return BBRT_OK;
     }
 };
 
-int run_wavefront(bbrt_scene* s, const bbrt::TraceArgs& A, cudaStream_t st) {
+// `graph` describes a graph-launched trace (to be checked once its work has
+// completed); graph.on is false for the host-driven rounds.
+int run_wavefront(bbrt_scene* s, const bbrt::TraceArgs& A, cudaStream_t st, GraphLaunch& graph) {
     WaveRun w;
     int rc = w.begin(s, A, st);
     while (!rc && !w.done) {
@@ -618,6 +856,7 @@ int run_wavefront(bbrt_scene* s, const bbrt::TraceArgs& A, cudaStream_t st) {
         rc = w.step();
     }
     if (rc) return rc;
+    graph = w.graph;
     return w.finish();
 }
 
@@ -689,13 +928,18 @@ int run_trace_device(bbrt_scene* s, const double* d_o, const double* d_d, long l
     bbrt::TraceArgs A;
     int rc = prepare_trace(s, d_o, d_d, n, max_bounces, out_dev, hit_counts, count_from, st, want_stats, A);
     if (rc) return rc;
+    GraphLaunch graph;
     if (n < scene_tuning(s).wave_min_rays) {
         BBRT_CUDA(timed(s, K_TAIL, st, [&] { return bbrt::launch_trace(s->dev, A, st, s->sm_count); }));
     } else {
-        rc = run_wavefront(s, A, st);
+        rc = run_wavefront(s, A, st, graph);
         if (rc) return rc;
     }
-    return complete_trace(s, st, want_stats, host_stats, kernel_ms);
+    rc = complete_trace(s, st, want_stats, host_stats, kernel_ms);
+    if (rc || !graph.on) return rc;
+    // a graph-launched trace: one host wait, for its device-side bounds
+    BBRT_CUDA(cudaEventSynchronize(s->ev[1]));
+    return check_wave_graph(s, graph);
 }
 
 }  // namespace
@@ -1703,6 +1947,7 @@ BBRT_API int bbrt_scene_set_tuning(bbrt_scene_t s, const bbrt_tuning* t) {
     if (!s || !t) return fail(BBRT_ERR_ARG, "bbrt_scene_set_tuning: NULL argument");
     if (t->advance_shape < 0 || t->advance_shape > 6) return fail(BBRT_ERR_ARG, "bbrt_scene_set_tuning: advance_shape must be 0..6");
     if (t->wave_tail < 0 || t->wave_min_rays < 0) return fail(BBRT_ERR_ARG, "bbrt_scene_set_tuning: negative size");
+    if (t->graph_rounds != 0 && t->graph_rounds != 1) return fail(BBRT_ERR_ARG, "bbrt_scene_set_tuning: graph_rounds must be 0 or 1");
     std::lock_guard<std::mutex> g(s->mu);
     s->tune = *t;
     s->tune_set = true;
@@ -1763,6 +2008,13 @@ BBRT_API int bbrt_scene_autotune(bbrt_scene_t s, const double* origins, const do
         if (rc || tl == cur.wave_tail) continue;
         bbrt_tuning c = cur;
         c.wave_tail = tl;
+        double ms = 0.0;
+        rc = time_one(c, ms);
+        if (!rc && ms < cur_ms) { cur = c; cur_ms = ms; }
+    }
+    if (!rc) {   // graph-launched rounds or host-driven ones
+        bbrt_tuning c = cur;
+        c.graph_rounds = cur.graph_rounds ? 0 : 1;
         double ms = 0.0;
         rc = time_one(c, ms);
         if (!rc && ms < cur_ms) { cur = c; cur_ms = ms; }
@@ -1862,6 +2114,8 @@ BBRT_API int bbrt_trace_batch(const bbrt_scene_t* scenes, int n_scenes, const do
     if (!rc && cudaEventSynchronize(end) != cudaSuccess) rc = fail(BBRT_ERR_CUDA, "bbrt_trace_batch: synchronisation failed");
     for (int k = 0; k < n_scenes && !rc; ++k)
         if (cudaStreamSynchronize(scenes[k]->stream) != cudaSuccess) rc = fail(BBRT_ERR_CUDA, "bbrt_trace_batch: synchronisation failed");
+    for (int k = 0; k < n_scenes && !rc; ++k)
+        if (runs[k].graph.on) rc = check_wave_graph(scenes[k], runs[k].graph);
     if (!rc && batch_ms) {
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, start, end);

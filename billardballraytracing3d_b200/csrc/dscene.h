@@ -152,7 +152,22 @@ struct WaveArgs {
     int* qs_stack = nullptr;
     int resume_queries = 1;
     int group_newton = 0;                      // Newton solves by 8-lane groups when the patches allow it
+    // Graph-launched trace: the launch's item count (runnable rays, requests,
+    // tail rays) is read from this device word instead of the host argument,
+    // and the Newton kernel copies each request it solves to next_req (the
+    // next round's runnable set); null in the host-driven trace.
+    const unsigned int* count_dev = nullptr;
+    NewtonRequest* next_req = nullptr;
 };
+
+// Round counters of the wavefront trace in device memory: [0..3] as
+// WaveArgs::counters; the rest are the round control of the graph-launched
+// trace, written by k_wave_decide after each k_advance.
+constexpr int kWcNext = 4;     // requests solved this round, runnable next round (0: rounds end)
+constexpr int kWcTail = 5;     // requests left to the tail kernel (the last, small round)
+constexpr int kWcRounds = 6;   // rounds whose requests went to Newton
+constexpr int kWcBound = 7;    // the round bound was reached
+constexpr int kWaveCounters = 8;
 
 constexpr int kQsInt = 6;
 constexpr int kSaveStack = 24;

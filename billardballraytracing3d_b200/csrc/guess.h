@@ -98,9 +98,10 @@ cudaError_t mlp_train_batch(const MlpBatch& Bt, const MlpNet& M, cudaStream_t st
 cudaError_t mlp_adam(const MlpNet& M, float* m1, float* m2, long long n, float lr, int step, cudaStream_t st);
 cudaError_t mlp_infer_features(const float* feat, const int* pid, long long n, const MlpNet& M, double* out,
                                cudaStream_t st);
+// n_dev (graph launch): the request count is read on the device; n sizes the grid.
 cudaError_t mlp_infer_requests(const NewtonRequest* req, long long n, const double* o, const double* d,
                                const int* obj_sub, const double* frame, const MlpNet& M, double* out,
-                               cudaStream_t st);
+                               cudaStream_t st, const unsigned int* n_dev = nullptr);
 cudaError_t mlp_make_rows(const GuessSample* S, long long n, const double* frame, float* feat, int* pid, float* tgt,
                           float* lbl, cudaStream_t st);
 

@@ -394,10 +394,15 @@ __global__ void __launch_bounds__(128, 1) k_mlp_train(MlpBatch Bt, MlpNet M) {
 // and scale); outputs (u, v, t, logit) per row.
 // TMEM: one 128-column accumulator reused by every layer.
 template <class Rows>
-__global__ void __launch_bounds__(128, 1) k_mlp_infer(Rows rows, long long n, MlpNet M, double* __restrict__ out) {
+__global__ void __launch_bounds__(128, 1) k_mlp_infer(Rows rows, long long n, const unsigned int* n_dev, MlpNet M,
+                                                     double* __restrict__ out) {
     extern __shared__ __align__(1024) uint8_t sm[];
     __shared__ __align__(8) uint64_t mbar_s;
     __shared__ uint32_t tslot;
+    // Graph launch: the row count is on the device; blocks without a tile
+    // leave before loading weights or taking TMEM (uniform over the block).
+    if (n_dev) n = *n_dev;
+    if (blockIdx.x >= (n + 127) / 128) return;
     const int tid = threadIdx.x, warp = tid >> 5;
     load_weights(sm, M.image, M.P, kInferBias);
     const float* sb = reinterpret_cast<const float*>(sm + kInferBias);
@@ -590,7 +595,8 @@ cudaError_t mlp_adam(const MlpNet& M, float* m1, float* m2, long long n, float l
 }
 
 template <class Rows>
-static cudaError_t infer(const Rows& rows, long long n, const MlpNet& M, double* out, cudaStream_t st) {
+static cudaError_t infer(const Rows& rows, long long n, const MlpNet& M, double* out, cudaStream_t st,
+                         const unsigned int* n_dev = nullptr) {
     static bool attr = false;
     if (!attr) {
         cudaError_t e = cudaFuncSetAttribute(k_mlp_infer<Rows>, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmem);
@@ -600,7 +606,7 @@ static cudaError_t infer(const Rows& rows, long long n, const MlpNet& M, double*
     const long long tiles = (n + 127) / 128;
     const long long grid = tiles < sm_count_cached() ? tiles : sm_count_cached();
     if (grid <= 0) return cudaSuccess;
-    k_mlp_infer<Rows><<<static_cast<unsigned>(grid), 128, kInferSmem, st>>>(rows, n, M, out);
+    k_mlp_infer<Rows><<<static_cast<unsigned>(grid), 128, kInferSmem, st>>>(rows, n, n_dev, M, out);
     return cudaGetLastError();
 }
 
@@ -611,8 +617,8 @@ cudaError_t mlp_infer_features(const float* feat, const int* pid, long long n, c
 
 cudaError_t mlp_infer_requests(const NewtonRequest* req, long long n, const double* o, const double* d,
                                const int* obj_sub, const double* frame, const MlpNet& M, double* out,
-                               cudaStream_t st) {
-    return infer(RequestRows{ req, o, d, obj_sub, frame }, n, M, out, st);
+                               cudaStream_t st, const unsigned int* n_dev) {
+    return infer(RequestRows{ req, o, d, obj_sub, frame }, n, M, out, st, n_dev);
 }
 
 cudaError_t mlp_make_rows(const GuessSample* S, long long n, const double* frame, float* feat, int* pid, float* tgt,

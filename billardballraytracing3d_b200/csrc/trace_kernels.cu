@@ -715,6 +715,9 @@ __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, Wav
     for (int k = threadIdx.x; k < 6 * S.smem_nodes; k += blockDim.x) sbox[k] = S.node_box[k];
     for (int k = threadIdx.x; k < 4 * S.smem_nodes; k += blockDim.x) slink[k] = S.node_link[k];
     __syncthreads();
+    // Runnable rays of this round: the host's count, or (graph-launched
+    // trace) the count the previous round's control kernel left on the device.
+    const long long n_run = W.count_dev ? static_cast<long long>(*W.count_dev) : W.n_runnable;
     // Watchdog: a launch that runs far past any real trace (about 17 s of SM
     // clock) records an error and ends instead of holding the GPU.
     const long long t_start = clock64();
@@ -979,7 +982,7 @@ __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, Wav
         const bool need = (mode == M_IDLE);
         const long long fs = warp_append(&W.counters[2], need);
         if (need) {
-            if (fs < W.n_runnable) {
+            if (fs < n_run) {
                 cray = Counters();
                 nres = 0;
                 if (W.runnable == nullptr) {
@@ -1022,10 +1025,13 @@ __device__ __forceinline__ int newton_mode(const DScene& S, int pidx, const V3& 
 // inside the patch within guess_t_window patch sizes of the stage-1 t, and
 // otherwise the solve restarts from the stage-1 triangle (the reference's start).
 __global__ void __launch_bounds__(128) k_newton(DScene S, TraceArgs A, WaveArgs W, long long n_req) {
+    if (W.count_dev) n_req = *W.count_dev;
+    if (blockIdx.x * static_cast<long long>(blockDim.x) >= n_req) return;   // graph launch: spare blocks
     const long long j = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
     long long iters = 0, iters32 = 0, used = 0, fallback = 0;
     if (j < n_req) {
         const NewtonRequest q = W.req[j];
+        if (W.next_req) W.next_req[j] = q;
         const V3 o = load3(W.o + 3LL * q.ray);
         const V3 d = load3(W.d + 3LL * q.ray);
         const int pidx = S.obj_sub[q.obj];
@@ -1080,11 +1086,14 @@ __global__ void __launch_bounds__(128) k_newton(DScene S, TraceArgs A, WaveArgs 
 // k_newton with 8 lanes per request (patches of at most 8 nodes per axis):
 // the same starts, fallbacks and results, bit for bit.
 __global__ void __launch_bounds__(128) k_newton_grp(DScene S, TraceArgs A, WaveArgs W, long long n_req) {
+    if (W.count_dev) n_req = *W.count_dev;
+    if (blockIdx.x * static_cast<long long>(blockDim.x) / kGroup >= n_req) return;   // graph launch: spare blocks
     const Grp G = make_grp();
     const long long j = (blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x) / kGroup;
     long long iters = 0, iters32 = 0, used = 0, fallback = 0;
     if (j < n_req) {   // uniform over the group
         const NewtonRequest q = W.req[j];
+        if (W.next_req && G.g == 0) W.next_req[j] = q;
         const V3 o = load3(W.o + 3LL * q.ray);
         const V3 d = load3(W.d + 3LL * q.ray);
         const int pidx = S.obj_sub[q.obj];
@@ -1139,6 +1148,10 @@ __global__ void __launch_bounds__(128) k_newton_grp(DScene S, TraceArgs A, WaveA
 // current bounce's query restarts from the root, so the result is the same.
 __global__ void __launch_bounds__(128) k_resume(DScene S, TraceArgs A, WaveArgs W, const NewtonRequest* reqs,
                                                 const int* rays, long long n) {
+    if (W.count_dev) {
+        n = *W.count_dev;
+        if (blockIdx.x * static_cast<long long>(blockDim.x) >= n) return;   // graph launch: spare blocks
+    }
     const long long slot = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
     Counters ctr;
     RayTally tally;
@@ -1246,6 +1259,7 @@ __global__ void __launch_bounds__(128, MINB) k_resume_warp(DScene S, TraceArgs A
     for (int k = threadIdx.x; k < 6 * S.smem_nodes; k += blockDim.x) sbox[k] = S.node_box[k];
     for (int k = threadIdx.x; k < 4 * S.smem_nodes; k += blockDim.x) slink[k] = S.node_link[k];
     __syncthreads();
+    if (W.count_dev) n = *W.count_dev;
     const int lane = threadIdx.x & 31;
     const long long warp = (blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x) >> 5;
     const long long n_warps = (static_cast<long long>(gridDim.x) * blockDim.x) >> 5;
@@ -1480,6 +1494,40 @@ cudaError_t launch_advance(const DScene& S, const TraceArgs& A, const WaveArgs& 
         case 6: return launch_advance_shape<384, 1>(S, A, W, sm_count, 3400, stream);
         default: return launch_advance_shape<128, 3>(S, A, W, sm_count, 1536, stream);
     }
+}
+
+// Round control of the graph-launched trace, after each k_advance: the same
+// decision the host-driven loop takes from the round's counters.  No requests,
+// or a watchdog stop: the rounds end.  At most wave_tail requests: the rounds
+// end and the tail kernel finishes those rays.  Otherwise the requests go to
+// Newton and become the next round's runnable set; the loop repeats unless
+// this was round max_rounds (flagged for the host as an error).  Every
+// repetition raises counters[kWcRounds], so the loop ends after at most
+// max_rounds rounds whatever the counts.
+__global__ void k_wave_decide(unsigned int* c, long long wave_tail, long long max_rounds,
+                              cudaGraphConditionalHandle loop) {
+    if (threadIdx.x != 0) return;
+    const long long n_req = c[0];
+    unsigned int next = 0, tail = 0, go = 0;
+    if (c[3] == 0u && n_req > 0) {
+        if (n_req <= wave_tail) tail = static_cast<unsigned int>(n_req);
+        else next = static_cast<unsigned int>(n_req);
+    }
+    if (next) {
+        const unsigned int r = c[kWcRounds] + 1u;
+        c[kWcRounds] = r;
+        if (static_cast<long long>(r) >= max_rounds) c[kWcBound] = 1u;
+        else go = 1u;
+    }
+    c[kWcNext] = next;
+    c[kWcTail] = tail;
+    cudaGraphSetConditional(loop, go);
+}
+
+cudaError_t launch_wave_decide(unsigned int* counters, long long wave_tail, long long max_rounds,
+                               cudaGraphConditionalHandle loop, cudaStream_t stream) {
+    k_wave_decide<<<1, 32, 0, stream>>>(counters, wave_tail, max_rounds, loop);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_newton(const DScene& S, const TraceArgs& A, const WaveArgs& W, long long n_req, cudaStream_t stream) {

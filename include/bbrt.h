@@ -372,9 +372,11 @@ BBRT_API int  bbrt_mlp_infer_check(const float* params, int n_patches, const flo
  *
  * Traces the ray batch of each scene (device arrays, as with BBRT_DEVICE_PTRS;
  * scenes distinct) with all scenes in flight together: each scene's trace
- * runs on its own stream and the wavefront rounds of all scenes interleave,
- * with one host wait per round for the whole batch, so small scenes run
- * alongside large ones instead of one after the other.  Each scene's results
+ * runs on its own stream, as one graph launch per scene (graph_rounds, the
+ * default: no host wait until the end of the batch) or with the host-driven
+ * rounds of all scenes interleaved (one host wait per round for the whole
+ * batch), so small scenes run alongside large ones instead of one after the
+ * other.  Each scene's results
  * are those of bbrt_trace on it alone.  stats (optional) sums the counters of
  * all scenes; batch_ms (optional) is the device time from the batch's first
  * launch to its last. */
@@ -387,8 +389,8 @@ BBRT_API int bbrt_trace_batch(const bbrt_scene_t* scenes, int n_scenes, const do
  * The schedule changes only the order and grouping of work, never a result
  * (every schedule gives the same bits; GPU-tested).  A scene starts with the
  * library defaults (environment overrides BBRT_ADV_SHAPE, BBRT_WARP_S1,
- * BBRT_ORDER_RAYS, BBRT_WARP_TAIL, BBRT_WAVE_TAIL, BBRT_WAVE_MIN are read
- * once per process). */
+ * BBRT_ORDER_RAYS, BBRT_WARP_TAIL, BBRT_WAVE_TAIL, BBRT_WAVE_MIN, BBRT_GRAPH
+ * are read once per process). */
 typedef struct bbrt_tuning {
     int advance_shape;        /* k_advance launch shape, threads x blocks per SM: 0 = 128x3, 1 = 256x2,
                                  2 = 128x4, 3 = 512x1 (default), 4 = 768x1, 5 = 1024x1, 6 = 384x1 */
@@ -397,13 +399,16 @@ typedef struct bbrt_tuning {
     int warp_tail;            /* 1 (default): the tail one warp per ray, else one thread per ray */
     long long wave_tail;      /* rays still waiting when the tail takes over (16384) */
     long long wave_min_rays;  /* smaller batches run the fused per-thread kernel (8192) */
+    int graph_rounds;         /* 1 (default): the whole wavefront trace is one CUDA graph launch whose
+                                 round loop is a device-side conditional node (no host wait per round;
+                                 one graph per argument set, kept for reuse); 0: rounds driven by the host */
 } bbrt_tuning;
 
 BBRT_API int bbrt_scene_get_tuning(bbrt_scene_t scene, bbrt_tuning* out);
 BBRT_API int bbrt_scene_set_tuning(bbrt_scene_t scene, const bbrt_tuning* tuning);
 /* Times candidate schedules on the given rays (host arrays; the scene's
  * current precision and guess modes), by coordinate descent over the launch
- * shape, then the tail size, `trials` timed traces each after one untimed
+ * shape, then the tail size, then graph-launched vs host-driven rounds, `trials` timed traces each after one untimed
  * one; keeps the fastest in the scene and returns it with its mean device
  * time per trace. */
 BBRT_API int bbrt_scene_autotune(bbrt_scene_t scene, const double* origins, const double* dirs, long long n,
