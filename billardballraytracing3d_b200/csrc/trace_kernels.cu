@@ -1216,7 +1216,12 @@ __device__ QHit warp_bvh_query(const DScene& S, const V3& o, const V3& d, int cu
                         double u0, v0;
                         key_to_uv(S, s1.key, u0, v0);
                         long long it = 0;
-                        r = newton_exact(S, pidx, o, d, u0, v0, s1.t, h, it);
+                        // One ray per warp: the solve is latency-bound, so
+                        // when every patch axis has at most 8 nodes each
+                        // 8-lane group evaluates it with one node row per lane
+                        // (the same result bit for bit; all four groups agree).
+                        if (S.max_nodes <= kGroup) r = grp_newton_exact(S, pidx, o, d, u0, v0, s1.t, h, it, make_grp());
+                        else r = newton_exact(S, pidx, o, d, u0, v0, s1.t, h, it);
                         if (lane == 0) ctr.newton_iters += it;
                     }
                 } else {
