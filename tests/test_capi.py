@@ -34,7 +34,9 @@ def test_library_exports_every_declared_symbol(built):
 def test_struct_layouts_match_header(built):
     structs = {"bbrt_config": C.Config, "bbrt_patch_desc": C.PatchDesc, "bbrt_object_desc": C.ObjectDesc,
                "bbrt_patch_file": C.PatchFile, "bbrt_scene_info": C.SceneInfo, "bbrt_object_info": C.ObjectInfo,
-               "bbrt_hit": C.Hit, "bbrt_trace_out": C.TraceOut, "bbrt_trace_stats": C.TraceStats}
+               "bbrt_hit": C.Hit, "bbrt_trace_out": C.TraceOut, "bbrt_trace_stats": C.TraceStats,
+               "bbrt_tuning": C.Tuning, "bbrt_guess_train_config": C.GuessTrainConfig,
+               "bbrt_guess_train_report": C.GuessTrainReport}
     src = '#include <stdio.h>\n#include "bbrt.h"\nint main(void){\n'
     for name in structs:
         src += f'printf("{name} %zu\\n", sizeof({name}));\n'
@@ -176,8 +178,10 @@ def test_bounce_map_rays_equal_oracle(built):
 def test_scene_tuning_roundtrip_and_validation(built):
     sc = api.Scene(scenes.scene_two_spheres(), config=C.default_config(coarse_grid_n=9))
     t = sc.tuning()
-    assert t["advance_shape"] == 3 and t["warp_stage1"] == 1 and t["wave_tail"] == 16384
-    t2 = sc.tuning(advance_shape=6, wave_tail=8192)
-    assert t2["advance_shape"] == 6 and t2["wave_tail"] == 8192 and sc.tuning() == t2
+    assert t["advance_shape"] == 3 and t["warp_stage1"] == 1 and t["wave_tail"] == 16384 and t["graph_rounds"] == 1
+    t2 = sc.tuning(advance_shape=6, wave_tail=8192, graph_rounds=0)
+    assert t2["advance_shape"] == 6 and t2["wave_tail"] == 8192 and t2["graph_rounds"] == 0 and sc.tuning() == t2
     with pytest.raises(RuntimeError, match="advance_shape"):
         sc.tuning(advance_shape=9)
+    with pytest.raises(RuntimeError, match="graph_rounds"):
+        sc.tuning(graph_rounds=2)
