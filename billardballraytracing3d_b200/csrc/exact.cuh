@@ -266,8 +266,23 @@ __device__ __forceinline__ bool newton_fp32(const DScene& S, int pidx, const V3&
             float rs[9];
             for (int f = 0; f < 9; ++f) rs[f] = 0.0f;
             const float* row = Fd + static_cast<long long>(i) * J * 12;
-            for (int j = 0; j < J; ++j)
-                for (int f = 0; f < 9; ++f) rs[f] = fmaf(bv[j], row[j * 12 + f], rs[f]);
+            for (int j = 0; j < J; ++j) {
+                // a node's 12 floats start on a 16-byte boundary (checked at
+                // upload): fields 0-7 as two 16-byte loads, field 8 alone
+                const float4 fa = *reinterpret_cast<const float4*>(row + j * 12);
+                const float4 fb = *reinterpret_cast<const float4*>(row + j * 12 + 4);
+                const float f8 = row[j * 12 + 8];
+                const float b = bv[j];
+                rs[0] = fmaf(b, fa.x, rs[0]);
+                rs[1] = fmaf(b, fa.y, rs[1]);
+                rs[2] = fmaf(b, fa.z, rs[2]);
+                rs[3] = fmaf(b, fa.w, rs[3]);
+                rs[4] = fmaf(b, fb.x, rs[4]);
+                rs[5] = fmaf(b, fb.y, rs[5]);
+                rs[6] = fmaf(b, fb.z, rs[6]);
+                rs[7] = fmaf(b, fb.w, rs[7]);
+                rs[8] = fmaf(b, f8, rs[8]);
+            }
             for (int f = 0; f < 9; ++f) e[f] = fmaf(li, rs[f], e[f]);
         }
         const float Fx = e[0] - fmaf(tf, dx, ox), Fy = e[1] - fmaf(tf, dy, oy), Fz = e[2] - fmaf(tf, dz, oz);
