@@ -312,11 +312,11 @@ int ensure_uploaded(bbrt_scene* s) {
         const std::vector<float> f32(H.p_fields.begin(), H.p_fields.end());
         if ((rc = s->upload(n32, D.p_nodes32))) return rc;
         if ((rc = s->upload(f32, D.p_fields32))) return rc;
-        // the FP32 Newton phase reads a node's fields with 16-byte loads:
-        // every node starts at a multiple of kFields floats from an aligned base
+        // both Newton phases read a node's fields with 16-byte loads: every
+        // node starts at a multiple of kFields values from an aligned base
         static_assert(bbrt::kFields % 4 == 0, "FP32 node records must be whole 16-byte units");
-        if (reinterpret_cast<uintptr_t>(D.p_fields32) % 16 != 0)
-            return fail(BBRT_ERR_CUDA, "bbrt_scene_upload: FP32 field array not 16-byte aligned");
+        if (reinterpret_cast<uintptr_t>(D.p_fields32) % 16 != 0 || reinterpret_cast<uintptr_t>(D.p_fields) % 16 != 0)
+            return fail(BBRT_ERR_CUDA, "bbrt_scene_upload: field arrays not 16-byte aligned");
         const std::vector<double> fr = patch_frames(H);
         if ((rc = s->upload(fr, s->guess.frame))) return rc;
     }

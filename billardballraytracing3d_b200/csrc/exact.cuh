@@ -157,6 +157,42 @@ __device__ __forceinline__ void eval_fields(const double* __restrict__ F, int I,
     }
 }
 
+// eval_fields<9> from field 0, each node's fields 0-7 read as four 16-byte
+// loads and field 8 alone (a node's 12 doubles start on a 16-byte boundary,
+// checked at upload); the same values in the same order.
+__device__ __forceinline__ void eval_fields9(const double* __restrict__ F, int I, int J, const double* bu,
+                                             const double* bv, double* out) {
+#pragma unroll
+    for (int f = 0; f < 9; ++f) out[f] = 0.0;
+    for (int i = 0; i < I; ++i) {
+        const double li = bu[i];
+        if (li == 0.0) continue;
+        double rs[9];
+#pragma unroll
+        for (int f = 0; f < 9; ++f) rs[f] = 0.0;
+        const double* row = F + static_cast<long long>(i) * J * 12;
+        for (int j = 0; j < J; ++j) {
+            const double lj = bv[j];
+            const double2 f01 = *reinterpret_cast<const double2*>(row + j * 12);
+            const double2 f23 = *reinterpret_cast<const double2*>(row + j * 12 + 2);
+            const double2 f45 = *reinterpret_cast<const double2*>(row + j * 12 + 4);
+            const double2 f67 = *reinterpret_cast<const double2*>(row + j * 12 + 6);
+            const double f8 = row[j * 12 + 8];
+            rs[0] += lj * f01.x;
+            rs[1] += lj * f01.y;
+            rs[2] += lj * f23.x;
+            rs[3] += lj * f23.y;
+            rs[4] += lj * f45.x;
+            rs[5] += lj * f45.y;
+            rs[6] += lj * f67.x;
+            rs[7] += lj * f67.y;
+            rs[8] += lj * f8;
+        }
+#pragma unroll
+        for (int f = 0; f < 9; ++f) out[f] += li * rs[f];
+    }
+}
+
 // Per-ray outcome of one object intersect: hit, miss, or a Newton failure.
 struct QHit {
     double t;
@@ -184,7 +220,7 @@ __device__ __forceinline__ int newton_exact(const DScene& S, int pidx, const V3 
         basis_1d(un, uw, I, u, bu);
         basis_1d(vn, vw, J, v, bv);
         double e[9];
-        eval_fields<9>(F, I, J, bu, bv, 0, e);
+        eval_fields9(F, I, J, bu, bv, e);
         const V3 R = v3(o.x + t * d.x, o.y + t * d.y, o.z + t * d.z);
         const double Fx = e[0] - R.x, Fy = e[1] - R.y, Fz = e[2] - R.z;
         const double a11 = e[3], a12 = e[6], a13 = -d.x;
