@@ -338,6 +338,12 @@ int ensure_uploaded(bbrt_scene* s) {
         D.cull_radius = s->cull.radius;
         for (int a = 0; a < 3; ++a) D.cull_center[a] = s->cull.center[a];
     }
+    // the kernels read node boxes, cell data and cull boxes with 8- and
+    // 16-byte loads; every record starts at a whole multiple of 8 or 16 bytes
+    // from its array's start, so the starts must be 16-byte aligned
+    for (const void* p : std::initializer_list<const void*>{ D.node_box, D.c_cell, D.c_cell_box, D.c_block_box })
+        if (reinterpret_cast<uintptr_t>(p) % 16 != 0)
+            return fail(BBRT_ERR_CUDA, "bbrt_scene_upload: scene array not 16-byte aligned");
     BBRT_CUDA(s->stats.ensure(sizeof(long long) * bbrt::ST_COUNT));
     BBRT_CUDA(s->work.ensure(sizeof(unsigned long long)));
     s->uploaded = true;

@@ -99,13 +99,20 @@ __device__ __forceinline__ bool mt_full(const V3& o, const V3& d, const V3& v0, 
 }
 
 // Slab test of BVH.hpp:14-37 (tmin_out is never used by the caller there).
+// Node boxes are 6 doubles on a 48-byte stride from a 16-byte aligned array
+// (global memory checked at upload, shared copies declared aligned): read as
+// three 16-byte loads.
 __device__ __forceinline__ bool ray_box_exact(const V3& o, const double inv[3], const double* box, double best_t) {
     double tmin = -CUDART_INF, tmax = CUDART_INF;
     const double oo[3] = { o.x, o.y, o.z };
+    const double2 b01 = *reinterpret_cast<const double2*>(box);
+    const double2 b23 = *reinterpret_cast<const double2*>(box + 2);
+    const double2 b45 = *reinterpret_cast<const double2*>(box + 4);
+    const double bx[6] = { b01.x, b01.y, b23.x, b23.y, b45.x, b45.y };
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        double t1 = (box[a] - oo[a]) * inv[a];
-        double t2 = (box[3 + a] - oo[a]) * inv[a];
+        double t1 = (bx[a] - oo[a]) * inv[a];
+        double t2 = (bx[3 + a] - oo[a]) * inv[a];
         if (inv[a] < 0.0) { const double s = t1; t1 = t2; t2 = s; }
         tmin = smax(tmin, t1);
         tmax = smin(tmax, t2);

@@ -64,8 +64,26 @@ __device__ __forceinline__ void grp_eval(const double* __restrict__ F, int I, in
     for (int j = 0; j < J; ++j) {
         const double lj = __shfl_sync(G.mask, bv, G.base + j);
         if (row) {
+            if constexpr (NF == 9 && FIRST == 0) {
+                // fields 0-7 as four 16-byte loads (a node's 12 doubles start
+                // on a 16-byte boundary, checked at upload), field 8 alone
+                const double2 f01 = *reinterpret_cast<const double2*>(rp + j * 12);
+                const double2 f23 = *reinterpret_cast<const double2*>(rp + j * 12 + 2);
+                const double2 f45 = *reinterpret_cast<const double2*>(rp + j * 12 + 4);
+                const double2 f67 = *reinterpret_cast<const double2*>(rp + j * 12 + 6);
+                rs[0] += lj * f01.x;
+                rs[1] += lj * f01.y;
+                rs[2] += lj * f23.x;
+                rs[3] += lj * f23.y;
+                rs[4] += lj * f45.x;
+                rs[5] += lj * f45.y;
+                rs[6] += lj * f67.x;
+                rs[7] += lj * f67.y;
+                rs[8] += lj * rp[j * 12 + 8];
+            } else {
 #pragma unroll
-            for (int f = 0; f < NF; ++f) rs[f] += lj * rp[j * 12 + f];
+                for (int f = 0; f < NF; ++f) rs[f] += lj * rp[j * 12 + f];
+            }
         }
     }
 #pragma unroll

@@ -65,12 +65,17 @@ __device__ __forceinline__ CullRay make_cull_ray(const DScene& S, const V3& o, c
 // FP32 slab test of the ray [0, inf) against a box inflated by c.delta.
 // Conservative: a triangle inside the box that the exact FP64 test accepts
 // always passes (the inflation bounds both roundings); only work is skipped.
+// Boxes are 6 floats on a 24-byte stride from a 16-byte aligned array
+// (checked at upload): read as three 8-byte loads.
 __device__ __forceinline__ bool cull_box(const float* __restrict__ b, const CullRay& c) {
-    float t1 = (b[0] - c.delta - c.ox) * c.ix, t2 = (b[3] + c.delta - c.ox) * c.ix;
+    const float2 b01 = *reinterpret_cast<const float2*>(b);
+    const float2 b23 = *reinterpret_cast<const float2*>(b + 2);
+    const float2 b45 = *reinterpret_cast<const float2*>(b + 4);
+    float t1 = (b01.x - c.delta - c.ox) * c.ix, t2 = (b23.y + c.delta - c.ox) * c.ix;
     float tmin = fmaxf(0.0f, fminf(t1, t2)), tmax = fmaxf(t1, t2);
-    t1 = (b[1] - c.delta - c.oy) * c.iy; t2 = (b[4] + c.delta - c.oy) * c.iy;
+    t1 = (b01.y - c.delta - c.oy) * c.iy; t2 = (b45.x + c.delta - c.oy) * c.iy;
     tmin = fmaxf(tmin, fminf(t1, t2)); tmax = fminf(tmax, fmaxf(t1, t2));
-    t1 = (b[2] - c.delta - c.oz) * c.iz; t2 = (b[5] + c.delta - c.oz) * c.iz;
+    t1 = (b23.x - c.delta - c.oz) * c.iz; t2 = (b45.y + c.delta - c.oz) * c.iz;
     tmin = fmaxf(tmin, fminf(t1, t2)); tmax = fminf(tmax, fmaxf(t1, t2));
     return tmin <= tmax;
 }
@@ -484,11 +489,14 @@ __device__ __forceinline__ void stage1_tri(const double* __restrict__ X, const d
     const int nc = n - 1;
     const double* r0 = X + static_cast<long long>(i * n + j) * 3;
     const double* r1 = r0 + 3 * n;
+    // cell normal and sagitta: 4 doubles on a 32-byte stride (16-byte loads)
     const double* c = CC + static_cast<long long>(i * nc + j) * 4;
-    const V3 cn = v3(c[0], c[1], c[2]);
+    const double2 c01 = *reinterpret_cast<const double2*>(c);
+    const double2 c23 = *reinterpret_cast<const double2*>(c + 2);
+    const V3 cn = v3(c01.x, c01.y, c23.x);
     const int k = step >> 1;
     const double sg = (k == 0) ? 0.0 : ((k == 1) ? 1.0 : -1.0);
-    const double dd = sg * c[3];
+    const double dd = sg * c23.y;
     const V3 p00 = load3(r0), p11 = load3(r1 + 3);
     const V3 pm = (step & 1) ? load3(r0 + 3) : load3(r1);   // p01 for the second triangle, p10 for the first
     const V3 q00 = v3(p00.x + cn.x * dd, p00.y + cn.y * dd, p00.z + cn.z * dd);
@@ -709,7 +717,7 @@ __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, Wav
     const int lane = threadIdx.x & 31;
     // The first S.smem_nodes BVH nodes (breadth-first order: the top levels)
     // are staged in shared memory for the whole launch.
-    extern __shared__ double smem_bvh[];
+    extern __shared__ __align__(16) double smem_bvh[];
     double* sbox = smem_bvh;
     int* slink = reinterpret_cast<int*>(smem_bvh + 6 * S.smem_nodes);
     for (int k = threadIdx.x; k < 6 * S.smem_nodes; k += blockDim.x) sbox[k] = S.node_box[k];
@@ -1258,7 +1266,7 @@ __device__ QHit warp_bvh_query(const DScene& S, const V3& o, const V3& d, int cu
 template <int MINB>
 __global__ void __launch_bounds__(128, MINB) k_resume_warp(DScene S, TraceArgs A, WaveArgs W,
                                                            const NewtonRequest* reqs, const int* rays, long long n) {
-    extern __shared__ double smem_tail[];
+    extern __shared__ __align__(16) double smem_tail[];
     double* sbox = smem_tail;
     int* slink = reinterpret_cast<int*>(smem_tail + 6 * S.smem_nodes);
     for (int k = threadIdx.x; k < 6 * S.smem_nodes; k += blockDim.x) sbox[k] = S.node_box[k];
