@@ -782,7 +782,7 @@ struct WaveRun {
             }));
             W.order = static_cast<const int*>(s->order.p);
         }
-        BBRT_CUDA(cudaMemsetAsync(W.counters, 0, 4 * sizeof(unsigned int), st));
+        BBRT_CUDA(cudaMemsetAsync(W.counters, 0, bbrt::kWaveCounters * sizeof(unsigned int), st));
         // every round finishes at least one query or one Newton solve of each runnable ray
         max_rounds = 4 + static_cast<long long>(A.max_bounces + 1) * (s->host.n_objects + 1);
         return launch_round();

@@ -161,13 +161,16 @@ struct WaveArgs {
 };
 
 // Round counters of the wavefront trace in device memory: [0..3] as
-// WaveArgs::counters; the rest are the round control of the graph-launched
-// trace, written by k_wave_decide after each k_advance.
+// WaveArgs::counters; [4..7] are the round control of the graph-launched
+// trace, written by k_wave_decide after each k_advance; [8..9] hand out the
+// tail kernels' rays.  All start at zero for each trace.
 constexpr int kWcNext = 4;     // requests solved this round, runnable next round (0: rounds end)
 constexpr int kWcTail = 5;     // requests left to the tail kernel (the last, small round)
 constexpr int kWcRounds = 6;   // rounds whose requests went to Newton
 constexpr int kWcBound = 7;    // the round bound was reached
-constexpr int kWaveCounters = 8;
+constexpr int kWcTailNext = 8; // next slot of the tail kernel (rays handed out one at a time)
+constexpr int kWcOvfNext = 9;  // next slot of the overflow tail
+constexpr int kWaveCounters = 10;
 
 constexpr int kQsInt = 6;
 constexpr int kSaveStack = 24;

@@ -1278,7 +1278,17 @@ __global__ void __launch_bounds__(128, MINB) k_resume_warp(DScene S, TraceArgs A
     const long long n_warps = (static_cast<long long>(gridDim.x) * blockDim.x) >> 5;
     Counters ctr;
     RayTally tally;
-    for (long long slot = warp; slot < n; slot += n_warps) {
+    // The tail's time is that of its slowest warp: rays are handed out one
+    // at a time from a counter, so a warp that drew a long chain takes no
+    // further rays while others do (a fixed stride when no counter is given).
+    unsigned int* next = W.counters ? W.counters + (reqs ? kWcTailNext : kWcOvfNext) : nullptr;
+    auto take = [&](long long fixed) -> long long {
+        if (!next) return fixed;
+        unsigned int v = 0;
+        if (lane == 0) v = atomicAdd(next, 1u);
+        return static_cast<long long>(__shfl_sync(0xffffffffu, v, 0));
+    };
+    for (long long slot = take(warp); slot < n; slot = take(slot + n_warps)) {
         const long long i = reqs ? reqs[slot].ray : rays[slot];
         int nres;
         RayCtx r = load_ray(W, i, nres);
