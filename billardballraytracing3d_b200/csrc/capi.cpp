@@ -2014,7 +2014,7 @@ BBRT_API int bbrt_scene_autotune(bbrt_scene_t s, const double* origins, const do
         rc = time_one(c, ms);
         if (!rc && ms < cur_ms) { cur = c; cur_ms = ms; }
     }
-    const long long tails[] = { 4096, 8192, 16384, 32768 };
+    const long long tails[] = { 4096, 8192, 16384, 32768, 65536 };
     for (long long tl : tails) {
         if (rc || tl == cur.wave_tail) continue;
         bbrt_tuning c = cur;
