@@ -46,6 +46,9 @@ cudaError_t launch_resume_warp(const DScene& S, const TraceArgs& A, const WaveAr
 cudaError_t launch_resume(const DScene& S, const TraceArgs& A, const WaveArgs& W, const NewtonRequest* reqs,
                           const int* rays, long long n, cudaStream_t stream);
 size_t ray_order_workspace_bytes(long long n);
+int request_sort_max_objects();
+cudaError_t sort_requests(const NewtonRequest* req, long long n, const unsigned* n_dev, int n_objects, void* ws,
+                          NewtonRequest* out, cudaStream_t stream);
 cudaError_t ray_order(const double* o, const double* d, long long n, const double center[3], double radius,
                       void* ws, int* order, cudaStream_t stream);
 cudaError_t launch_query(const DScene& S, const QueryArgs& Q, cudaStream_t stream);
@@ -460,6 +463,7 @@ struct Tuning {
     int tail_shape = 0;               // k_resume_warp launch shape (see launch_resume_warp)
     int group_newton = 0;             // k_newton by 8-lane groups (exact, measured slower: off)
     int graph_rounds = 1;             // the rounds as one CUDA graph with a device-side loop
+    int sort_requests = 1;            // group each round's Newton requests by patch before solving them
 };
 
 // Launch-shape knobs; defaults tuned on B200, overridable for experiments by
@@ -479,6 +483,7 @@ const Tuning& tuning() {
         if (const char* e = std::getenv("BBRT_TAIL_SHAPE")) v.tail_shape = std::atoi(e);
         if (const char* e = std::getenv("BBRT_GROUP_NEWTON")) v.group_newton = std::atoi(e);
         if (const char* e = std::getenv("BBRT_GRAPH")) v.graph_rounds = std::atoi(e);
+        if (const char* e = std::getenv("BBRT_SORT_REQ")) v.sort_requests = std::atoi(e);
         return v;
     }();
     return t;
@@ -523,6 +528,12 @@ cudaError_t run_tail(bbrt_scene* s, const bbrt::TraceArgs& A, const bbrt::WaveAr
     if (scene_tuning(s).warp_tail)
         return bbrt::launch_resume_warp(s->dev, A, W, reqs, rays, n, s->sm_count, tuning().tail_shape, st);
     return bbrt::launch_resume(s->dev, A, W, reqs, rays, n, st);
+}
+
+// Whether a round's Newton requests are grouped by patch before solving (one
+// counting-sort bucket per object); the sort uses the ray-order workspace.
+bool sort_round_requests(const bbrt_scene* s) {
+    return tuning().sort_requests && s->host.n_objects >= 1 && s->host.n_objects <= bbrt::request_sort_max_objects();
 }
 
 // ---- the wavefront trace as one CUDA graph ------------------------------------
@@ -591,8 +602,11 @@ int build_wave_graph(bbrt_scene* s, const bbrt::TraceArgs& A, const bbrt_tuning&
     Wr.runnable = req_b;                   // later rounds: last round's requests
     Wr.req = req_a;
     Wr.count_dev = c + bbrt::kWcNext;
-    Wn.req = req_a;
-    Wn.next_req = req_b;
+    // Newton solves req_b: the requests grouped by patch (sorted from req_a),
+    // or copied there by k_newton itself as it solves them in place
+    const bool sort = sort_round_requests(s);
+    Wn.req = sort ? req_b : req_a;
+    Wn.next_req = sort ? nullptr : req_b;
     Wn.count_dev = c + bbrt::kWcNext;
     double* gout = static_cast<double*>(s->guess.out.p);
     if (learned) {
@@ -607,8 +621,10 @@ int build_wave_graph(bbrt_scene* s, const bbrt::TraceArgs& A, const bbrt_tuning&
     auto round = [&](cudaStream_t q, const bbrt::WaveArgs& Wa, cudaGraphConditionalHandle loop) -> cudaError_t {
         cudaError_t e = bbrt::launch_advance(s->dev, A, Wa, s->sm_count, T.advance_shape, q);
         if (e == cudaSuccess) e = bbrt::launch_wave_decide(c, T.wave_tail, max_rounds, loop, q);
+        if (e == cudaSuccess && sort)
+            e = bbrt::sort_requests(req_a, n, c + bbrt::kWcNext, s->host.n_objects, s->order_ws.p, req_b, q);
         if (e == cudaSuccess && learned)
-            e = bbrt::mlp_infer_requests(req_a, n, W.o, W.d, s->dev.obj_sub, s->guess.frame, net, gout, q,
+            e = bbrt::mlp_infer_requests(Wn.req, n, W.o, W.d, s->dev.obj_sub, s->guess.frame, net, gout, q,
                                          c + bbrt::kWcNext);
         if (e == cudaSuccess) e = bbrt::launch_newton(s->dev, A, Wn, n, q);
         return e;
@@ -667,7 +683,8 @@ int build_wave_graph(bbrt_scene* s, const bbrt::TraceArgs& A, const bbrt_tuning&
     }
     out.graph = g;
     out.exec = x;
-    const long long per_round = 3 + (learned ? 1 : 0);   // advance, decide, [infer], Newton
+    // advance, decide, [4 sort kernels], [infer], Newton
+    const long long per_round = 3 + (learned ? 1 : 0) + (sort ? 4 : 0);
     out.launches_round = per_round;
     out.launches_fixed = (T.order_rays ? 4 : 0) + per_round + 2;
     return BBRT_OK;
@@ -682,6 +699,7 @@ int launch_wave_graph(bbrt_scene* s, const bbrt::TraceArgs& A, const bbrt_tuning
         BBRT_CUDA(s->order_ws.ensure(bbrt::ray_order_workspace_bytes(n)));
         BBRT_CUDA(s->order.ensure(sizeof(int) * static_cast<size_t>(n)));
     }
+    if (sort_round_requests(s)) BBRT_CUDA(s->order_ws.ensure(bbrt::ray_order_workspace_bytes(n)));
     if (learned) BBRT_CUDA(s->guess.out.ensure(sizeof(double) * 4 * static_cast<size_t>(n)));
     const long long max_rounds = 4 + static_cast<long long>(A.max_bounces + 1) * (s->host.n_objects + 1);
     GraphKey k;
@@ -704,7 +722,8 @@ int launch_wave_graph(bbrt_scene* s, const bbrt::TraceArgs& A, const bbrt_tuning
                          static_cast<long long>(T.advance_shape), static_cast<long long>(T.warp_stage1),
                          static_cast<long long>(T.order_rays), static_cast<long long>(T.warp_tail), T.wave_tail,
                          static_cast<long long>(tuning().resume_queries), static_cast<long long>(tuning().group_newton),
-                         static_cast<long long>(tuning().tail_shape), max_rounds })
+                         static_cast<long long>(tuning().tail_shape), max_rounds,
+                         static_cast<long long>(sort_round_requests(s)) })
         k.put(x);
     k.put(s->guess.min_logit);
     k.put(s->guess.t_window);
@@ -765,6 +784,7 @@ struct WaveRun {
             return launch_wave_graph(s, A, T, st, graph);
         }
         bbrt::wave_layout(s->wave.p, n, W, req_a, req_b);
+        if (sort_round_requests(s)) BBRT_CUDA(s->order_ws.ensure(bbrt::ray_order_workspace_bytes(n)));
         W.counters = static_cast<unsigned int*>(s->wave_ctr.p);
         W.warp_stage1 = T.warp_stage1;
         W.resume_queries = tuning().resume_queries;
@@ -821,6 +841,15 @@ struct WaveRun {
             return BBRT_OK;
         }
         if (log_rounds) BBRT_CUDA(cudaEventRecord(s->ev[2], st));
+        if (sort_round_requests(s)) {
+            // group the requests by patch into the other list, which Newton
+            // solves and the next round runs; the next requests go to this one
+            bbrt::NewtonRequest* grouped = (W.req == req_a) ? req_b : req_a;
+            BBRT_CUDA(timed(s, K_ORDER, st, [&] {
+                return bbrt::sort_requests(W.req, n_req, nullptr, s->host.n_objects, s->order_ws.p, grouped, st);
+            }));
+            W.req = grouped;
+        }
         W.guess = nullptr;
         if (s->host.cfg.guess == BBRT_GUESS_LEARNED && s->guess.trained) {
             BBRT_CUDA(s->guess.out.ensure(sizeof(double) * 4 * static_cast<size_t>(n_req)));

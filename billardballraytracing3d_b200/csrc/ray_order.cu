@@ -9,6 +9,8 @@
 // ray's result is written to its own index.
 #include <cuda_runtime.h>
 
+#include "dscene.h"
+
 namespace bbrt {
 
 constexpr int kOrderBits = 18;
@@ -132,6 +134,53 @@ cudaError_t ray_order(const double* o, const double* d, long long n, const doubl
     k_order_scan_local<<<kScanBlocks, kScanBlock, 0, stream>>>(hist, block_sums);
     k_order_scan_add<<<kScanBlocks, kScanBlock, 0, stream>>>(hist, block_sums);
     k_order_scatter<<<blocks, 256, 0, stream>>>(keys, n, hist, order);
+    return cudaGetLastError();
+}
+
+// ---- a round's Newton requests grouped by patch object ----------------------
+//
+// The same counting sort over the object index: the requests of one patch end
+// up next to each other, so the lanes of a Newton warp share their patch's
+// node-field loads.  Each request is solved on its own and written to its
+// own (ray, entry), so only the order of the work changes.  With n_dev (a
+// graph launch) the count is read on the device and n only sizes the grid.
+
+__global__ void k_req_hist(const NewtonRequest* __restrict__ req, long long n, const unsigned* n_dev,
+                           unsigned* __restrict__ hist) {
+    if (n_dev) n = *n_dev;
+    const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (i >= n) return;
+    atomicAdd(hist + req[i].obj, 1u);
+}
+
+__global__ void k_req_scatter(const NewtonRequest* __restrict__ req, long long n, const unsigned* n_dev,
+                              unsigned* __restrict__ cursor, NewtonRequest* __restrict__ out) {
+    if (n_dev) n = *n_dev;
+    const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (i >= n) return;
+    const NewtonRequest q = req[i];
+    out[atomicAdd(cursor + q.obj, 1u)] = q;
+}
+
+// Largest object count the request sort handles (one bucket per object).
+int request_sort_max_objects() { return kOrderBuckets; }
+
+// out[0, count) = req[0, count) grouped by object; `ws` holds
+// ray_order_workspace_bytes(any n); n_objects <= request_sort_max_objects().
+cudaError_t sort_requests(const NewtonRequest* req, long long n, const unsigned* n_dev, int n_objects, void* ws,
+                          NewtonRequest* out, cudaStream_t stream) {
+    if (n <= 0) return cudaSuccess;
+    if (n_objects < 1 || n_objects > kOrderBuckets) return cudaErrorInvalidValue;
+    unsigned* hist = static_cast<unsigned*>(ws);
+    unsigned* block_sums = hist + kOrderBuckets;
+    const int scan_blocks = (n_objects + kScanBlock - 1) / kScanBlock;
+    cudaError_t e = cudaMemsetAsync(hist, 0, sizeof(unsigned) * kScanBlock * scan_blocks, stream);
+    if (e != cudaSuccess) return e;
+    const unsigned blocks = static_cast<unsigned>((n + 255) / 256);
+    k_req_hist<<<blocks, 256, 0, stream>>>(req, n, n_dev, hist);
+    k_order_scan_local<<<scan_blocks, kScanBlock, 0, stream>>>(hist, block_sums);
+    k_order_scan_add<<<scan_blocks, kScanBlock, 0, stream>>>(hist, block_sums);
+    k_req_scatter<<<blocks, 256, 0, stream>>>(req, n, n_dev, hist, out);
     return cudaGetLastError();
 }
 

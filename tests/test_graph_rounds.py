@@ -3,6 +3,8 @@ default) against the host-driven rounds (graph_rounds = 0): the same results
 bit for bit and the same counters, in every arithmetic mode, with the round
 loop taken many times, never, and with rays that overflow the resolved list.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -46,8 +48,9 @@ def test_graph_rounds_equal_host_rounds_every_mode(built):
         _assert_same(h, g)
         assert g["stats"]["rounds"] >= 2
         # the graph's launches: ordering, then per round advance / decide /
-        # [inference] / Newton, then the two tail kernels
-        per_round = 4 if guess == C.GUESS_LEARNED else 3
+        # [four request-grouping kernels] / [inference] / Newton, then the two
+        # tail kernels
+        per_round = (4 if guess == C.GUESS_LEARNED else 3) + (4 if os.environ.get("BBRT_SORT_REQ", "1") != "0" else 0)
         assert g["stats"]["launches"] == 4 + per_round * g["stats"]["rounds"] + 2
         if guess == C.GUESS_LEARNED:
             assert g["stats"]["guess_used"] > 0
