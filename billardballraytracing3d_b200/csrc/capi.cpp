@@ -47,8 +47,8 @@ cudaError_t launch_resume(const DScene& S, const TraceArgs& A, const WaveArgs& W
                           const int* rays, long long n, cudaStream_t stream);
 size_t ray_order_workspace_bytes(long long n);
 int request_sort_max_objects();
-cudaError_t sort_requests(const NewtonRequest* req, long long n, const unsigned* n_dev, int n_objects, void* ws,
-                          NewtonRequest* out, cudaStream_t stream);
+cudaError_t sort_requests(const NewtonRequest* req, long long n, const unsigned* n_dev, int n_objects, int side,
+                          int coarse_cells, void* ws, NewtonRequest* out, cudaStream_t stream);
 cudaError_t ray_order(const double* o, const double* d, long long n, const double center[3], double radius,
                       void* ws, int* order, cudaStream_t stream);
 cudaError_t launch_query(const DScene& S, const QueryArgs& Q, cudaStream_t stream);
@@ -464,6 +464,7 @@ struct Tuning {
     int group_newton = 0;             // k_newton by 8-lane groups (exact, measured slower: off)
     int graph_rounds = 1;             // the rounds as one CUDA graph with a device-side loop
     int sort_requests = 1;            // group each round's Newton requests by patch before solving them
+    int sort_side = 4;                // ... and within a patch by the side x side region of the stage-1 cell
 };
 
 // Launch-shape knobs; defaults tuned on B200, overridable for experiments by
@@ -484,6 +485,7 @@ const Tuning& tuning() {
         if (const char* e = std::getenv("BBRT_GROUP_NEWTON")) v.group_newton = std::atoi(e);
         if (const char* e = std::getenv("BBRT_GRAPH")) v.graph_rounds = std::atoi(e);
         if (const char* e = std::getenv("BBRT_SORT_REQ")) v.sort_requests = std::atoi(e);
+        if (const char* e = std::getenv("BBRT_SORT_SIDE")) v.sort_side = std::max(1, std::atoi(e));
         return v;
     }();
     return t;
@@ -622,7 +624,8 @@ int build_wave_graph(bbrt_scene* s, const bbrt::TraceArgs& A, const bbrt_tuning&
         cudaError_t e = bbrt::launch_advance(s->dev, A, Wa, s->sm_count, T.advance_shape, q);
         if (e == cudaSuccess) e = bbrt::launch_wave_decide(c, T.wave_tail, max_rounds, loop, q);
         if (e == cudaSuccess && sort)
-            e = bbrt::sort_requests(req_a, n, c + bbrt::kWcNext, s->host.n_objects, s->order_ws.p, req_b, q);
+            e = bbrt::sort_requests(req_a, n, c + bbrt::kWcNext, s->host.n_objects, tuning().sort_side,
+                                    s->dev.coarse_n - 1, s->order_ws.p, req_b, q);
         if (e == cudaSuccess && learned)
             e = bbrt::mlp_infer_requests(Wn.req, n, W.o, W.d, s->dev.obj_sub, s->guess.frame, net, gout, q,
                                          c + bbrt::kWcNext);
@@ -846,7 +849,8 @@ struct WaveRun {
             // solves and the next round runs; the next requests go to this one
             bbrt::NewtonRequest* grouped = (W.req == req_a) ? req_b : req_a;
             BBRT_CUDA(timed(s, K_ORDER, st, [&] {
-                return bbrt::sort_requests(W.req, n_req, nullptr, s->host.n_objects, s->order_ws.p, grouped, st);
+                return bbrt::sort_requests(W.req, n_req, nullptr, s->host.n_objects, tuning().sort_side,
+                                           s->dev.coarse_n - 1, s->order_ws.p, grouped, st);
             }));
             W.req = grouped;
         }

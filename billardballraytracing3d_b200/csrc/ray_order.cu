@@ -145,42 +145,54 @@ cudaError_t ray_order(const double* o, const double* d, long long n, const doubl
 // own (ray, entry), so only the order of the work changes.  With n_dev (a
 // graph launch) the count is read on the device and n only sizes the grid.
 
-__global__ void k_req_hist(const NewtonRequest* __restrict__ req, long long n, const unsigned* n_dev,
-                           unsigned* __restrict__ hist) {
+// Bucket of a request: its object, refined (side > 1) by the side x side
+// region of the patch that holds its stage-1 cell (key = cell * 6 + test).
+__device__ __forceinline__ unsigned req_bucket(const NewtonRequest& q, int side, int nc) {
+    if (side <= 1) return static_cast<unsigned>(q.obj);
+    const int cell = q.key / 6, ci = cell / nc, cj = cell - ci * nc;
+    return static_cast<unsigned>(q.obj) * side * side + (ci * side / nc) * side + (cj * side / nc);
+}
+
+__global__ void k_req_hist(const NewtonRequest* __restrict__ req, long long n, const unsigned* n_dev, int side,
+                           int nc, unsigned* __restrict__ hist) {
     if (n_dev) n = *n_dev;
     const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
     if (i >= n) return;
-    atomicAdd(hist + req[i].obj, 1u);
+    atomicAdd(hist + req_bucket(req[i], side, nc), 1u);
 }
 
-__global__ void k_req_scatter(const NewtonRequest* __restrict__ req, long long n, const unsigned* n_dev,
-                              unsigned* __restrict__ cursor, NewtonRequest* __restrict__ out) {
+__global__ void k_req_scatter(const NewtonRequest* __restrict__ req, long long n, const unsigned* n_dev, int side,
+                              int nc, unsigned* __restrict__ cursor, NewtonRequest* __restrict__ out) {
     if (n_dev) n = *n_dev;
     const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
     if (i >= n) return;
     const NewtonRequest q = req[i];
-    out[atomicAdd(cursor + q.obj, 1u)] = q;
+    out[atomicAdd(cursor + req_bucket(q, side, nc), 1u)] = q;
 }
 
 // Largest object count the request sort handles (one bucket per object).
 int request_sort_max_objects() { return kOrderBuckets; }
 
-// out[0, count) = req[0, count) grouped by object; `ws` holds
+// out[0, count) = req[0, count) grouped by object, and within an object by
+// the side x side region of its stage-1 cell (coarse_cells cells per patch
+// side; side 1 when the buckets would not fit); `ws` holds
 // ray_order_workspace_bytes(any n); n_objects <= request_sort_max_objects().
-cudaError_t sort_requests(const NewtonRequest* req, long long n, const unsigned* n_dev, int n_objects, void* ws,
-                          NewtonRequest* out, cudaStream_t stream) {
+cudaError_t sort_requests(const NewtonRequest* req, long long n, const unsigned* n_dev, int n_objects, int side,
+                          int coarse_cells, void* ws, NewtonRequest* out, cudaStream_t stream) {
     if (n <= 0) return cudaSuccess;
     if (n_objects < 1 || n_objects > kOrderBuckets) return cudaErrorInvalidValue;
+    if (side < 1 || coarse_cells < 1 || static_cast<long long>(n_objects) * side * side > kOrderBuckets) side = 1;
     unsigned* hist = static_cast<unsigned*>(ws);
     unsigned* block_sums = hist + kOrderBuckets;
-    const int scan_blocks = (n_objects + kScanBlock - 1) / kScanBlock;
+    const int buckets = n_objects * side * side;
+    const int scan_blocks = (buckets + kScanBlock - 1) / kScanBlock;
     cudaError_t e = cudaMemsetAsync(hist, 0, sizeof(unsigned) * kScanBlock * scan_blocks, stream);
     if (e != cudaSuccess) return e;
     const unsigned blocks = static_cast<unsigned>((n + 255) / 256);
-    k_req_hist<<<blocks, 256, 0, stream>>>(req, n, n_dev, hist);
+    k_req_hist<<<blocks, 256, 0, stream>>>(req, n, n_dev, side, coarse_cells, hist);
     k_order_scan_local<<<scan_blocks, kScanBlock, 0, stream>>>(hist, block_sums);
     k_order_scan_add<<<scan_blocks, kScanBlock, 0, stream>>>(hist, block_sums);
-    k_req_scatter<<<blocks, 256, 0, stream>>>(req, n, n_dev, hist, out);
+    k_req_scatter<<<blocks, 256, 0, stream>>>(req, n, n_dev, side, coarse_cells, hist, out);
     return cudaGetLastError();
 }
 
