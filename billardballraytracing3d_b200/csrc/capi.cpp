@@ -50,7 +50,7 @@ int request_sort_max_objects();
 cudaError_t sort_requests(const NewtonRequest* req, long long n, const unsigned* n_dev, int n_objects, int side,
                           int coarse_cells, void* ws, NewtonRequest* out, cudaStream_t stream);
 cudaError_t ray_order(const double* o, const double* d, long long n, const double center[3], double radius,
-                      void* ws, int* order, cudaStream_t stream);
+                      void* ws, int* order, cudaStream_t stream, bool entry);
 cudaError_t launch_query(const DScene& S, const QueryArgs& Q, cudaStream_t stream);
 cudaError_t launch_trace_noalloc(const DScene& S, TraceArgs A, bool count_hits, long long* hit_counts_out,
                                  long long* host_stats, cudaStream_t stream, int sm_count);
@@ -465,6 +465,7 @@ struct Tuning {
     int graph_rounds = 1;             // the rounds as one CUDA graph with a device-side loop
     int sort_requests = 1;            // group each round's Newton requests by patch before solving them
     int sort_side = 4;                // ... and within a patch by the side x side region of the stage-1 cell
+    int order_entry = 1;              // round-0 order keyed on the scene-sphere entry point (else the origin)
 };
 
 // Launch-shape knobs; defaults tuned on B200, overridable for experiments by
@@ -486,6 +487,7 @@ const Tuning& tuning() {
         if (const char* e = std::getenv("BBRT_GRAPH")) v.graph_rounds = std::atoi(e);
         if (const char* e = std::getenv("BBRT_SORT_REQ")) v.sort_requests = std::atoi(e);
         if (const char* e = std::getenv("BBRT_SORT_SIDE")) v.sort_side = std::max(1, std::atoi(e));
+        if (const char* e = std::getenv("BBRT_ORDER_ENTRY")) v.order_entry = std::atoi(e);
         return v;
     }();
     return t;
@@ -642,7 +644,7 @@ int build_wave_graph(bbrt_scene* s, const bbrt::TraceArgs& A, const bbrt_tuning&
     if (e == cudaSuccess && T.order_rays) {
         const double radius = s->cull.radius > 0.0 ? s->cull.radius : s->host.scene_diagonal;
         e = bbrt::ray_order(A.origins, A.dirs, n, s->cull.center, radius, s->order_ws.p,
-                            static_cast<int*>(s->order.p), cs);
+                            static_cast<int*>(s->order.p), cs, tuning().order_entry != 0);
     }
     if (e == cudaSuccess) e = cudaMemsetAsync(c, 0, bbrt::kWaveCounters * sizeof(unsigned int), cs);
     if (e == cudaSuccess) e = round(cs, W0, loop);
@@ -801,7 +803,7 @@ struct WaveRun {
             const double radius = s->cull.radius > 0.0 ? s->cull.radius : s->host.scene_diagonal;
             BBRT_CUDA(timed(s, K_ORDER, st, [&] {
                 return bbrt::ray_order(A.origins, A.dirs, n, s->cull.center, radius, s->order_ws.p,
-                                       static_cast<int*>(s->order.p), st);
+                                       static_cast<int*>(s->order.p), st, tuning().order_entry != 0);
             }));
             W.order = static_cast<const int*>(s->order.p);
         }

@@ -1,8 +1,9 @@
 // Coherent processing order for a batch of rays.
 //
 // Rays are bucketed by an 18-bit key — the octant of the direction (3 bits)
-// over a 15-bit Morton code of the origin quantised to 32 cells per axis
-// inside a cube of four scene radii — with a counting sort: histogram,
+// over a 15-bit Morton code, quantised to 32 cells per axis, of the point
+// where the ray enters the sphere around the scene (or of its origin) — with
+// a counting sort: histogram,
 // exclusive scan (two passes), scatter.  Warps then hold rays that start close together
 // and head the same way, so their BVH walks and stage-1 patch tests follow
 // the same paths.  Only the order in which rays are processed changes; every
@@ -38,13 +39,32 @@ __device__ __forceinline__ unsigned ray_key(const double* o, const double* d, co
     return (oct << 15) | morton;
 }
 
+// The point where a ray enters the sphere (c, r) around the scene — the origin
+// when it starts inside or misses — so that rays which meet the scene at the
+// same place in the same direction octant share a key.
+__device__ __forceinline__ void entry_point(const double* o, const double* d, const double c[3], double r,
+                                            double* p) {
+    const double ox = o[0] - c[0], oy = o[1] - c[1], oz = o[2] - c[2];
+    const double dd = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+    const double b = ox * d[0] + oy * d[1] + oz * d[2];
+    const double cc = ox * ox + oy * oy + oz * oz - r * r;
+    const double disc = b * b - dd * cc;
+    double t = 0.0;
+    if (cc > 0.0 && dd > 0.0 && disc > 0.0) t = (-b - sqrt(disc)) / dd;
+    if (!(t > 0.0)) t = 0.0;
+    for (int a = 0; a < 3; ++a) p[a] = o[a] + t * d[a];
+}
+
 __global__ void k_order_hist(const double* __restrict__ o, const double* __restrict__ d, long long n, double cx,
-                             double cy, double cz, double inv_span, unsigned* __restrict__ keys,
+                             double cy, double cz, double inv_span, double entry_r, unsigned* __restrict__ keys,
                              unsigned* __restrict__ hist) {
     const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
     if (i >= n) return;
     const double c[3] = { cx, cy, cz };
-    const unsigned k = ray_key(o + 3 * i, d + 3 * i, c, inv_span);
+    double p[3];
+    if (entry_r > 0.0) entry_point(o + 3 * i, d + 3 * i, c, entry_r, p);
+    else for (int a = 0; a < 3; ++a) p[a] = o[3 * i + a];
+    const unsigned k = ray_key(p, d + 3 * i, c, inv_span);
     keys[i] = k;
     atomicAdd(hist + k, 1u);
 }
@@ -120,17 +140,20 @@ size_t ray_order_workspace_bytes(long long n) {
 }
 
 // order[n] receives the processing order.  `ws` holds ray_order_workspace_bytes(n).
+// entry: key on the point where each ray enters the scene's sphere (else on its origin).
 cudaError_t ray_order(const double* o, const double* d, long long n, const double center[3], double radius,
-                      void* ws, int* order, cudaStream_t stream) {
+                      void* ws, int* order, cudaStream_t stream, bool entry) {
     if (n <= 0) return cudaSuccess;
     unsigned* hist = static_cast<unsigned*>(ws);
     unsigned* block_sums = hist + kOrderBuckets;
     unsigned* keys = block_sums + kScanBlocks;
     cudaError_t e = cudaMemsetAsync(hist, 0, sizeof(unsigned) * kOrderBuckets, stream);
     if (e != cudaSuccess) return e;
-    const double inv_span = radius > 0.0 ? 1.0 / (4.0 * radius) : 1.0;
+    // origins: a cube of four radii; entry points: the sphere's own cube
+    const double inv_span = radius > 0.0 ? 1.0 / ((entry ? 2.0 : 4.0) * radius) : 1.0;
     const unsigned blocks = static_cast<unsigned>((n + 255) / 256);
-    k_order_hist<<<blocks, 256, 0, stream>>>(o, d, n, center[0], center[1], center[2], inv_span, keys, hist);
+    k_order_hist<<<blocks, 256, 0, stream>>>(o, d, n, center[0], center[1], center[2], inv_span,
+                                             entry && radius > 0.0 ? radius : 0.0, keys, hist);
     k_order_scan_local<<<kScanBlocks, kScanBlock, 0, stream>>>(hist, block_sums);
     k_order_scan_add<<<kScanBlocks, kScanBlock, 0, stream>>>(hist, block_sums);
     k_order_scatter<<<blocks, 256, 0, stream>>>(keys, n, hist, order);
