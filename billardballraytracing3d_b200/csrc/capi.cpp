@@ -289,6 +289,9 @@ int ensure_uploaded(bbrt_scene* s) {
             nlink[4 * h + 3] = 0;
         }
     }
+    // the traversal stack keeps a node index in 24 bits
+    if (nn >= (static_cast<size_t>(1) << 24))
+        return fail(BBRT_ERR_UNSUPPORTED, "bbrt_scene_upload: more than 16,777,215 BVH nodes");
     // up to 3400 nodes (64 bytes each, 217 KB) in shared memory; launch shapes
     // with several blocks per SM stage fewer
     D.smem_nodes = static_cast<int>(std::min<size_t>(nn, 3400));
@@ -466,6 +469,7 @@ struct Tuning {
     int sort_requests = 1;            // group each round's Newton requests by patch before solving them
     int sort_side = 4;                // ... and within a patch by the side x side region of the stage-1 cell
     int order_entry = 1;              // round-0 order keyed on the scene-sphere entry point (else the origin)
+    int child_test = -1;              // k_advance child tests: -1 when the BVH exceeds the staged nodes, 0 / 1
 };
 
 // Launch-shape knobs; defaults tuned on B200, overridable for experiments by
@@ -488,6 +492,7 @@ const Tuning& tuning() {
         if (const char* e = std::getenv("BBRT_SORT_REQ")) v.sort_requests = std::atoi(e);
         if (const char* e = std::getenv("BBRT_SORT_SIDE")) v.sort_side = std::max(1, std::atoi(e));
         if (const char* e = std::getenv("BBRT_ORDER_ENTRY")) v.order_entry = std::atoi(e);
+        if (const char* e = std::getenv("BBRT_CHILD_TEST")) v.child_test = std::atoi(e);
         return v;
     }();
     return t;
@@ -598,6 +603,7 @@ int build_wave_graph(bbrt_scene* s, const bbrt::TraceArgs& A, const bbrt_tuning&
     W.counters = c;
     W.warp_stage1 = T.warp_stage1;
     W.resume_queries = tuning().resume_queries;
+    W.child_test = tuning().child_test;
     W.group_newton = tuning().group_newton;
     W.n_runnable = n;   // sizes the persistent grid; later rounds read their count
     if (T.order_rays) W.order = static_cast<const int*>(s->order.p);
@@ -793,6 +799,7 @@ struct WaveRun {
         W.counters = static_cast<unsigned int*>(s->wave_ctr.p);
         W.warp_stage1 = T.warp_stage1;
         W.resume_queries = tuning().resume_queries;
+        W.child_test = tuning().child_test;
         W.group_newton = tuning().group_newton;
         W.runnable = nullptr;
         W.n_runnable = n;

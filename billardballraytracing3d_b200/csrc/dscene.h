@@ -152,6 +152,8 @@ struct WaveArgs {
     int* qs_stack = nullptr;
     int resume_queries = 1;
     int group_newton = 0;                      // Newton solves by 8-lane groups when the patches allow it
+    int child_test = -1;                       // k_advance tests a node's children with it (-1: when the
+                                               // tree is larger than the shared-memory copy)
     // Graph-launched trace: the launch's item count (runnable rays, requests,
     // tail rays) is read from this device word instead of the host argument,
     // and the Newton kernel copies each request it solves to next_req (the

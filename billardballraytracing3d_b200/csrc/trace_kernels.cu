@@ -614,6 +614,7 @@ struct AdvState {
     bool use_cull;
     CullRay cr;
     double best_t;
+    int best_ver;    // times best_t went down in this query, saturating at kStackAlways
     int best_obj;    // -1: no hit yet
     int best_e;      // resolved entry of the best patch hit, -1 for a triangle
     double tri_u, tri_v;
@@ -627,6 +628,17 @@ struct AdvState {
     Stage1 s1;
 };
 
+// Traversal stack entries of k_advance: node index in the low 24 bits, and
+// in the top 8 the best_ver at which the node's box passed ray_box_exact when
+// its parent pushed it.  A popped node whose tag equals the query's current
+// best_ver passed with the same best_t, so it passes again; any other tag
+// (kStackAlways: the root, resumed stacks, a saturated best_ver) re-tests the
+// box with the current best_t — the reference's test at the reference's
+// time, so the visit sequence is the reference's.
+constexpr unsigned kStackAlways = 0xFFu;
+constexpr unsigned kStackIdx = 0x00FFFFFFu;
+__device__ __forceinline__ int stack_entry(int idx, unsigned ver) { return static_cast<int>((ver << 24) | static_cast<unsigned>(idx)); }
+
 __device__ __forceinline__ void adv_start_query(const DScene& S, const TraceArgs& A, const RayCtx& r, AdvState& q,
                                                 int* stack) {
     q.inv[0] = 1.0 / r.d.x;
@@ -638,13 +650,14 @@ __device__ __forceinline__ void adv_start_query(const DScene& S, const TraceArgs
     q.use_cull = cull_ok(S, A.cull, r.o, r.d);
     if (q.use_cull) q.cr = make_cull_ray(S, r.o, r.d);
     q.best_t = CUDART_INF;
+    q.best_ver = 0;
     q.best_obj = -1;
     q.best_e = -1;
     q.err = 0;
     q.err_obj = -1;
     q.ev0 = q.ev1 = 0.0;
     q.sp = 0;
-    stack[q.sp++] = 0;
+    stack[q.sp++] = stack_entry(0, kStackAlways);
 }
 
 // Keeps the traversal state of a query that suspends for a Newton solve
@@ -665,8 +678,9 @@ __device__ __forceinline__ void save_query(const WaveArgs& W, long long i, const
     qd[0] = q.best_t;
     qd[1] = q.tri_u;
     qd[2] = q.tri_v;
+    // saved entries re-test their boxes when popped after the resume
     int* st = W.qs_stack + i * kSaveStack;
-    for (int k = 0; k < q.sp; ++k) st[k] = stack[k];
+    for (int k = 0; k < q.sp; ++k) st[k] = stack_entry(stack[k] & static_cast<int>(kStackIdx), kStackAlways);
 }
 
 // Resumes a suspended query where it stopped (false when none was saved).
@@ -700,8 +714,9 @@ __device__ __forceinline__ bool resume_query(const DScene& S, const TraceArgs& A
 constexpr long long kAdvanceWatchdog = 1LL << 35;   // SM cycles
 
 // NT threads per block, MINB blocks per SM requested from the register
-// allocator (launch shape variants of the same body).
-template <int NT, int MINB>
+// allocator (launch shape variants of the same body); CHILD: a node's
+// children are tested with it (see the traversal stack tags).
+template <int NT, int MINB, bool CHILD>
 __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, WaveArgs W) {
     Counters ctr, cray;
     RayTally tally;
@@ -740,12 +755,17 @@ __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, Wav
             if (q.sp == 0) {
                 mode = M_RESOLVE;
             } else {
-                const int idx = stack[--q.sp];
-                ++cray.node_tests;
-                const bool staged = idx < S.smem_nodes;
-                const double* box = staged ? sbox + 6 * idx : S.node_box + 6LL * idx;
-                if (ray_box_exact(r.o, q.inv, box, q.best_t)) {
-                    const int* link = staged ? slink + 4 * idx : S.node_link + 4LL * idx;
+                const int ent = stack[--q.sp];
+                const int idx = ent & static_cast<int>(kStackIdx);
+                const unsigned tag = static_cast<unsigned>(ent) >> 24;
+                bool pass = true;
+                if (tag == kStackAlways || tag != static_cast<unsigned>(q.best_ver)) {
+                    ++cray.node_tests;
+                    pass = ray_box_exact(r.o, q.inv, idx < S.smem_nodes ? sbox + 6 * idx : S.node_box + 6LL * idx,
+                                         q.best_t);
+                }
+                if (pass) {
+                    const int* link = idx < S.smem_nodes ? slink + 4 * idx : S.node_link + 4LL * idx;
                     if (link[1] < 0) {
                         q.leaf_start = link[0];
                         q.leaf_count = link[2];
@@ -755,10 +775,29 @@ __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, Wav
                         q.err = BBRT_RAY_STACK_OVERFLOW;
                         q.err_obj = -1;
                         mode = M_RESOLVE;
-                    } else {
+                    } else if constexpr (!CHILD) {
+                        // children tested when popped (tagged to re-test)
                         const int left = link[0], right = link[1];
-                        if (q.neg[link[3]]) { stack[q.sp++] = left; stack[q.sp++] = right; }
-                        else                { stack[q.sp++] = right; stack[q.sp++] = left; }
+                        const int el = stack_entry(left, kStackAlways), er = stack_entry(right, kStackAlways);
+                        if (q.neg[link[3]]) { stack[q.sp++] = el; stack[q.sp++] = er; }
+                        else                { stack[q.sp++] = er; stack[q.sp++] = el; }
+                    } else {
+                        // both children's boxes now (independent loads); a
+                        // child that fails would fail when popped as well
+                        const int left = link[0], right = link[1];
+                        const bool pl = ray_box_exact(
+                            r.o, q.inv, left < S.smem_nodes ? sbox + 6 * left : S.node_box + 6LL * left, q.best_t);
+                        const bool pr = ray_box_exact(
+                            r.o, q.inv, right < S.smem_nodes ? sbox + 6 * right : S.node_box + 6LL * right, q.best_t);
+                        cray.node_tests += 2;
+                        const unsigned v = static_cast<unsigned>(q.best_ver);
+                        if (q.neg[link[3]]) {
+                            if (pl) stack[q.sp++] = stack_entry(left, v);
+                            if (pr) stack[q.sp++] = stack_entry(right, v);
+                        } else {
+                            if (pr) stack[q.sp++] = stack_entry(right, v);
+                            if (pl) stack[q.sp++] = stack_entry(left, v);
+                        }
                     }
                 }
             }
@@ -771,6 +810,7 @@ __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, Wav
                     QHit h;
                     if (triangle_intersect(S, S.obj_sub[obj], r.o, r.d, h, cray) && h.t < q.best_t) {
                         q.best_t = h.t;
+                        if (q.best_ver < static_cast<int>(kStackAlways)) ++q.best_ver;
                         q.best_obj = obj;
                         q.best_e = -1;
                         q.tri_u = h.u;
@@ -794,6 +834,7 @@ __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, Wav
                             const double t = W.res_data[ei * kResData];
                             if (t < q.best_t) {
                                 q.best_t = t;
+                                if (q.best_ver < static_cast<int>(kStackAlways)) ++q.best_ver;
                                 q.best_obj = obj;
                                 q.best_e = e;
                             }
@@ -1476,17 +1517,15 @@ void wave_layout(void* ws, long long n, WaveArgs& W, NewtonRequest*& req_a, Newt
 
 size_t wave_workspace_bytes(long long n) { return wave_bytes_per_ray() * n + 20 * 256; }
 
-template <int NT, int MINB>
-static cudaError_t launch_advance_shape(const DScene& S, const TraceArgs& A, const WaveArgs& W, int sm_count,
-                                        int max_smem_nodes, cudaStream_t stream) {
-    DScene Sl = S;
-    if (Sl.smem_nodes > max_smem_nodes) Sl.smem_nodes = max_smem_nodes;
+template <int NT, int MINB, bool CHILD>
+static cudaError_t launch_advance_variant(const DScene& Sl, const TraceArgs& A, const WaveArgs& W, int sm_count,
+                                          cudaStream_t stream) {
     const size_t smem = static_cast<size_t>(Sl.smem_nodes) * (6 * sizeof(double) + 4 * sizeof(int));
-    cudaError_t e = cudaFuncSetAttribute(k_advance<NT, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(k_advance<NT, MINB, CHILD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_advance<NT, MINB>, NT, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_advance<NT, MINB, CHILD>, NT, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
     // A small round (the late ones) is spread over every SM with smaller
@@ -1498,8 +1537,20 @@ static cudaError_t launch_advance_shape(const DScene& S, const TraceArgs& A, con
     long long blocks = static_cast<long long>(per_sm) * sm_count;
     const long long need = (W.n_runnable + threads - 1) / threads;
     if (blocks > need) blocks = need;
-    k_advance<NT, MINB><<<static_cast<unsigned>(blocks), threads, smem, stream>>>(Sl, A, W);
+    k_advance<NT, MINB, CHILD><<<static_cast<unsigned>(blocks), threads, smem, stream>>>(Sl, A, W);
     return cudaGetLastError();
+}
+
+template <int NT, int MINB>
+static cudaError_t launch_advance_shape(const DScene& S, const TraceArgs& A, const WaveArgs& W, int sm_count,
+                                        int max_smem_nodes, cudaStream_t stream) {
+    DScene Sl = S;
+    if (Sl.smem_nodes > max_smem_nodes) Sl.smem_nodes = max_smem_nodes;
+    // children tested with their parent (loads overlapped) when part of the
+    // tree stays in global memory; unless set (0 / 1) by the caller
+    const bool child = W.child_test < 0 ? S.n_nodes > Sl.smem_nodes : W.child_test != 0;
+    return child ? launch_advance_variant<NT, MINB, true>(Sl, A, W, sm_count, stream)
+                 : launch_advance_variant<NT, MINB, false>(Sl, A, W, sm_count, stream);
 }
 
 // Launch shapes of k_advance: 0 = 128 threads x 3 blocks per SM,
