@@ -470,6 +470,7 @@ struct Tuning {
     int sort_side = 4;                // ... and within a patch by the side x side region of the stage-1 cell
     int order_entry = 1;              // round-0 order keyed on the scene-sphere entry point (else the origin)
     int child_test = -1;              // k_advance child tests: -1 when the BVH exceeds the staged nodes, 0 / 1
+    int half_stage1 = 1;              // k_advance stage 1 of two patches at a time by half-warps
 };
 
 // Launch-shape knobs; defaults tuned on B200, overridable for experiments by
@@ -493,6 +494,7 @@ const Tuning& tuning() {
         if (const char* e = std::getenv("BBRT_SORT_SIDE")) v.sort_side = std::max(1, std::atoi(e));
         if (const char* e = std::getenv("BBRT_ORDER_ENTRY")) v.order_entry = std::atoi(e);
         if (const char* e = std::getenv("BBRT_CHILD_TEST")) v.child_test = std::atoi(e);
+        if (const char* e = std::getenv("BBRT_HALF_S1")) v.half_stage1 = std::atoi(e);
         return v;
     }();
     return t;
@@ -604,6 +606,7 @@ int build_wave_graph(bbrt_scene* s, const bbrt::TraceArgs& A, const bbrt_tuning&
     W.warp_stage1 = T.warp_stage1;
     W.resume_queries = tuning().resume_queries;
     W.child_test = tuning().child_test;
+    W.half_stage1 = tuning().half_stage1;
     W.group_newton = tuning().group_newton;
     W.n_runnable = n;   // sizes the persistent grid; later rounds read their count
     if (T.order_rays) W.order = static_cast<const int*>(s->order.p);
@@ -800,6 +803,7 @@ struct WaveRun {
         W.warp_stage1 = T.warp_stage1;
         W.resume_queries = tuning().resume_queries;
         W.child_test = tuning().child_test;
+        W.half_stage1 = tuning().half_stage1;
         W.group_newton = tuning().group_newton;
         W.runnable = nullptr;
         W.n_runnable = n;

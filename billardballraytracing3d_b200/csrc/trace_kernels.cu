@@ -583,6 +583,73 @@ __device__ Stage1 warp_patch_stage1(const DScene& S, int pidx, const V3& o, cons
     return best;
 }
 
+// Stage 1 of one patch by a half-warp (lane hl of the half whose lanes are
+// hmask, the first being hbase): warp_patch_stage1's block, cell and
+// triangle tests over 16 lanes, and the same (t, key) winner on every lane of
+// the half.  With at most 16 blocks per patch and 16 cells per block each
+// level is still one ballot, so two halves take two patches in the time the
+// whole warp takes one.  The half's test counts (uniform over it) go to c.
+__device__ Stage1 half_patch_stage1(const DScene& S, int pidx, const V3& o, const V3& d, bool use_cull,
+                                    const CullRay& cr, int hl, unsigned hmask, int hbase, Counters& c) {
+    constexpr int WH = 16;
+    const int n = S.coarse_n, nc = n - 1;
+    const double* X = S.c_xyz + static_cast<long long>(pidx) * n * n * 3;
+    const double* CC = S.c_cell + static_cast<long long>(pidx) * nc * nc * 4;
+    Stage1 best;
+    ++c.patch_tests;
+    if (!(finite3(o) && finite3(d))) {
+        Counters dummy;
+        best = patch_stage1(S, pidx, o, d, false, cr, dummy);
+        c.tri_tests += 6LL * nc * nc;
+        return best;
+    }
+    if (use_cull) {
+        const int B = S.block_cells, NB = S.n_blocks_side, NB2 = NB * NB;
+        const float* BB = S.c_block_box + static_cast<long long>(pidx) * NB2 * 6;
+        const float* CB = S.c_cell_box + static_cast<long long>(pidx) * nc * nc * 6;
+        for (int b0 = 0; b0 < NB2; b0 += WH) {
+            const int b = b0 + hl;
+            unsigned bm = (__ballot_sync(hmask, b < NB2 && cull_box(BB + b * 6, cr)) >> hbase) & 0xFFFFu;
+            c.cell_tests += min(WH, NB2 - b0);
+            while (bm) {
+                const int bl = __ffs(bm) - 1;
+                bm &= bm - 1;
+                const int bi = (b0 + bl) / NB, bj = (b0 + bl) % NB;
+                const int i0 = bi * B, j0 = bj * B;
+                const int h = min(nc, i0 + B) - i0, w = min(nc, j0 + B) - j0;
+                for (int c0 = 0; c0 < h * w; c0 += WH) {
+                    const int ce = c0 + hl;
+                    const unsigned cm =
+                        (__ballot_sync(hmask, ce < h * w && cull_box(CB + ((i0 + ce / w) * nc + j0 + ce % w) * 6, cr)) >>
+                         hbase) & 0xFFFFu;
+                    c.cell_tests += min(WH, h * w - c0);
+                    c.tri_tests += 6 * __popc(cm);
+                    const int total = __popc(cm) * 6;
+                    for (int p0 = 0; p0 < total; p0 += WH) {
+                        const int p = p0 + hl;
+                        if (p < total) {
+                            const int cell = c0 + __fns(cm, 0, p / 6 + 1);
+                            stage1_tri(X, CC, n, i0 + cell / w, j0 + cell % w, p % 6, o, d, best);
+                        }
+                    }
+                }
+            }
+        }
+    } else {
+        const int total = nc * nc * 6;
+        for (int p = hl; p < total; p += WH) stage1_tri(X, CC, n, (p / 6) / nc, (p / 6) % nc, p % 6, o, d, best);
+        c.tri_tests += total;
+    }
+#pragma unroll
+    for (int off = WH / 2; off > 0; off >>= 1) {
+        const int oh = __shfl_xor_sync(hmask, best.have ? 1 : 0, off);
+        const double ot = __shfl_xor_sync(hmask, best.t, off);
+        const int ok = __shfl_xor_sync(hmask, best.key, off);
+        if (oh) best.consider(ot, ok);
+    }
+    return best;
+}
+
 // Advance-kernel modes.  The kernel is persistent: each lane owns one ray at
 // a time and the body is one flat loop in which every iteration does one
 // small unit of work for the lane's ray (one BVH node test, one leaf object,
@@ -715,8 +782,10 @@ constexpr long long kAdvanceWatchdog = 1LL << 35;   // SM cycles
 
 // NT threads per block, MINB blocks per SM requested from the register
 // allocator (launch shape variants of the same body); CHILD: a node's
-// children are tested with it (see the traversal stack tags).
-template <int NT, int MINB, bool CHILD>
+// children are tested with it (see the traversal stack tags); HALF: the
+// warp's queued stage 1s are taken two at a time by half-warps (patches of at
+// most 16 blocks of at most 16 cells).
+template <int NT, int MINB, bool CHILD, bool HALF>
 __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, WaveArgs W) {
     Counters ctr, cray;
     RayTally tally;
@@ -966,7 +1035,63 @@ __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, Wav
         // all 32 lanes: the block, cell and triangle tests of the patch are
         // split over the lanes and the (t, key) minimum is taken over the warp
         // (the same winner as the lane's own ordered loop).
-        if (W.warp_stage1) {
+        // (the HALF instance keeps the whole-warp path too and checks at run
+        // time: measured faster than an instance without it)
+        if (HALF && W.warp_stage1 && W.half_stage1 && S.n_blocks_side * S.n_blocks_side <= 16 &&
+            S.block_cells * S.block_cells <= 16) {
+            // two patches at a time, one per half-warp (the second half
+            // repeats the first patch when only one waits)
+            unsigned pend = __ballot_sync(kFull, mode == M_S1_WARP);
+            while (pend) {
+                const int src0 = __ffs(pend) - 1;
+                pend &= pend - 1;
+                const int src1 = pend ? __ffs(pend) - 1 : -1;
+                if (pend) pend &= pend - 1;
+                const int hh = lane >> 4;
+                const int src = (hh == 0 || src1 < 0) ? src0 : src1;
+                V3 so, sd;
+                so.x = __shfl_sync(kFull, r.o.x, src);
+                so.y = __shfl_sync(kFull, r.o.y, src);
+                so.z = __shfl_sync(kFull, r.o.z, src);
+                sd.x = __shfl_sync(kFull, r.d.x, src);
+                sd.y = __shfl_sync(kFull, r.d.y, src);
+                sd.z = __shfl_sync(kFull, r.d.z, src);
+                const int spidx = __shfl_sync(kFull, q.pidx, src);
+                const bool scull = __shfl_sync(kFull, q.use_cull ? 1 : 0, src) != 0;
+                CullRay scr;
+                scr.ox = __shfl_sync(kFull, q.cr.ox, src);
+                scr.oy = __shfl_sync(kFull, q.cr.oy, src);
+                scr.oz = __shfl_sync(kFull, q.cr.oz, src);
+                scr.ix = __shfl_sync(kFull, q.cr.ix, src);
+                scr.iy = __shfl_sync(kFull, q.cr.iy, src);
+                scr.iz = __shfl_sync(kFull, q.cr.iz, src);
+                scr.delta = __shfl_sync(kFull, q.cr.delta, src);
+                Counters c2;
+                const Stage1 res = half_patch_stage1(S, spidx, so, sd, scull, scr, lane & 15, 0xFFFFu << (16 * hh),
+                                                     16 * hh, c2);
+                __syncwarp();
+#pragma unroll
+                for (int hv = 0; hv < 2; ++hv) {
+                    const int leader = 16 * hv;
+                    const int have = __shfl_sync(kFull, res.have ? 1 : 0, leader);
+                    const double st = __shfl_sync(kFull, res.t, leader);
+                    const int sk = __shfl_sync(kFull, res.key, leader);
+                    const long long pt = __shfl_sync(kFull, c2.patch_tests, leader);
+                    const long long ct = __shfl_sync(kFull, c2.cell_tests, leader);
+                    const long long tt = __shfl_sync(kFull, c2.tri_tests, leader);
+                    const int owner = hv == 0 ? src0 : src1;
+                    if (lane == owner) {
+                        q.s1.have = have != 0;
+                        q.s1.t = st;
+                        q.s1.key = sk;
+                        cray.patch_tests += pt;
+                        cray.cell_tests += ct;
+                        cray.tri_tests += tt;
+                        mode = M_S1_DONE;
+                    }
+                }
+            }
+        } else if (W.warp_stage1) {
             unsigned pend = __ballot_sync(kFull, mode == M_S1_WARP);
             while (pend) {
                 const int src = __ffs(pend) - 1;
@@ -1517,15 +1642,15 @@ void wave_layout(void* ws, long long n, WaveArgs& W, NewtonRequest*& req_a, Newt
 
 size_t wave_workspace_bytes(long long n) { return wave_bytes_per_ray() * n + 20 * 256; }
 
-template <int NT, int MINB, bool CHILD>
+template <int NT, int MINB, bool CHILD, bool HALF>
 static cudaError_t launch_advance_variant(const DScene& Sl, const TraceArgs& A, const WaveArgs& W, int sm_count,
                                           cudaStream_t stream) {
     const size_t smem = static_cast<size_t>(Sl.smem_nodes) * (6 * sizeof(double) + 4 * sizeof(int));
-    cudaError_t e = cudaFuncSetAttribute(k_advance<NT, MINB, CHILD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(k_advance<NT, MINB, CHILD, HALF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_advance<NT, MINB, CHILD>, NT, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_advance<NT, MINB, CHILD, HALF>, NT, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
     // A small round (the late ones) is spread over every SM with smaller
@@ -1537,7 +1662,7 @@ static cudaError_t launch_advance_variant(const DScene& Sl, const TraceArgs& A, 
     long long blocks = static_cast<long long>(per_sm) * sm_count;
     const long long need = (W.n_runnable + threads - 1) / threads;
     if (blocks > need) blocks = need;
-    k_advance<NT, MINB, CHILD><<<static_cast<unsigned>(blocks), threads, smem, stream>>>(Sl, A, W);
+    k_advance<NT, MINB, CHILD, HALF><<<static_cast<unsigned>(blocks), threads, smem, stream>>>(Sl, A, W);
     return cudaGetLastError();
 }
 
@@ -1549,8 +1674,13 @@ static cudaError_t launch_advance_shape(const DScene& S, const TraceArgs& A, con
     // children tested with their parent (loads overlapped) when part of the
     // tree stays in global memory; unless set (0 / 1) by the caller
     const bool child = W.child_test < 0 ? S.n_nodes > Sl.smem_nodes : W.child_test != 0;
-    return child ? launch_advance_variant<NT, MINB, true>(Sl, A, W, sm_count, stream)
-                 : launch_advance_variant<NT, MINB, false>(Sl, A, W, sm_count, stream);
+    if (child) return launch_advance_variant<NT, MINB, true, false>(Sl, A, W, sm_count, stream);
+    // half-warp stage 1 where a patch's blocks and a block's cells fit 16 lanes
+    // (with the child tests as well it measured slower: not combined)
+    const bool half = W.half_stage1 && W.warp_stage1 && S.n_blocks_side * S.n_blocks_side <= 16 &&
+                      S.block_cells * S.block_cells <= 16;
+    return half ? launch_advance_variant<NT, MINB, false, true>(Sl, A, W, sm_count, stream)
+                : launch_advance_variant<NT, MINB, false, false>(Sl, A, W, sm_count, stream);
 }
 
 // Launch shapes of k_advance: 0 = 128 threads x 3 blocks per SM,
