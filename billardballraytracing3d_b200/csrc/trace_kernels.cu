@@ -1671,16 +1671,17 @@ static cudaError_t launch_advance_shape(const DScene& S, const TraceArgs& A, con
                                         int max_smem_nodes, cudaStream_t stream) {
     DScene Sl = S;
     if (Sl.smem_nodes > max_smem_nodes) Sl.smem_nodes = max_smem_nodes;
-    // children tested with their parent (loads overlapped) when part of the
-    // tree stays in global memory; unless set (0 / 1) by the caller
-    const bool child = W.child_test < 0 ? S.n_nodes > Sl.smem_nodes : W.child_test != 0;
-    if (child) return launch_advance_variant<NT, MINB, true, false>(Sl, A, W, sm_count, stream);
-    // half-warp stage 1 where a patch's blocks and a block's cells fit 16 lanes
-    // (with the child tests as well it measured slower: not combined)
+    // Half-warp stage 1 where a patch's blocks and a block's cells fit 16
+    // lanes; else child tests when part of the tree stays in global memory.
+    // The two together measured slower than either, and on both scenes
+    // measured the half-warp stage 1 beats the child tests.
+    if (W.child_test > 0) return launch_advance_variant<NT, MINB, true, false>(Sl, A, W, sm_count, stream);
     const bool half = W.half_stage1 && W.warp_stage1 && S.n_blocks_side * S.n_blocks_side <= 16 &&
                       S.block_cells * S.block_cells <= 16;
-    return half ? launch_advance_variant<NT, MINB, false, true>(Sl, A, W, sm_count, stream)
-                : launch_advance_variant<NT, MINB, false, false>(Sl, A, W, sm_count, stream);
+    if (half) return launch_advance_variant<NT, MINB, false, true>(Sl, A, W, sm_count, stream);
+    const bool child = W.child_test < 0 && S.n_nodes > Sl.smem_nodes;
+    return child ? launch_advance_variant<NT, MINB, true, false>(Sl, A, W, sm_count, stream)
+                 : launch_advance_variant<NT, MINB, false, false>(Sl, A, W, sm_count, stream);
 }
 
 // Launch shapes of k_advance: 0 = 128 threads x 3 blocks per SM,
