@@ -1673,8 +1673,8 @@ static cudaError_t launch_advance_shape(const DScene& S, const TraceArgs& A, con
     if (Sl.smem_nodes > max_smem_nodes) Sl.smem_nodes = max_smem_nodes;
     // Half-warp stage 1 where a patch's blocks and a block's cells fit 16
     // lanes; else child tests when part of the tree stays in global memory.
-    // The two together measured slower than either, and on both scenes
-    // measured the half-warp stage 1 beats the child tests.
+    // The two together measured slower than either, and on both measured
+    // scenes the half-warp stage 1 beat the child tests.
     if (W.child_test > 0) return launch_advance_variant<NT, MINB, true, false>(Sl, A, W, sm_count, stream);
     const bool half = W.half_stage1 && W.warp_stage1 && S.n_blocks_side * S.n_blocks_side <= 16 &&
                       S.block_cells * S.block_cells <= 16;
