@@ -70,6 +70,10 @@ def parse():
                     help="also time K uneven scenes traced together (bbrt_trace_batch) vs one after another")
     ap.add_argument("--forms", default="plain,split,learned",
                     help="forms to time besides the headline (learned); e.g. 'learned' alone for profiling")
+    ap.add_argument("--second", default="ellipsoids",
+                    help="second workload whose plain / split / learned forms are reported beside the "
+                         "headline ('' skips it)")
+    ap.add_argument("--second-rays", type=int, default=None, help="rays of the second workload (default: its own)")
     return ap.parse_args()
 
 
@@ -164,7 +168,7 @@ def advance_roofline(st, fp64_peak, fp32_peak, l2_peak):
     """Roofline of the dominant kernel, k_advance, from its own counters and its
     own device time (CUDA events around each launch inside the library).
 
-    Work per unit (the model DESIGN.md states):
+    Work per unit:
       BVH node test          12 FP64 FLOP, 64 B (box + links)
       block / cell box test  18 FP32 FLOP, 24 B
       Moller-Trumbore test   28 FP64 FLOP up to the division-free rejection
@@ -335,27 +339,53 @@ def _max_over_ranks(kern_s, total_b, dev, world):
     return float(t.item()), int(b.item())
 
 
-def _accuracy(scene, o, d, maxb, C, K=8):
+def _newton_failures(status, C):
+    return int(np.isin(status, [C.RAY_NEWTON_SINGULAR, C.RAY_NEWTON_NOCONV, C.RAY_NEWTON_DOMAIN]).sum())
+
+
+def _accuracy(scene, o, d, maxb, C):
     """The learned FP32/FP64 form against the plain FP64 form (bit-identical to
-    the reference) on the same rays: share of rays with the same status and
-    hit-object sequence, largest hit-point difference over those rays, and
-    Newton failures of each."""
-    outs = ("status", "bounce_count", "hit_object", "hit_point")
+    the reference) on the same rays, every bounce of every ray recorded: share
+    of rays with the same status and hit-object sequence (also over the rays
+    whose incidence cosine exceeds 1e-3 at every bounce), the largest
+    difference of any hit point, end point and exit direction over those rays,
+    and Newton failures of each form."""
+    from billardballraytracing3d_b200 import api
     scene.set_modes(C.PREC_FP64, C.GUESS_TRIANGLE)
-    a = scene.trace(o, d, maxb, record=K, outputs=outs)
+    a = api.trace_recording_all(scene, o, d, maxb)
     scene.set_modes(C.PREC_SPLIT, C.GUESS_LEARNED)
-    b = scene.trace(o, d, maxb, record=K, outputs=outs)
-    same = (a["status"] == b["status"]) & (a["bounce_count"] == b["bounce_count"])
-    same &= np.all(a["hit_object"] == b["hit_object"], axis=1)
-    mask = np.arange(K)[None, :] < np.minimum(a["bounce_count"], K)[:, None]
-    diff = np.abs(a["hit_point"] - b["hit_point"]).max(axis=2)
-    err = float(np.max(np.where(mask & same[:, None], diff, 0.0)))
-    newton_fail = lambda r: int(np.isin(r["status"], [C.RAY_NEWTON_SINGULAR, C.RAY_NEWTON_NOCONV,  # noqa: E731
-                                                      C.RAY_NEWTON_DOMAIN]).sum())
-    return {"rays": int(o.shape[0]), "sequence_agreement": float(np.mean(same)), "max_hit_err_agreeing": err,
-            "hit_err_bound": 1e-10, "within_bound": bool(err <= 1e-10),
-            "newton_failures_plain": newton_fail(a), "newton_failures_learned": newton_fail(b),
-            "compared": f"status, hit-object sequence and first {K} hit points vs the plain FP64 form"}
+    b = api.trace_recording_all(scene, o, d, maxb)
+    K = max(a["hit_object"].shape[1], b["hit_object"].shape[1])
+    if a["hit_object"].shape[1] != K:
+        scene.set_modes(C.PREC_FP64, C.GUESS_TRIANGLE)
+        a = scene.trace(o, d, maxb, record=K)
+    if b["hit_object"].shape[1] != K:
+        scene.set_modes(C.PREC_SPLIT, C.GUESS_LEARNED)
+        b = scene.trace(o, d, maxb, record=K)
+    r = api.compare_traces(a, b, o)
+    r.update({"newton_failures_plain": _newton_failures(a["status"], C),
+              "newton_failures_learned": _newton_failures(b["status"], C),
+              "off_patch_misses_learned": int(b["stats"]["off_patch"]),
+              "went_inside_plain": int((a["status"] == C.RAY_WENT_INSIDE).sum()),
+              "went_inside_learned": int((b["status"] == C.RAY_WENT_INSIDE).sum()),
+              "recorded_bounces": int(K),
+              "compared": "status, hit-object sequence and every recorded hit point, end point and exit direction "
+                          "vs the plain FP64 form"})
+    return r
+
+
+def _form_report(secs, b, st, steps):
+    """One timed form: rate, step time, Newton work per hit and kernel split."""
+    bounces = max(1, st["bounces"])
+    fails = sum(st["status_hist"][k] for k in (2, 3, 4))
+    return {"value": b / secs, "unit": UNIT, "ms_per_step": 1e3 * secs / steps,
+            "newton_iters_fp64": st["newton_iters"], "newton_iters_fp32": st["newton_iters_fp32"],
+            "newton_iters_per_hit": (st["newton_iters"] + st["newton_iters_fp32"]) / bounces,
+            "newton_iters_fp64_per_hit": st["newton_iters"] / bounces,
+            "newton_failed_rays": int(fails), "newton_failure_rate": fails / max(1, st["rays"]),
+            "off_patch_misses": st.get("off_patch", 0),
+            "newton_ms": st["newton_ms"], "guess_ms": st["guess_ms"],
+            "advance_ms": st["advance_ms"], "tail_ms": st["tail_ms"]}
 
 
 def run_ours(args, rank, world, local_rank):
@@ -456,10 +486,7 @@ def run_ours(args, rank, world, local_rank):
         else None
     per_launch_s = kern_s / args.steps
     roofline = advance_roofline(stats, fp64_peak, fp32_peak, l2_peak) if stats else None
-    form = lambda secs, b, st: {"value": b / secs, "unit": UNIT, "ms_per_step": 1e3 * secs / args.steps,  # noqa: E731
-                                "newton_iters_fp64": st["newton_iters"], "newton_iters_fp32": st["newton_iters_fp32"],
-                                "newton_ms": st["newton_ms"], "guess_ms": st["guess_ms"],
-                                "advance_ms": st["advance_ms"], "tail_ms": st["tail_ms"]}
+    form = lambda secs, b, st: _form_report(secs, b, st, args.steps)  # noqa: E731
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * per_launch_s, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32 (BF16 MLP guess)", "data": "synthetic",
@@ -483,11 +510,56 @@ def run_ours(args, rank, world, local_rank):
             if stats else None,
             "wall_s_timed_region": wall,
             "counters_per_step": {k: v for k, v in (stats or {}).items() if k not in ("kernel_ms", "total_ms")}}
+    if args.second:
+        line["second_workload"] = second_workload(args, dev, stream, flush)
     if args.multi_scene > 0:
         line["multi_scene"] = multi_scene(args.multi_scene, args.steps, dev)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(patches, o, d, maxb, cn, tol, args.cpu_seconds)
     print(json.dumps(line), flush=True)
+
+
+def second_workload(args, dev, stream, flush):
+    """The second workload (default: the random-ellipsoid scene, 16 ellipsoids
+    x 384 patches, 4,194,304 rays in a 20-degree cone, <= 100 bounces) traced
+    in the plain FP64 form, the split form and the learned-guess form (network
+    trained on this GPU on a separately seeded ray set of the same source),
+    each timed like the headline; with Newton failure rates, Newton iterations
+    per hit, and the learned form's accuracy against the plain one."""
+    import torch
+    from billardballraytracing3d_b200 import _capi as C
+    from billardballraytracing3d_b200 import api, scenes
+    patches, o, d, maxb, cn, tol = scenes.workload(args.second, args.second_rays)
+    n = o.shape[0]
+    sc = api.Scene(patches, config=C.default_config(coarse_grid_n=cn, newton_tol=tol, cull=args.cull))
+    sc.upload()
+    train_o, train_d = scenes.cone_rays(args.train_rays, 99, *TRAIN_SOURCE.get(args.second, (5.0, 3.0, 10.0)))
+    training = sc.guess_train(train_o, train_d, maxb, epochs=args.train_epochs)
+    to = torch.from_numpy(np.ascontiguousarray(o)).to(dev)
+    td = torch.from_numpy(np.ascontiguousarray(d)).to(dev)
+    st_ = torch.empty(n, dtype=torch.int32, device=dev)
+    bc = torch.empty(n, dtype=torch.int32, device=dev)
+    ed = torch.empty((n, 3), dtype=torch.float64, device=dev)
+    outs = dict(status=st_.data_ptr(), bounce_count=bc.data_ptr(), exit_dir=ed.data_ptr())
+    steps, warmup = max(1, min(args.steps, 5)), 3
+    forms = {}
+    for name, prec, guess in (("plain_fp64_triangle", C.PREC_FP64, C.GUESS_TRIANGLE),
+                              ("split_triangle", C.PREC_SPLIT, C.GUESS_TRIANGLE),
+                              ("learned_split", C.PREC_SPLIT, C.GUESS_LEARNED)):
+        sc.set_modes(prec, guess)
+        secs, _, st = _trace_form(sc, to, td, n, maxb, outs, stream, flush, steps, warmup, dev, 1)
+        forms[name] = _form_report(secs, int(bc.sum().item()) * steps, st, steps)
+    forms["learned_over_plain"] = forms["learned_split"]["value"] / forms["plain_fp64_triangle"]["value"]
+    acc = None
+    if args.accuracy_rays > 0:
+        m = min(n, args.accuracy_rays)
+        acc = _accuracy(sc, o[:m], d[:m], maxb, C)
+    sc.set_modes(C.PREC_FP64, C.GUESS_TRIANGLE)
+    return {"config": workload_config(args.second, n, maxb, cn, tol), "steps": steps, "warmup": warmup,
+            "forms": forms, "accuracy": acc, "guess_training": training,
+            "note": "device time per step (CUDA events, L2 flushed before each step), default launch schedule; "
+                    "newton_failure_rate = rays failed by Newton / rays; newton_iters_per_hit = FP32 + FP64 "
+                    "Newton iterations / ray-bounces"}
 
 
 def multi_scene(k, steps, dev):

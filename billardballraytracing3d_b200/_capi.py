@@ -166,6 +166,7 @@ class TraceStats(ctypes.Structure):
         ("tail_tri_tests", ctypes.c_longlong), ("tail_newton_iters", ctypes.c_longlong),
         ("launches", ctypes.c_longlong),
         ("guess_used", ctypes.c_longlong), ("guess_fallback", ctypes.c_longlong), ("guess_ms", ctypes.c_double),
+        ("off_patch", ctypes.c_longlong),
     ]
 
     def as_dict(self):
@@ -178,7 +179,8 @@ class Tuning(ctypes.Structure):
     _fields_ = [
         ("advance_shape", ctypes.c_int), ("warp_stage1", ctypes.c_int), ("order_rays", ctypes.c_int),
         ("warp_tail", ctypes.c_int), ("wave_tail", ctypes.c_longlong), ("wave_min_rays", ctypes.c_longlong),
-        ("graph_rounds", ctypes.c_int),
+        ("graph_rounds", ctypes.c_int), ("watchdog_cycles", ctypes.c_longlong),
+        ("mma_wait_cycles", ctypes.c_longlong),
     ]
 
     def as_dict(self):

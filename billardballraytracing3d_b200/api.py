@@ -302,3 +302,65 @@ def read_patch_file(path: str) -> Dict:
         return out
     finally:
         lib.bbrt_patch_file_free(ctypes.byref(f))
+
+
+def trace_recording_all(scene: "Scene", origins, dirs, max_bounces: int, first_record: int = 16) -> TraceResult:
+    """scene.trace with every bounce of every ray recorded: traces with
+    `first_record` recorded bounces and, when some ray bounced more often,
+    again with the largest bounce count."""
+    r = scene.trace(origins, dirs, max_bounces, record=first_record)
+    k = int(r["bounce_count"].max()) if r["bounce_count"].size else 0
+    if k > first_record:
+        r = scene.trace(origins, dirs, max_bounces, record=k)
+    return r
+
+
+def min_incidence_cos(origins, r: TraceResult) -> np.ndarray:
+    """Per ray, the smallest incidence cosine over its recorded bounces,
+    recomputed from the path alone: the ray arrives along d_in and leaves
+    along d_out = d_in - 2 (d_in . n) n, so |d_in . n| = sqrt((1 - d_in . d_out) / 2).
+    The leg after the last hit is exit_dir; rays without a hit get 1."""
+    o = np.asarray(origins, dtype=np.float64).reshape(-1, 3)
+    b = r["bounce_count"]
+    n, K = r["hit_point"].shape[:2]
+    pts = np.concatenate([o[:, None, :], r["hit_point"]], axis=1)            # [n, K+1, 3]
+    legs = np.diff(pts, axis=1)                                                # leg k ends at hit k
+    legs /= np.maximum(np.linalg.norm(legs, axis=2, keepdims=True), 1e-300)
+    out_legs = np.concatenate([legs[:, 1:], np.zeros((n, 1, 3))], axis=1)
+    last = np.clip(b - 1, 0, max(K - 1, 0))
+    out_legs[np.arange(n), last] = r["exit_dir"]
+    cos2 = np.clip((1.0 - np.sum(legs * out_legs, axis=2)) * 0.5, 0.0, 1.0)
+    cos = np.sqrt(cos2)
+    mask = np.arange(K)[None, :] < np.minimum(b, K)[:, None]
+    return np.where(mask, cos, 1.0).min(axis=1) if K else np.ones(n)
+
+
+def compare_traces(ref: TraceResult, other: TraceResult, origins=None, bound: float = 1e-10,
+                   grazing_cos: float = 1e-3) -> Dict:
+    """Ray-by-ray agreement of two traces of the same rays, both recorded
+    with every bounce (trace_recording_all): the share of rays with the same
+    status, bounce count and hit-object sequence, and over those rays the
+    largest difference of any recorded hit point, of the end point and of the
+    exit direction.  With `origins`, the same share over the rays whose
+    incidence cosine (in `ref`) exceeds `grazing_cos` at every bounce."""
+    K = ref["hit_object"].shape[1]
+    if int(ref["bounce_count"].max(initial=0)) > K or int(other["bounce_count"].max(initial=0)) > other["hit_object"].shape[1]:
+        raise ValueError("compare_traces: a trace did not record every bounce")
+    if other["hit_object"].shape[1] != K:
+        raise ValueError("compare_traces: the traces recorded different bounce counts")
+    same = (ref["status"] == other["status"]) & (ref["bounce_count"] == other["bounce_count"])
+    same &= np.all(ref["hit_object"] == other["hit_object"], axis=1)
+    mask = np.arange(K)[None, :] < np.minimum(ref["bounce_count"], K)[:, None]
+    diff = np.abs(ref["hit_point"] - other["hit_point"]).max(axis=2) if K else np.zeros((same.size, 0))
+    err_hit = float(np.max(np.where(mask & same[:, None], diff, 0.0), initial=0.0))
+    err_end = float(np.max(np.where(same[:, None], np.abs(ref["end_point"] - other["end_point"]), 0.0), initial=0.0))
+    err_exit = float(np.max(np.where(same[:, None], np.abs(ref["exit_dir"] - other["exit_dir"]), 0.0), initial=0.0))
+    out = {"rays": int(same.size), "sequence_agreement": float(np.mean(same)) if same.size else 1.0,
+           "max_hit_err_agreeing": err_hit, "max_end_point_err_agreeing": err_end,
+           "max_exit_dir_err_agreeing": err_exit, "bounces_compared": int(mask.sum()),
+           "hit_err_bound": bound, "within_bound": bool(max(err_hit, err_end, err_exit) <= bound)}
+    if origins is not None:
+        ok = min_incidence_cos(origins, ref) > grazing_cos
+        out["non_grazing_rays"] = int(ok.sum())
+        out["sequence_agreement_non_grazing"] = float(np.mean(same[ok])) if ok.any() else 1.0
+    return out

@@ -52,6 +52,7 @@ cudaError_t sort_requests(const NewtonRequest* req, long long n, const unsigned*
 cudaError_t ray_order(const double* o, const double* d, long long n, const double center[3], double radius,
                       void* ws, int* order, cudaStream_t stream, bool entry);
 cudaError_t launch_query(const DScene& S, const QueryArgs& Q, cudaStream_t stream);
+cudaError_t noalloc_prepare();
 cudaError_t launch_trace_noalloc(const DScene& S, TraceArgs A, bool count_hits, long long* hit_counts_out,
                                  long long* host_stats, cudaStream_t stream, int sm_count);
 int launch_umma_check(const uint16_t* A, const uint16_t* B, float* D, int* err, cudaStream_t st);
@@ -242,6 +243,9 @@ int ensure_uploaded(bbrt_scene* s) {
     BBRT_CUDA(cudaGetDevice(&s->device));
     BBRT_CUDA(cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, s->device));
     BBRT_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    // the allocation-free trace's module (scratch array and kernel) is loaded
+    // here, so that bbrt_trace_noalloc itself never triggers a module load
+    BBRT_CUDA(bbrt::noalloc_prepare());
     for (auto& e : s->ev) BBRT_CUDA(cudaEventCreate(&e));
     for (auto& e : s->kev) BBRT_CUDA(cudaEventCreate(&e));
     const bbrt::HostScene& H = s->host;
@@ -423,6 +427,7 @@ void fill_stats(bbrt_scene* s, const long long* st, long long n, float kernel_ms
     out->tail_rays = st[bbrt::ST_TAIL_RAYS];
     out->guess_used = st[bbrt::ST_GUESS_USED];
     out->guess_fallback = st[bbrt::ST_GUESS_FALLBACK];
+    out->off_patch = st[bbrt::ST_OFF_PATCH];
     double* dst[5] = { &out->order_ms, &out->advance_ms, &out->newton_ms, &out->tail_ms, &out->guess_ms };
     for (const auto& sp : s->kspans) {
         float ms = 0.0f;
@@ -509,6 +514,7 @@ bbrt::MlpNet guess_net(bbrt_scene* s) {
     M.loss = static_cast<float*>(s->guess.loss.p);
     M.out = nullptr;
     M.err = static_cast<int*>(s->guess.err.p);
+    M.mbar_limit = s->tune_set && s->tune.mma_wait_cycles > 0 ? s->tune.mma_wait_cycles : bbrt::kMbarDefault;
     return M;
 }
 
@@ -531,8 +537,15 @@ bbrt_tuning scene_tuning(const bbrt_scene* s) {
     t.wave_tail = T.wave_tail;
     t.wave_min_rays = T.wave_min_rays;
     t.graph_rounds = T.graph_rounds;
+    t.watchdog_cycles = 0;
+    t.mma_wait_cycles = 0;
     return t;
 }
+
+// The k_advance watchdog and the tensor-core wait bound of a schedule
+// (0 in the schedule: the defaults).
+long long watchdog_cycles(const bbrt_tuning& T) { return T.watchdog_cycles > 0 ? T.watchdog_cycles : 1LL << 35; }
+long long mma_wait_cycles(const bbrt_tuning& T) { return T.mma_wait_cycles > 0 ? T.mma_wait_cycles : bbrt::kMbarDefault; }
 
 cudaError_t run_tail(bbrt_scene* s, const bbrt::TraceArgs& A, const bbrt::WaveArgs& W,
                      const bbrt::NewtonRequest* reqs, const int* rays, long long n, cudaStream_t st) {
@@ -608,6 +621,7 @@ int build_wave_graph(bbrt_scene* s, const bbrt::TraceArgs& A, const bbrt_tuning&
     W.child_test = tuning().child_test;
     W.half_stage1 = tuning().half_stage1;
     W.group_newton = tuning().group_newton;
+    W.watchdog_cycles = watchdog_cycles(T);
     W.n_runnable = n;   // sizes the persistent grid; later rounds read their count
     if (T.order_rays) W.order = static_cast<const int*>(s->order.p);
     bbrt::WaveArgs W0 = W, Wr = W, Wn = W, Wt = W, Wo = W;
@@ -737,7 +751,8 @@ int launch_wave_graph(bbrt_scene* s, const bbrt::TraceArgs& A, const bbrt_tuning
                          static_cast<long long>(T.order_rays), static_cast<long long>(T.warp_tail), T.wave_tail,
                          static_cast<long long>(tuning().resume_queries), static_cast<long long>(tuning().group_newton),
                          static_cast<long long>(tuning().tail_shape), max_rounds,
-                         static_cast<long long>(sort_round_requests(s)) })
+                         static_cast<long long>(sort_round_requests(s)), watchdog_cycles(T), mma_wait_cycles(T),
+                         static_cast<long long>(A.off_patch_miss) })
         k.put(x);
     k.put(s->guess.min_logit);
     k.put(s->guess.t_window);
@@ -805,6 +820,7 @@ struct WaveRun {
         W.child_test = tuning().child_test;
         W.half_stage1 = tuning().half_stage1;
         W.group_newton = tuning().group_newton;
+        W.watchdog_cycles = watchdog_cycles(T);
         W.runnable = nullptr;
         W.n_runnable = n;
         W.req = req_a;
@@ -917,6 +933,23 @@ int run_wavefront(bbrt_scene* s, const bbrt::TraceArgs& A, cudaStream_t st, Grap
     return w.finish();
 }
 
+// Whether a trace of this scene runs the learned guess (its wavefront rounds do).
+bool learned_trace(const bbrt_scene* s) {
+    return s->host.cfg.guess == BBRT_GUESS_LEARNED && s->guess.trained && s->guess.err.p;
+}
+
+// Whether every tensor-core completion wait of a learned trace finished in
+// time (the flag is cleared when the trace is prepared).  After the trace's
+// work has completed.
+int check_guess_waits(bbrt_scene* s, cudaStream_t st) {
+    if (!learned_trace(s)) return BBRT_OK;
+    int e = 0;
+    BBRT_CUDA(cudaMemcpyAsync(&e, s->guess.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    BBRT_CUDA(cudaStreamSynchronize(st));
+    if (e) return fail(BBRT_ERR_KERNEL, "bbrt_trace: a tensor-core completion wait of the learned guess timed out");
+    return BBRT_OK;
+}
+
 // Launches the trace kernel on device arrays.  hit_counts (device, may be
 // null) receives per-object counts for bounces with index >= count_from.
 // Trace arguments of one call and the per-call resets (statistics, ray
@@ -954,6 +987,10 @@ int prepare_trace(bbrt_scene* s, const double* d_o, const double* d_d, long long
     A.sample_cap_neg = s->rec_cap_neg;
     if (want_stats) BBRT_CUDA(cudaMemsetAsync(s->stats.p, 0, sizeof(long long) * bbrt::ST_COUNT, st));
     BBRT_CUDA(cudaMemsetAsync(s->work.p, 0, sizeof(unsigned long long), st));
+    if (learned_trace(s)) {
+        BBRT_CUDA(cudaMemsetAsync(s->guess.err.p, 0, sizeof(int), st));
+        A.off_patch_miss = 1;
+    }
     s->timing = want_stats;
     s->kev_used = 0;
     s->kspans.clear();
@@ -993,10 +1030,13 @@ int run_trace_device(bbrt_scene* s, const double* d_o, const double* d_d, long l
         if (rc) return rc;
     }
     rc = complete_trace(s, st, want_stats, host_stats, kernel_ms);
-    if (rc || !graph.on) return rc;
-    // a graph-launched trace: one host wait, for its device-side bounds
-    BBRT_CUDA(cudaEventSynchronize(s->ev[1]));
-    return check_wave_graph(s, graph);
+    if (!rc && graph.on) {
+        // a graph-launched trace: one host wait, for its device-side bounds
+        BBRT_CUDA(cudaEventSynchronize(s->ev[1]));
+        rc = check_wave_graph(s, graph);
+    }
+    if (!rc && n >= scene_tuning(s).wave_min_rays) rc = check_guess_waits(s, st);
+    return rc;
 }
 
 }  // namespace
@@ -2005,6 +2045,8 @@ BBRT_API int bbrt_scene_set_tuning(bbrt_scene_t s, const bbrt_tuning* t) {
     if (t->advance_shape < 0 || t->advance_shape > 6) return fail(BBRT_ERR_ARG, "bbrt_scene_set_tuning: advance_shape must be 0..6");
     if (t->wave_tail < 0 || t->wave_min_rays < 0) return fail(BBRT_ERR_ARG, "bbrt_scene_set_tuning: negative size");
     if (t->graph_rounds != 0 && t->graph_rounds != 1) return fail(BBRT_ERR_ARG, "bbrt_scene_set_tuning: graph_rounds must be 0 or 1");
+    if (t->watchdog_cycles < 0 || t->mma_wait_cycles < 0)
+        return fail(BBRT_ERR_ARG, "bbrt_scene_set_tuning: negative wait bound");
     std::lock_guard<std::mutex> g(s->mu);
     s->tune = *t;
     s->tune_set = true;
@@ -2173,6 +2215,8 @@ BBRT_API int bbrt_trace_batch(const bbrt_scene_t* scenes, int n_scenes, const do
         if (cudaStreamSynchronize(scenes[k]->stream) != cudaSuccess) rc = fail(BBRT_ERR_CUDA, "bbrt_trace_batch: synchronisation failed");
     for (int k = 0; k < n_scenes && !rc; ++k)
         if (runs[k].graph.on) rc = check_wave_graph(scenes[k], runs[k].graph);
+    for (int k = 0; k < n_scenes && !rc; ++k)
+        if (n[k] >= scene_tuning(scenes[k]).wave_min_rays) rc = check_guess_waits(scenes[k], scenes[k]->stream);
     if (!rc && batch_ms) {
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, start, end);
@@ -2200,6 +2244,7 @@ BBRT_API int bbrt_trace_batch(const bbrt_scene_t* scenes, int n_scenes, const do
             stats->tail_rays += one.tail_rays;
             stats->guess_used += one.guess_used;
             stats->guess_fallback += one.guess_fallback;
+            stats->off_patch += one.off_patch;
         }
         if (batch_ms) stats->kernel_ms = stats->total_ms = *batch_ms;
     }

@@ -3,6 +3,9 @@
 // allocation; passed to kernels by value.
 #pragma once
 
+#include <cuda_runtime.h>
+
+#include <cmath>
 #include <cstdint>
 
 namespace bbrt {
@@ -73,6 +76,8 @@ enum StatSlot {
     ST_TAIL_NODE_TESTS = ST_HIST0 + 8, ST_TAIL_CELL_TESTS, ST_TAIL_TRI_TESTS, ST_TAIL_NEWTON_ITERS, ST_TAIL_RAYS,
     // learned guess: Newton solves started from the network, and those that fell back to the triangle
     ST_GUESS_USED, ST_GUESS_FALLBACK,
+    // learned form: patches whose Newton root lay outside the patch, taken as not hit
+    ST_OFF_PATCH,
     ST_COUNT
 };
 
@@ -103,7 +108,20 @@ struct TraceArgs {
     GuessSample* samples = nullptr;
     unsigned long long* sample_count = nullptr;
     long long sample_cap_pos = 0, sample_cap_neg = 0;
+    // Learned form: a patch whose Newton solve converges to a root outside
+    // the patch's parameter domain (|u| or |v| > 1 + 1e-6) is taken as not
+    // hit instead of failing the ray, unless the network placed a confident
+    // hit well inside the patch (then the root is suspect and the failure
+    // stands).  Off (0) in the plain and split forms, which keep the
+    // reference's failure.
+    int off_patch_miss = 0;
 };
+
+// Network outputs (u, v, t, logit) that place a confident hit well inside
+// the patch: they veto the learned form's off-patch miss.
+__host__ __device__ inline bool guess_inside(const double* g, double min_logit) {
+    return g != nullptr && g[3] > min_logit && fabs(g[0]) <= 0.95 && fabs(g[1]) <= 0.95;
+}
 
 // A patch query of the current bounce whose stage-1 winner needs Newton.
 struct NewtonRequest {
@@ -161,6 +179,8 @@ struct WaveArgs {
     // next round's runnable set); null in the host-driven trace.
     const unsigned int* count_dev = nullptr;
     NewtonRequest* next_req = nullptr;
+    // k_advance stops (counters[3] set) once it has run this many SM cycles.
+    long long watchdog_cycles = 1LL << 35;
 };
 
 // Round counters of the wavefront trace in device memory: [0..3] as

@@ -30,6 +30,9 @@ constexpr int kTrainX = kImageBytes, kTrainH1 = kTrainX + 128 * kIn * 2, kTrainH
 constexpr int kInferX = kImageBytes, kInferH = kInferX + 128 * kIn * 2, kInferBias = kInferH + 128 * kH * 2,
               kInferSmem = kInferBias + (3 * kH + kOut) * 4;
 
+// Default bound of a tensor-core completion wait (SM cycles, about 2 s).
+constexpr long long kMbarDefault = 4000000000LL;
+
 constexpr float kGeluC = 0.7978845608028654f;   // sqrt(2 / pi)
 constexpr float kGeluA = 0.044715f;
 
@@ -91,6 +94,7 @@ struct MlpNet {
     float* loss;            // loss accumulator
     float* out;             // optional [B][4] forward outputs of a training batch
     int* err;               // set when an MMA completion wait timed out
+    long long mbar_limit = kMbarDefault;   // SM cycles a completion wait may take before it gives up
 };
 
 cudaError_t mlp_pack(const float* P, uint8_t* image, cudaStream_t st);

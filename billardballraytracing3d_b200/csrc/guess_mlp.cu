@@ -23,7 +23,7 @@ namespace bbrt {
 
 using namespace umma;
 
-constexpr long long kMbarLimit = 4000000000LL;   // SM cycles (about 2 s) before a wait reports failure
+constexpr long long kMbarLimit = kMbarDefault;   // the self-check's bound (about 2 s of SM cycles)
 
 // ---- self-check of the operand layouts -------------------------------------
 //
@@ -137,10 +137,13 @@ __device__ __forceinline__ void ep_gelu(uint32_t lane_base, int zc, const float*
 }
 
 // One stage boundary: operands written and fenced by every thread, TMEM reads
-// done; thread 0 issues the MMAs of `issue` and commits; everyone waits.
-// Returns false (uniformly) when the wait timed out.
+// done; thread 0 issues the MMAs of `issue` and commits; everyone waits, at
+// most `limit` SM cycles.  Returns false (uniformly) when the wait timed out;
+// a thread whose wait gave up waits once more, with the default bound, so
+// that the MMAs already issued have finished with their operands and their
+// accumulator before the caller leaves and frees tensor memory.
 template <class Issue>
-__device__ __forceinline__ bool mma_stage(uint32_t mbar, uint32_t& phase, Issue&& issue) {
+__device__ __forceinline__ bool mma_stage(uint32_t mbar, uint32_t& phase, long long limit, Issue&& issue) {
     fence_before_sync();
     __syncthreads();
     fence_after_sync();
@@ -148,7 +151,8 @@ __device__ __forceinline__ bool mma_stage(uint32_t mbar, uint32_t& phase, Issue&
         issue();
         commit(mbar);
     }
-    const bool w = mbar_wait(mbar, phase, kMbarLimit);
+    const bool w = mbar_wait(mbar, phase, limit);
+    if (!w) mbar_wait(mbar, phase, kMbarDefault);
     phase ^= 1u;
     const bool ok = __syncthreads_and(w) != 0;
     fence_after_sync();
@@ -254,25 +258,25 @@ __global__ void __launch_bounds__(128, 1) k_mlp_train(MlpBatch Bt, MlpNet M) {
         }
         fence_async_smem();
         // ---- forward
-        ok = mma_stage(mbar, phase, [&] {
+        ok = mma_stage(mbar, phase, M.mbar_limit, [&] {
             for (int k = 0; k < kIn / 16; ++k) mma(tm, kmajor_desc(aX, kIn, k), kmajor_desc(aW0, kIn, k), ID_F, k > 0);
         });
         if (!ok) break;
         ep_gelu(lb, 0, sb, tH1, tid);
         fence_async_smem();
-        ok = mma_stage(mbar, phase, [&] {
+        ok = mma_stage(mbar, phase, M.mbar_limit, [&] {
             for (int k = 0; k < kH / 16; ++k) mma(tm + 128, kmajor_desc(aH1, kH, k), kmajor_desc(aW1, kH, k), ID_F, k > 0);
         });
         if (!ok) break;
         ep_gelu(lb, 128, sb + kH, tH2, tid);
         fence_async_smem();
-        ok = mma_stage(mbar, phase, [&] {
+        ok = mma_stage(mbar, phase, M.mbar_limit, [&] {
             for (int k = 0; k < kH / 16; ++k) mma(tm + 256, kmajor_desc(aH2, kH, k), kmajor_desc(aW2, kH, k), ID_F, k > 0);
         });
         if (!ok) break;
         ep_gelu(lb, 256, sb + 2 * kH, tH3, tid);
         fence_async_smem();
-        ok = mma_stage(mbar, phase, [&] {
+        ok = mma_stage(mbar, phase, M.mbar_limit, [&] {
             for (int k = 0; k < kH / 16; ++k) mma(tm + 384, kmajor_desc(aH3, kH, k), kmajor_desc(aW3, kH, k), ID_F16, k > 0);
         });
         if (!ok) break;
@@ -312,7 +316,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp_train(MlpBatch Bt, MlpNet M) {
         }
         fence_async_smem();
         // ---- backward, layer 3: dW3 = dZ4^T H3 (as [i][o] in TMEM, stored [o][i]), dH3 = dZ4 W3
-        ok = mma_stage(mbar, phase, [&] {
+        ok = mma_stage(mbar, phase, M.mbar_limit, [&] {
             for (int k = 0; k < 8; ++k)
                 mma(tm + 384, mnmajor_desc(aH3, kH, k), mnmajor_desc(aG4, kOut, k), idesc_bf16(128, 16, true, true), k > 0);
         });
@@ -323,20 +327,20 @@ __global__ void __launch_bounds__(128, 1) k_mlp_train(MlpBatch Bt, MlpNet M) {
 #pragma unroll
             for (int j = 0; j < 4; ++j) atomicAdd(G + oW3 + j * kH + tid, g[j]);
         }
-        ok = mma_stage(mbar, phase, [&] {
+        ok = mma_stage(mbar, phase, M.mbar_limit, [&] {
             mma(tm + 384, kmajor_desc(aG4, kOut, 0), mnmajor_desc(aW3, kH, 0), idesc_bf16(128, 128, false, true), false);
         });
         if (!ok) break;
         ep_dgelu(lb, 384, 256, sb + 2 * kH, tH3, tid, G + oB2);   // dZ3 over H3
         fence_async_smem();
         // ---- layer 2
-        ok = mma_stage(mbar, phase, [&] {
+        ok = mma_stage(mbar, phase, M.mbar_limit, [&] {
             for (int k = 0; k < 8; ++k)
                 mma(tm + 384, mnmajor_desc(aH3, kH, k), mnmajor_desc(aH2, kH, k), idesc_bf16(128, 128, true, true), k > 0);
         });
         if (!ok) break;
         ep_dw_oi(lb, 384, kH, G + oW2, tid);
-        ok = mma_stage(mbar, phase, [&] {
+        ok = mma_stage(mbar, phase, M.mbar_limit, [&] {
             for (int k = 0; k < 8; ++k)
                 mma(tm + 384, kmajor_desc(aH3, kH, k), mnmajor_desc(aW2, kH, k), idesc_bf16(128, 128, false, true), k > 0);
         });
@@ -344,13 +348,13 @@ __global__ void __launch_bounds__(128, 1) k_mlp_train(MlpBatch Bt, MlpNet M) {
         ep_dgelu(lb, 384, 128, sb + kH, tH2, tid, G + oB1);        // dZ2 over H2
         fence_async_smem();
         // ---- layer 1
-        ok = mma_stage(mbar, phase, [&] {
+        ok = mma_stage(mbar, phase, M.mbar_limit, [&] {
             for (int k = 0; k < 8; ++k)
                 mma(tm + 384, mnmajor_desc(aH2, kH, k), mnmajor_desc(aH1, kH, k), idesc_bf16(128, 128, true, true), k > 0);
         });
         if (!ok) break;
         ep_dw_oi(lb, 384, kH, G + oW1, tid);
-        ok = mma_stage(mbar, phase, [&] {
+        ok = mma_stage(mbar, phase, M.mbar_limit, [&] {
             for (int k = 0; k < 8; ++k)
                 mma(tm + 384, kmajor_desc(aH2, kH, k), mnmajor_desc(aW1, kH, k), idesc_bf16(128, 128, false, true), k > 0);
         });
@@ -358,13 +362,13 @@ __global__ void __launch_bounds__(128, 1) k_mlp_train(MlpBatch Bt, MlpNet M) {
         ep_dgelu(lb, 384, 0, sb, tH1, tid, G + oB0);                // dZ1 over H1
         fence_async_smem();
         // ---- layer 0: dW0 = dZ1^T X, dX = dZ1 W0 (embedding gradients)
-        ok = mma_stage(mbar, phase, [&] {
+        ok = mma_stage(mbar, phase, M.mbar_limit, [&] {
             for (int k = 0; k < 8; ++k)
                 mma(tm + 384, mnmajor_desc(aH1, kH, k), mnmajor_desc(aX, kIn, k), idesc_bf16(128, 64, true, true), k > 0);
         });
         if (!ok) break;
         ep_dw_oi(lb, 384, kIn, G + oW0, tid);
-        ok = mma_stage(mbar, phase, [&] {
+        ok = mma_stage(mbar, phase, M.mbar_limit, [&] {
             for (int k = 0; k < 8; ++k)
                 mma(tm + 384, kmajor_desc(aH1, kH, k), mnmajor_desc(aW0, kIn, k), idesc_bf16(128, 64, false, true), k > 0);
         });
@@ -433,25 +437,25 @@ __global__ void __launch_bounds__(128, 1) k_mlp_infer(Rows rows, long long n, co
             for (int k = 0; k < kGeo; ++k) geo[k] = 0.0f;
         put_input_row(tX, tid, geo, valid ? M.P + oE + static_cast<long long>(patch) * kEmb : nullptr);
         fence_async_smem();
-        ok = mma_stage(mbar, phase, [&] {
+        ok = mma_stage(mbar, phase, M.mbar_limit, [&] {
             for (int k = 0; k < kIn / 16; ++k) mma(tm, kmajor_desc(aX, kIn, k), kmajor_desc(aW0, kIn, k), ID_F, k > 0);
         });
         if (!ok) break;
         ep_gelu(lb, 0, sb, tH, tid);
         fence_async_smem();
-        ok = mma_stage(mbar, phase, [&] {
+        ok = mma_stage(mbar, phase, M.mbar_limit, [&] {
             for (int k = 0; k < kH / 16; ++k) mma(tm, kmajor_desc(aH, kH, k), kmajor_desc(aW1, kH, k), ID_F, k > 0);
         });
         if (!ok) break;
         ep_gelu(lb, 0, sb + kH, tH, tid);
         fence_async_smem();
-        ok = mma_stage(mbar, phase, [&] {
+        ok = mma_stage(mbar, phase, M.mbar_limit, [&] {
             for (int k = 0; k < kH / 16; ++k) mma(tm, kmajor_desc(aH, kH, k), kmajor_desc(aW2, kH, k), ID_F, k > 0);
         });
         if (!ok) break;
         ep_gelu(lb, 0, sb + 2 * kH, tH, tid);
         fence_async_smem();
-        ok = mma_stage(mbar, phase, [&] {
+        ok = mma_stage(mbar, phase, M.mbar_limit, [&] {
             for (int k = 0; k < kH / 16; ++k)
                 mma(tm, kmajor_desc(aH, kH, k), kmajor_desc(aW3, kH, k), idesc_bf16(128, 16, false, false), k > 0);
         });

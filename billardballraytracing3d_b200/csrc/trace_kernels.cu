@@ -28,6 +28,7 @@ namespace bbrt {
 
 struct Counters {
     long long node_tests = 0, patch_tests = 0, cell_tests = 0, tri_tests = 0, newton_iters = 0;
+    long long off_patch = 0;   // learned form: Newton roots outside their patch taken as misses
 };
 
 // Per-ray data of the FP32 cull test (computed once per query).
@@ -212,7 +213,9 @@ __device__ __forceinline__ int object_intersect(const DScene& S, int obj, const 
 
 // BVH::intersect with a 64-entry stack.  Returns the closest hit (obj >= 0),
 // a miss (obj < 0, err 0), or the first Newton failure met (err != 0).
-__device__ QHit bvh_query(const DScene& S, const V3& o, const V3& d, int cull_flag, Counters& ctr) {
+// off_patch_miss (learned form): a Newton root outside its patch is a miss.
+__device__ QHit bvh_query(const DScene& S, const V3& o, const V3& d, int cull_flag, Counters& ctr,
+                          bool off_patch_miss = false) {
     QHit best;
     best.obj = -1;
     best.err = 0;
@@ -237,6 +240,10 @@ __device__ QHit bvh_query(const DScene& S, const V3& o, const V3& d, int cull_fl
                 const int obj = S.leaf_objects[start + k];
                 QHit h;
                 const int r = object_intersect(S, obj, o, d, use_cull, cr, h, ctr);
+                if (off_patch_miss && h.err == BBRT_RAY_NEWTON_DOMAIN) {
+                    ++ctr.off_patch;
+                    continue;
+                }
                 if (h.err) {
                     h.obj = obj;
                     return h;
@@ -358,7 +365,7 @@ __device__ __forceinline__ void run_ray(const DScene& S, const TraceArgs& A, lon
     while (r.status < 0) {
         if (r.bounces >= A.max_bounces) { r.status = BBRT_RAY_MAX_BOUNCES; break; }
         ++queries;
-        const QHit h = bvh_query(S, r.o, r.d, A.cull, ctr);
+        const QHit h = bvh_query(S, r.o, r.d, A.cull, ctr, A.off_patch_miss != 0);
         if (!step_ray(S, A, i, r, h)) break;
     }
 }
@@ -399,6 +406,7 @@ __device__ __forceinline__ void flush_stats(const TraceArgs& A, const Counters& 
     warp_add(A.stats + ST_CELL_TESTS, ctr.cell_tests);
     warp_add(A.stats + ST_TRI_TESTS, ctr.tri_tests);
     warp_add(A.stats + ST_NEWTON_ITERS, ctr.newton_iters);
+    warp_add(A.stats + ST_OFF_PATCH, ctr.off_patch);
 #pragma unroll
     for (int k = 0; k < BBRT_RAY_STATUS_COUNT; ++k) warp_add(A.stats + ST_HIST0 + k, t.hist[k]);
 }
@@ -421,7 +429,7 @@ __global__ void __launch_bounds__(128) k_trace(DScene S, TraceArgs A) {
             run_ray(S, A, i, r, c1, tally.queries);
             add_ray_work(A, i, c1);
             ctr.node_tests += c1.node_tests; ctr.patch_tests += c1.patch_tests; ctr.cell_tests += c1.cell_tests;
-            ctr.tri_tests += c1.tri_tests; ctr.newton_iters += c1.newton_iters;
+            ctr.tri_tests += c1.tri_tests; ctr.newton_iters += c1.newton_iters; ctr.off_patch += c1.off_patch;
             finish_ray(A, i, r);
             tally.bounces += r.bounces;
             tally.hist[r.status]++;
@@ -778,7 +786,6 @@ __device__ __forceinline__ bool resume_query(const DScene& S, const TraceArgs& A
 // Advances runnable rays until each needs a Newton solve, overflows its
 // resolved list, or finishes.  Persistent: lanes fetch rays from the
 // runnable set until it is drained.
-constexpr long long kAdvanceWatchdog = 1LL << 35;   // SM cycles
 
 // NT threads per block, MINB blocks per SM requested from the register
 // allocator (launch shape variants of the same body); CHILD: a node's
@@ -810,12 +817,15 @@ __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, Wav
     // Runnable rays of this round: the host's count, or (graph-launched
     // trace) the count the previous round's control kernel left on the device.
     const long long n_run = W.count_dev ? static_cast<long long>(*W.count_dev) : W.n_runnable;
-    // Watchdog: a launch that runs far past any real trace (about 17 s of SM
-    // clock) records an error and ends instead of holding the GPU.
+    // Watchdog: a launch that runs far past any real trace (W.watchdog_cycles
+    // of SM clock, about 17 s by default) records an error and ends instead
+    // of holding the GPU; checked on the first iteration and every 1024th
+    // after it.  Both exits of the loop are warp-uniform (this vote and the
+    // drained vote at the end of the body).
     const long long t_start = clock64();
     unsigned int iter = 0;
     while (true) {
-        if ((++iter & 1023u) == 0u && __any_sync(0xffffffffu, clock64() - t_start > kAdvanceWatchdog)) {
+        if ((++iter & 1023u) == 1u && __any_sync(0xffffffffu, clock64() - t_start > W.watchdog_cycles)) {
             if ((threadIdx.x & 31) == 0) atomicOr(&W.counters[3], 1u);
             break;
         }
@@ -1202,7 +1212,7 @@ __global__ void __launch_bounds__(128) k_newton(DScene S, TraceArgs A, WaveArgs 
     if (W.count_dev) n_req = *W.count_dev;
     if (blockIdx.x * static_cast<long long>(blockDim.x) >= n_req) return;   // graph launch: spare blocks
     const long long j = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
-    long long iters = 0, iters32 = 0, used = 0, fallback = 0;
+    long long iters = 0, iters32 = 0, used = 0, fallback = 0, off = 0;
     if (j < n_req) {
         const NewtonRequest q = W.req[j];
         if (W.next_req) W.next_req[j] = q;
@@ -1241,7 +1251,15 @@ __global__ void __launch_bounds__(128) k_newton(DScene S, TraceArgs A, WaveArgs 
             key_to_uv(S, q.key, u0, v0);
             newton_mode(S, pidx, o, d, u0, v0, q.t0, h, iters, iters32);
         }
+        if (A.off_patch_miss && h.err == BBRT_RAY_NEWTON_DOMAIN &&
+            !guess_inside(W.guess ? W.guess + 4 * j : nullptr, W.guess_min_logit)) {
+            off = 1;   // not hit: resolved with t = +inf
+            h.err = 0;
+            h.t = CUDART_INF;
+        }
         if (A.samples && h.err == 0) record_sample(A, 1, o, d, pidx, h.u, h.v, h.t);
+        // a root outside the patch teaches the network a miss near the edge
+        if (A.samples && h.err == BBRT_RAY_NEWTON_DOMAIN) record_sample(A, 0, o, d, pidx, 0.0, 0.0, 0.0);
         const long long e = static_cast<long long>(q.ray) * kResolved + q.entry;
         double* rd = W.res_data + e * kResData;
         rd[0] = h.t; rd[1] = h.p.x; rd[2] = h.p.y; rd[3] = h.p.z;
@@ -1254,6 +1272,7 @@ __global__ void __launch_bounds__(128) k_newton(DScene S, TraceArgs A, WaveArgs 
         warp_add(A.stats + ST_NEWTON_ITERS_FP32, iters32);
         warp_add(A.stats + ST_GUESS_USED, used);
         warp_add(A.stats + ST_GUESS_FALLBACK, fallback);
+        warp_add(A.stats + ST_OFF_PATCH, off);
     }
 }
 
@@ -1264,7 +1283,7 @@ __global__ void __launch_bounds__(128) k_newton_grp(DScene S, TraceArgs A, WaveA
     if (blockIdx.x * static_cast<long long>(blockDim.x) / kGroup >= n_req) return;   // graph launch: spare blocks
     const Grp G = make_grp();
     const long long j = (blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x) / kGroup;
-    long long iters = 0, iters32 = 0, used = 0, fallback = 0;
+    long long iters = 0, iters32 = 0, used = 0, fallback = 0, off = 0;
     if (j < n_req) {   // uniform over the group
         const NewtonRequest q = W.req[j];
         if (W.next_req && G.g == 0) W.next_req[j] = q;
@@ -1298,8 +1317,15 @@ __global__ void __launch_bounds__(128) k_newton_grp(DScene S, TraceArgs A, WaveA
             key_to_uv(S, q.key, u0, v0);
             grp_newton_mode(S, pidx, o, d, u0, v0, q.t0, h, iters, iters32, G);
         }
+        if (A.off_patch_miss && h.err == BBRT_RAY_NEWTON_DOMAIN &&
+            !guess_inside(W.guess ? W.guess + 4 * j : nullptr, W.guess_min_logit)) {
+            off = 1;
+            h.err = 0;
+            h.t = CUDART_INF;
+        }
         if (G.g == 0) {
             if (A.samples && h.err == 0) record_sample(A, 1, o, d, pidx, h.u, h.v, h.t);
+            if (A.samples && h.err == BBRT_RAY_NEWTON_DOMAIN) record_sample(A, 0, o, d, pidx, 0.0, 0.0, 0.0);
             const long long e = static_cast<long long>(q.ray) * kResolved + q.entry;
             double* rd = W.res_data + e * kResData;
             rd[0] = h.t; rd[1] = h.p.x; rd[2] = h.p.y; rd[3] = h.p.z;
@@ -1308,12 +1334,13 @@ __global__ void __launch_bounds__(128) k_newton_grp(DScene S, TraceArgs A, WaveA
             if (A.ray_work) A.ray_work[4LL * q.ray + 3] += iters + iters32;
         }
     }
-    if (G.g != 0) iters = iters32 = used = fallback = 0;
+    if (G.g != 0) iters = iters32 = used = fallback = off = 0;
     if (A.stats) {
         warp_add(A.stats + ST_NEWTON_ITERS, iters);
         warp_add(A.stats + ST_NEWTON_ITERS_FP32, iters32);
         warp_add(A.stats + ST_GUESS_USED, used);
         warp_add(A.stats + ST_GUESS_FALLBACK, fallback);
+        warp_add(A.stats + ST_OFF_PATCH, off);
     }
 }
 
@@ -1355,7 +1382,7 @@ __global__ void __launch_bounds__(128) k_resume(DScene S, TraceArgs A, WaveArgs 
 // BVH::intersect for one ray with a whole warp (every lane returns the same result).
 // Nodes [0, staged) are read from the shared-memory copy (sbox, slink).
 __device__ QHit warp_bvh_query(const DScene& S, const V3& o, const V3& d, int cull_flag, int lane, Counters& ctr,
-                               const double* sbox, const int* slink, int staged) {
+                               const double* sbox, const int* slink, int staged, bool off_patch_miss) {
     QHit best;
     best.obj = -1;
     best.err = 0;
@@ -1401,6 +1428,10 @@ __device__ QHit warp_bvh_query(const DScene& S, const V3& o, const V3& d, int cu
                 } else {
                     Counters dummy;
                     r = triangle_intersect(S, S.obj_sub[obj], o, d, h, dummy);
+                }
+                if (off_patch_miss && h.err == BBRT_RAY_NEWTON_DOMAIN) {
+                    if (lane == 0) ++ctr.off_patch;
+                    continue;
                 }
                 if (h.err) {
                     h.obj = obj;
@@ -1462,7 +1493,8 @@ __global__ void __launch_bounds__(128, MINB) k_resume_warp(DScene S, TraceArgs A
         while (r.status < 0) {
             if (r.bounces >= A.max_bounces) { r.status = BBRT_RAY_MAX_BOUNCES; break; }
             if (lane == 0) ++tally.queries;
-            const QHit h = warp_bvh_query(S, r.o, r.d, A.cull, lane, c1, sbox, slink, S.smem_nodes);
+            const QHit h = warp_bvh_query(S, r.o, r.d, A.cull, lane, c1, sbox, slink, S.smem_nodes,
+                                          A.off_patch_miss != 0);
             if (!step_ray(S, A, i, r, h, lane == 0)) break;
         }
         if (lane == 0) {
@@ -1476,6 +1508,7 @@ __global__ void __launch_bounds__(128, MINB) k_resume_warp(DScene S, TraceArgs A
         ctr.cell_tests += c1.cell_tests;
         ctr.tri_tests += c1.tri_tests;
         ctr.newton_iters += c1.newton_iters;
+        ctr.off_patch += c1.off_patch;
     }
     flush_stats(A, ctr, tally, true);
 }
@@ -1563,6 +1596,7 @@ cudaError_t launch_trace(const DScene& S, const TraceArgs& A, cudaStream_t strea
 // use the array's name as a device address; noalloc_scratch() returns the
 // address the device sees.
 constexpr int kNoAllocHeader = 32;
+static_assert(1 + ST_COUNT <= kNoAllocHeader, "the statistics block would overlap the per-object hit counters");
 static __device__ __align__(256) unsigned long long g_noalloc_scratch[kNoAllocHeader + BBRT_NOALLOC_MAX_OBJECTS];
 
 // Device address of g_noalloc_scratch on the current device, looked up with
@@ -1584,6 +1618,19 @@ cudaError_t noalloc_scratch(unsigned long long** out) {
     }
     *out = static_cast<unsigned long long*>(addr[dev]);
     return cudaSuccess;
+}
+
+// Loads, on the current device, everything bbrt_trace_noalloc needs from this
+// module: the scratch array's address and the fused trace kernel.  Under lazy
+// module loading the first use of either would otherwise load the module
+// (which allocates device memory, the array included) inside the first
+// allocation-free call; bbrt_scene_upload calls this instead.
+cudaError_t noalloc_prepare() {
+    unsigned long long* p = nullptr;
+    cudaError_t e = noalloc_scratch(&p);
+    if (e != cudaSuccess) return e;
+    cudaFuncAttributes fa;
+    return cudaFuncGetAttributes(&fa, k_trace);
 }
 
 // The fused trace kernel with its scratch in g_noalloc_scratch.  Clears the

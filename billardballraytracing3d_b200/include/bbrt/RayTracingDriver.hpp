@@ -7,15 +7,19 @@
 // trace_ray/self_intersect_epsilon/write_vtk and exception texts.  The
 // trace itself runs on the GPU: run() traces all configured rays in batched
 // bbrt_trace calls (one per chunk of rays) and rebuilds every RayPath from
-// the recorded hits; trace_ray() is the one-ray form.  trace_rays() is the
+// the recorded hits; trace_ray() is the one-ray form (concurrent calls from
+// several threads are traced together as one batch).  trace_rays() is the
 // batch form for callers with their own rays.
 #pragma once
 
 #include <algorithm>
 #include <cmath>
+#include <condition_variable>
+#include <exception>
 #include <filesystem>
 #include <fstream>
 #include <memory>
+#include <mutex>
 #include <optional>
 #include <stdexcept>
 #include <string>
@@ -96,8 +100,62 @@ public:
     }
 
     // RayTracingDriver::trace_ray (RayTracingDriver.hpp:172-242) for one ray.
+    //
+    // The reference's drivers call this from many OpenMP threads at once
+    // (PlaneSourceDriver.hpp:96-99, BounceMapDriver.hpp:153-237); one GPU
+    // launch per ray would serialise them.  Concurrent calls are therefore
+    // combined: a caller queues its ray, and whichever caller finds no batch
+    // in flight takes every queued ray with the same max_bounces and traces
+    // them as one batch while the others wait (and queue the next batch).  A
+    // single-threaded caller still gets one launch per ray: loops that own
+    // their rays should call trace_rays() or run().  The result of every ray
+    // is the one trace_rays() gives it; an exception is rethrown in every
+    // caller of the failed batch.
     RayPath trace_ray(const Vec3& origin, const Vec3& direction, int max_bounces) const {
-        return trace_rays({ origin }, { direction }, max_bounces).front();
+        Combiner::Slot slot;
+        slot.origin = origin;
+        slot.direction = direction;
+        slot.max_bounces = max_bounces;
+        std::unique_lock<std::mutex> lk(comb_.mu);
+        comb_.queue.push_back(&slot);
+        while (!slot.done) {
+            if (comb_.busy) {
+                comb_.cv.wait(lk);
+                continue;
+            }
+            comb_.busy = true;
+            std::vector<Combiner::Slot*> batch;
+            std::vector<Combiner::Slot*> rest;
+            const int mb = comb_.queue.front()->max_bounces;
+            for (Combiner::Slot* q : comb_.queue) (q->max_bounces == mb ? batch : rest).push_back(q);
+            comb_.queue.swap(rest);
+            lk.unlock();
+            std::vector<Vec3> os, ds;
+            os.reserve(batch.size());
+            ds.reserve(batch.size());
+            for (const Combiner::Slot* q : batch) {
+                os.push_back(q->origin);
+                ds.push_back(q->direction);
+            }
+            std::vector<RayPath> res;
+            std::exception_ptr err;
+            try {
+                res = trace_rays(os, ds, mb);
+            } catch (...) {
+                err = std::current_exception();
+            }
+            lk.lock();
+            for (size_t k = 0; k < batch.size(); ++k) {
+                if (err) batch[k]->error = err;
+                else batch[k]->path = std::move(res[k]);
+                batch[k]->done = true;
+            }
+            comb_.busy = false;
+            comb_.cv.notify_all();
+        }
+        lk.unlock();
+        if (slot.error) std::rethrow_exception(slot.error);
+        return std::move(slot.path);
     }
 
     // trace_ray for every (origins[i], directions[i]), on the GPU in chunks.
@@ -160,6 +218,22 @@ private:
     std::vector<Vec3> sources_, directions_;
     std::vector<RayPath> paths_;
     std::unordered_map<const ScatObject*, size_t> index_of_;
+
+    // Rays of concurrent trace_ray() calls waiting to be traced together.
+    struct Combiner {
+        struct Slot {
+            Vec3 origin, direction;
+            int max_bounces = 0;
+            bool done = false;
+            RayPath path;
+            std::exception_ptr error;
+        };
+        std::mutex mu;
+        std::condition_variable cv;
+        std::vector<Slot*> queue;
+        bool busy = false;   // a batch is being traced
+    };
+    mutable Combiner comb_;
 
     static constexpr double kSelfIntersectEpsilonFactor = 1e-9;   // RayTracingDriver.hpp:328
     static constexpr double kSagittaClearanceFactor = 5.0;        // RayTracingDriver.hpp:337

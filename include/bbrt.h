@@ -75,7 +75,12 @@ enum {
 };
 enum {
     BBRT_GUESS_TRIANGLE = 0,  /* Newton starts from the stage-1 triangle (the reference) */
-    BBRT_GUESS_LEARNED = 1    /* Newton starts from the MLP guess; triangle on fallback   */
+    BBRT_GUESS_LEARNED = 1    /* Newton starts from the MLP guess; triangle on fallback.
+                                 A patch whose Newton root lies outside the patch is taken
+                                 as not hit (the ray goes on) instead of failing the ray,
+                                 unless the network places a confident hit well inside the
+                                 patch; the reference fails the ray there
+                                 (SurfacePatch.hpp:639-646)                              */
 };
 
 /* Trace-time and scene-build constants.  bbrt_config_init() fills the
@@ -210,6 +215,8 @@ typedef struct bbrt_trace_stats {
     long long guess_used;     /* Newton solves started from the learned guess */
     long long guess_fallback; /* ... of which restarted from the stage-1 triangle */
     double guess_ms;          /* learned-guess inference kernels */
+    long long off_patch;      /* learned form: patch queries whose Newton root lay outside the patch,
+                                 taken as "not hit" instead of a Newton failure of the ray */
 } bbrt_trace_stats;
 
 /* ---- library ---------------------------------------------------------- */
@@ -402,6 +409,16 @@ typedef struct bbrt_tuning {
     int graph_rounds;         /* 1 (default): the whole wavefront trace is one CUDA graph launch whose
                                  round loop is a device-side conditional node (no host wait per round;
                                  one graph per argument set, kept for reuse); 0: rounds driven by the host */
+    long long watchdog_cycles;  /* a k_advance launch that runs longer than this many SM clock cycles
+                                   stops, and the call returns BBRT_ERR_KERNEL ("watchdog") instead of
+                                   holding the GPU; 0 = the default, 2^35 (about 17 s at 1.97 GHz; a
+                                   round takes milliseconds).  Checked on a warp's first loop
+                                   iteration and every 1024th after it. */
+    long long mma_wait_cycles;  /* a tensor-core completion wait of the learned-guess kernels gives up
+                                   after this many SM clock cycles (it then waits once more, with the
+                                   default bound, for the MMAs in flight, frees its tensor memory and
+                                   leaves) and the call returns BBRT_ERR_KERNEL; 0 = the default,
+                                   4e9 (about 2 s) */
 } bbrt_tuning;
 
 BBRT_API int bbrt_scene_get_tuning(bbrt_scene_t scene, bbrt_tuning* out);
@@ -461,9 +478,11 @@ BBRT_API int bbrt_umma_check(const unsigned short* a, const unsigned short* b, f
  *
  * Every call shares the one array per device and clears what it uses at its
  * start, so calls whose work overlaps on the GPU (different streams or host
- * threads) race and give wrong results: serialise them.  The first call on
- * each device looks up the array's device address (cudaGetSymbolAddress);
- * make that first call before any stream capture. */
+ * threads) race and give wrong results: serialise them.  Putting the scene
+ * on the device (bbrt_scene_upload) also loads, on that device, the module
+ * holding the array and the kernel and looks up the array's device address
+ * (cudaGetSymbolAddress), so that no allocation-free call loads a module;
+ * upload before any stream capture. */
 #define BBRT_NOALLOC_MAX_OBJECTS 32768
 BBRT_API int bbrt_trace_noalloc(bbrt_scene_t scene, const double* origins, const double* dirs, long long n,
                                 int max_bounces, const bbrt_trace_out* out, long long* hit_counts,

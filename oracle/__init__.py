@@ -32,11 +32,23 @@ REF_TRI_BIN = os.path.join(HERE, "_ref", "triangle_intersect")
 P = lambda a: None if a is None else a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
 
 
-def build(reference_root: str = "/root/reference") -> None:
+def reference_root() -> str:
+    """Where the reference project's sources are looked for: the environment
+    variable BBRT_REFERENCE_ROOT, else a directory named `reference` beside
+    this repository's root.  Neither exists on a machine that only runs the
+    prebuilt oracle libraries."""
+    env = os.environ.get("BBRT_REFERENCE_ROOT")
+    if env:
+        return env
+    return os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")
+
+
+def build(reference_root_dir: str | None = None) -> None:
     """Compile the oracle port, and the reference oracle when its sources exist."""
     subprocess.run(["bash", os.path.join(HERE, "build_oracle.sh")], check=True)
-    if os.path.isdir(os.path.join(reference_root, "include")):
-        subprocess.run(["bash", os.path.join(HERE, "build_ref.sh"), reference_root], check=True)
+    reference_root_dir = reference_root_dir or reference_root()
+    if os.path.isdir(os.path.join(reference_root_dir, "include")):
+        subprocess.run(["bash", os.path.join(HERE, "build_ref.sh"), reference_root_dir], check=True)
 
 
 def reference_available() -> bool:

@@ -12,10 +12,12 @@
 # into `static inline` members in a throw-away copy of the headers made under
 # oracle/_ref/src, which is deleted again once the library is built.
 #
-# Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
+# Usage: oracle/build_ref.sh [REFERENCE_ROOT]
+#   REFERENCE_ROOT defaults to $BBRT_REFERENCE_ROOT, else to a directory named
+#   `reference` beside this repository's root.
 set -euo pipefail
 here="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-ref="${1:-/root/reference}"
+ref="${1:-${BBRT_REFERENCE_ROOT:-$(dirname "$(dirname "$here")")/reference}}"
 out="$here/_ref"
 if [ ! -d "$ref/include" ]; then
     echo "build_ref: no reference at $ref; nothing built" >&2

@@ -9,7 +9,7 @@
  * row-major only.  Summation order is fixed: for each C[i][j] the K products
  * are accumulated left to right into a zero-initialised double, then scaled by
  * alpha (and beta * C added when beta != 0).  The product's host scene
- * compiler (billardballraytracing3d_b200/csrc/scene_compile.cpp) uses exactly
+ * compiler (billardballraytracing3d_b200/csrc/scene_host.cpp) uses exactly
  * this order, so both see bit-identical coarse grids.  MKL's own blocking may
  * differ from this in the last ulp; no reference test pins that boundary.
  */

@@ -8,12 +8,14 @@
 //   drivers bmap  <patch_dir> <file_prefix> <first> <last> grid theta phi cone max_bounces <out_prefix>
 //
 // rays.bin: int64 n, then n origins (3 doubles each), then n directions.
+#include <atomic>
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
 #include <iomanip>
 #include <iostream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "BounceMapDriver.hpp"
@@ -59,6 +61,21 @@ int run_trace(char** a) {
     std::vector<RayTracingDriver::RayPath> one;
     for (long long i = 0; i < m; ++i) one.push_back(drv.trace_ray(src[i], dir[i], std::atoi(a[2])));
     dump_paths(drv, one, prefix + "paths_one.txt");
+    // Many threads calling trace_ray at once (the reference's OpenMP loop,
+    // PlaneSourceDriver.hpp:96-99): their rays are combined into batches,
+    // and every ray still gets its own path.
+    {
+        std::vector<RayTracingDriver::RayPath> par(static_cast<size_t>(n));
+        const int maxb = std::atoi(a[2]);
+        std::vector<std::thread> pool;
+        std::atomic<long long> next{ 0 };
+        for (int t = 0; t < 8; ++t)
+            pool.emplace_back([&] {
+                for (long long i = next++; i < n; i = next++) par[static_cast<size_t>(i)] = drv.trace_ray(src[i], dir[i], maxb);
+            });
+        for (auto& th : pool) th.join();
+        dump_paths(drv, par, prefix + "paths_threads.txt");
+    }
     std::ofstream info(prefix + "info.txt");
     info << std::setprecision(17) << drv.patches().size() << ' ' << drv.self_intersect_epsilon() << ' '
          << drv.self_intersect_epsilon(drv.patches().front().get()) << '\n';

@@ -42,7 +42,9 @@ def write_driver_scene(directory: str, n_samples: int = 2):
     return patches
 
 
-def main(ref_root: str = "/root/reference") -> None:
+def main(ref_root: str | None = None) -> None:
+    import oracle
+    ref_root = ref_root or oracle.reference_root()
     tmp = tempfile.mkdtemp(prefix="driver_errors_")
     try:
         exe = os.path.join(tmp, "driver_errors")

@@ -33,7 +33,7 @@ def compile_program(name, out_dir):
     cmd = ["g++", "-O1", "-std=c++17", "-Wall", "-Wextra", "-Werror",
            "-I", os.path.join(ROOT, "include"), "-I", os.path.join(PKG, "include", "bbrt"),
            os.path.join(ROOT, "tests", "cpp", name + ".cpp"), "-o", exe,
-           "-L", PKG, "-lbbrt_cuda", "-Wl,-rpath," + PKG]
+           "-L", PKG, "-lbbrt_cuda", "-Wl,-rpath," + PKG, "-pthread"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     assert r.returncode == 0, r.stderr[-4000:]
     return exe
@@ -187,6 +187,7 @@ def test_cpp_ray_tracing_driver(programs, driver_scene, tmp_path):
     got = parse_paths(prefix + "paths.txt")
     assert_same_paths(got, want)
     assert_same_paths(parse_paths(prefix + "paths_one.txt"), want[:8])
+    assert_same_paths(parse_paths(prefix + "paths_threads.txt"), want)
     assert {p["status"] for p in got} == {0, 2}   # escaped, and back-face errors
     assert max(p["bounces"] for p in got) >= 2
     with open(prefix + "traces.vtk") as f:

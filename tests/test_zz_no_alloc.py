@@ -11,7 +11,8 @@ Checked here, through the C ABI: two calls in a row give exactly the outputs
 of the allocating entry points (bbrt_trace on device pointers for the per-ray
 results, bbrt_plane_source for the hit counts), so the second call is not
 polluted by the first one's scratch; free device memory does not change
-across the calls; and the documented limits are enforced.  This file is
+across the two calls, which run right after the scene's upload and before
+any allocating trace; and the documented limits are enforced.  This file is
 collected last so that a stopping run has already run every other test.
 """
 import ctypes
@@ -58,7 +59,34 @@ def test_noalloc_trace_matches_allocating_entry_points(built):
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
 
-    # the allocating entry points (they also put the scene on the device)
+    lib.bbrt_trace_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_longlong,
+                                       ctypes.c_int, ctypes.POINTER(C.TraceOut), ctypes.c_void_p, ctypes.c_int,
+                                       ctypes.POINTER(C.TraceStats), ctypes.c_void_p]
+    counts = torch.full((sc.n_objects,), -1, dtype=torch.int64, device="cuda")
+    bufs, out = _device_outputs(torch, n, K)
+    # the scene goes to the device first (the one step that allocates); from
+    # here on, in a fresh process too, the allocation-free calls must leave
+    # free device memory unchanged, the first one included
+    sc.upload()
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
+    got_calls = []
+    for call in range(2):
+        for b in bufs.values():
+            b.fill_(-7)
+        counts.fill_(-1)
+        torch.cuda.synchronize()
+        st = C.TraceStats()
+        C.check(lib, lib.bbrt_trace_noalloc(sc.h, ctypes.c_void_p(to.data_ptr()), ctypes.c_void_p(td.data_ptr()), n,
+                                            20, ctypes.byref(out), ctypes.c_void_p(counts.data_ptr()), 1,
+                                            ctypes.byref(st), ctypes.c_void_p(stream.cuda_stream)),
+                "bbrt_trace_noalloc")
+        torch.cuda.synchronize()
+        got_calls.append(({k: v.cpu().numpy() for k, v in bufs.items()}, counts.cpu().numpy(),
+                          (st.rays, st.bounces, sum(st.status_hist))))
+    assert torch.cuda.mem_get_info()[0] == free_before
+
+    # the allocating entry points on the same rays
     ref_bufs, ref_out = _device_outputs(torch, n, K)
     C.check(lib, lib.bbrt_trace(sc.h, ctypes.c_void_p(to.data_ptr()), ctypes.c_void_p(td.data_ptr()), n, 20,
                                 C.DEVICE_PTRS, ctypes.byref(ref_out), None, ctypes.c_void_p(stream.cuda_stream)),
@@ -66,34 +94,13 @@ def test_noalloc_trace_matches_allocating_entry_points(built):
     ref_counts = sc.plane_source(c0, c1, dd, 64, 48, 20, count_direct_hit=False)
     torch.cuda.synchronize()
     ref = {k: v.cpu().numpy() for k, v in ref_bufs.items()}
-
-    lib.bbrt_trace_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_longlong,
-                                       ctypes.c_int, ctypes.POINTER(C.TraceOut), ctypes.c_void_p, ctypes.c_int,
-                                       ctypes.POINTER(C.TraceStats), ctypes.c_void_p]
-    counts = torch.full((sc.n_objects,), -1, dtype=torch.int64, device="cuda")
-    bufs, out = _device_outputs(torch, n, K)
-    free_before = None
-    for call in range(2):
-        for b in bufs.values():
-            b.fill_(-7)
-        counts.fill_(-1)
-        torch.cuda.synchronize()
-        if call == 1:
-            free_before = torch.cuda.mem_get_info()[0]
-        st = C.TraceStats()
-        C.check(lib, lib.bbrt_trace_noalloc(sc.h, ctypes.c_void_p(to.data_ptr()), ctypes.c_void_p(td.data_ptr()), n,
-                                            20, ctypes.byref(out), ctypes.c_void_p(counts.data_ptr()), 1,
-                                            ctypes.byref(st), ctypes.c_void_p(stream.cuda_stream)),
-                "bbrt_trace_noalloc")
-        torch.cuda.synchronize()
-        got = {k: v.cpu().numpy() for k, v in bufs.items()}
+    for call, (got, cnt, (rays, bounces, hist_total)) in enumerate(got_calls):
         for k in got:
             assert np.array_equal(got[k], ref[k]), (call, k)
-        assert np.array_equal(counts.cpu().numpy(), ref_counts), call
-        assert st.rays == n
-        assert st.bounces == int(ref["bounce_count"].sum())
-        assert sum(st.status_hist) == n
-    assert torch.cuda.mem_get_info()[0] == free_before
+        assert np.array_equal(cnt, ref_counts), call
+        assert rays == n
+        assert bounces == int(ref["bounce_count"].sum())
+        assert hist_total == n
 
 
 def test_noalloc_limits(built):
