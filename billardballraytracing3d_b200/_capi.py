@@ -35,6 +35,7 @@ RAY_NEWTON_SINGULAR = 2
 RAY_NEWTON_NOCONV = 3
 RAY_NEWTON_DOMAIN = 4
 RAY_WENT_INSIDE = 5
+SETUP_COARSE, SETUP_CELLS, SETUP_CELL_BOXES, SETUP_BLOCK_BOXES, SETUP_CULL = 0, 1, 2, 3, 4
 RAY_BAD_DIR = 6
 RAY_STACK_OVERFLOW = 7
 RAY_STATUS_COUNT = 8
@@ -68,6 +69,7 @@ class Config(ctypes.Structure):
         ("precision", ctypes.c_int),
         ("guess", ctypes.c_int),
         ("cull", ctypes.c_int),
+        ("setup_on_device", ctypes.c_int),
     ]
 
 
@@ -76,7 +78,7 @@ def default_config(**kw) -> Config:
     BVH.hpp:67; RayTracingDriver.hpp:328,337,344), overridable by keyword."""
     c = Config(coarse_grid_n=100, newton_max_iters=20, newton_tol=1e-3, leaf_threshold=4,
                self_intersect_eps_factor=1e-9, sagitta_clearance_factor=5.0, backface_tol=1e-9,
-               precision=PREC_FP64, guess=GUESS_TRIANGLE, cull=1)
+               precision=PREC_FP64, guess=GUESS_TRIANGLE, cull=1, setup_on_device=-1)
     for k, v in kw.items():
         if not hasattr(c, k):
             raise KeyError(k)
@@ -118,7 +120,7 @@ class SceneInfo(ctypes.Structure):
     _fields_ = [
         ("n_objects", ctypes.c_int), ("n_nodes", ctypes.c_int), ("max_depth", ctypes.c_int),
         ("scene_diagonal", ctypes.c_double), ("max_patch_sagitta", ctypes.c_double),
-        ("device_bytes", ctypes.c_longlong),
+        ("device_bytes", ctypes.c_longlong), ("setup_on_device", ctypes.c_int),
     ]
 
 
@@ -279,6 +281,7 @@ def _declare(lib):
     lib.bbrt_scene_destroy.restype = None
     lib.bbrt_scene_upload.argtypes = [V]
     lib.bbrt_scene_info_get.argtypes = [V, ctypes.POINTER(SceneInfo)]
+    lib.bbrt_scene_setup_get.argtypes = [V, I, V, ctypes.POINTER(ctypes.c_longlong)]
     lib.bbrt_object_info_get.argtypes = [V, I, ctypes.POINTER(ObjectInfo)]
     lib.bbrt_patch_coarse_grid.argtypes = [V, I, c_int_p, c_double_p, c_double_p, c_double_p,
                                            c_double_p, c_double_p]

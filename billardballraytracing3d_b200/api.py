@@ -103,6 +103,21 @@ class Scene:
                 "bbrt_intersect")
         return out
 
+    def setup_arrays(self) -> Dict[str, np.ndarray]:
+        """The scene's whole set-up (bbrt_scene_setup_get): coarse grids, cell
+        normals / sagittas, cull cell and block boxes, cull constants."""
+        out = {}
+        for name, what, dt in (("coarse", C.SETUP_COARSE, np.float64), ("cells", C.SETUP_CELLS, np.float64),
+                               ("cell_boxes", C.SETUP_CELL_BOXES, np.float32),
+                               ("block_boxes", C.SETUP_BLOCK_BOXES, np.float32), ("cull", C.SETUP_CULL, np.float64)):
+            n = ctypes.c_longlong()
+            C.check(self.lib, self.lib.bbrt_scene_setup_get(self.h, what, None, ctypes.byref(n)), "bbrt_scene_setup_get")
+            a = np.zeros(n.value, dt)
+            C.check(self.lib, self.lib.bbrt_scene_setup_get(self.h, what, ctypes.c_void_p(a.ctypes.data), ctypes.byref(n)),
+                    "bbrt_scene_setup_get")
+            out[name] = a
+        return out
+
     def trace(self, origins, dirs, max_bounces: int, record: int = 8, want_stats: bool = True,
               outputs: Sequence[str] = ("status", "bounce_count", "exit_dir", "end_point", "hit_object",
                                         "hit_point", "hit_uv", "err_object", "err_value")) -> TraceResult:

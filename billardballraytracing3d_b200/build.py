@@ -27,6 +27,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # per-source extra flags
 CU_FLAGS = {
     "trace_kernels.cu": ["-fmad=false"],
+    "scene_compile.cu": ["-fmad=false"],
 }
 
 

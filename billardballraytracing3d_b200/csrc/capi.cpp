@@ -29,6 +29,7 @@
 #include "../../include/bbrt.h"
 #include "dscene.h"
 #include "guess.h"
+#include "scene_compile.h"
 #include "scene_host.hpp"
 
 namespace bbrt {
@@ -105,6 +106,9 @@ struct bbrt_scene {
     bbrt::CullTables cull;
     bbrt::DScene dev;
     bool uploaded = false;
+    bool device_ready = false;      // device, stream and events chosen
+    bool tables_uploaded = false;   // patch node / field tables on the device
+    bool setup_on_device = false;   // coarse grids, cells and cull boxes computed on (and kept only on) the GPU
     int device = 0;
     int sm_count = 148;
     cudaStream_t stream = nullptr;
@@ -173,6 +177,16 @@ struct bbrt_scene {
     }
 
     template <class T>
+    int alloc(size_t n, T*& dst) {
+        void* p = nullptr;
+        BBRT_CUDA(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)));
+        allocs.push_back(p);
+        device_bytes += static_cast<long long>(n * sizeof(T));
+        dst = static_cast<T*>(p);
+        return BBRT_OK;
+    }
+
+    template <class T>
     int upload(const std::vector<T>& v, const T*& dst) {
         if (v.empty()) { dst = nullptr; return BBRT_OK; }
         void* p = nullptr;
@@ -235,8 +249,9 @@ std::vector<double> patch_frames(const bbrt::HostScene& H) {
     return fr;
 }
 
-int ensure_uploaded(bbrt_scene* s) {
-    if (s->uploaded) return BBRT_OK;
+// Binds the scene to the current device: its stream and events.
+int ensure_device(bbrt_scene* s) {
+    if (s->device_ready) return BBRT_OK;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0)
         return fail(BBRT_ERR_CUDA, "bbrt: no CUDA device available (the trace path has no CPU fallback)");
@@ -248,9 +263,116 @@ int ensure_uploaded(bbrt_scene* s) {
     BBRT_CUDA(bbrt::noalloc_prepare());
     for (auto& e : s->ev) BBRT_CUDA(cudaEventCreate(&e));
     for (auto& e : s->kev) BBRT_CUDA(cudaEventCreate(&e));
+    s->device_ready = true;
+    return BBRT_OK;
+}
+
+// The patch tables every patch kernel reads (node counts, offsets, nodes and
+// weights, node-major fields) and the coarse (u, v) values.
+int upload_patch_tables(bbrt_scene* s) {
+    if (s->tables_uploaded) return BBRT_OK;
     const bbrt::HostScene& H = s->host;
     bbrt::DScene& D = s->dev;
-    D = bbrt::DScene();
+    std::vector<int> dims(2 * static_cast<size_t>(H.n_patches));
+    for (int q = 0; q < H.n_patches; ++q) {
+        dims[2 * q] = H.p_imax[q];
+        dims[2 * q + 1] = H.p_jmax[q];
+    }
+    int rc;
+    if ((rc = s->upload(dims, D.p_dims))) return rc;
+    if ((rc = s->upload(H.p_node_off, D.p_node_off))) return rc;
+    if ((rc = s->upload(H.p_field_off, D.p_field_off))) return rc;
+    if ((rc = s->upload(H.p_nodes, D.p_nodes))) return rc;
+    if ((rc = s->upload(H.p_fields, D.p_fields))) return rc;
+    if ((rc = s->upload(H.coarse_uv, D.coarse_uv))) return rc;
+    s->tables_uploaded = true;
+    return BBRT_OK;
+}
+
+// The per-patch set-up of scene creation on the GPU (scene_compile.cu): the
+// coarse grids, cell data and cull boxes stay in device memory; boxes,
+// centroids and paddings come back for the host's BVH build, and the
+// per-patch edge / coordinate bounds for the cull constants.
+int device_setup(bbrt_scene* s) {
+    int rc;
+    if ((rc = ensure_device(s))) return rc;
+    if ((rc = upload_patch_tables(s))) return rc;
+    bbrt::HostScene& H = s->host;
+    bbrt::DScene& D = s->dev;
+    const int cn = H.coarse_n, nc = cn - 1, P = H.n_patches;
+    bbrt::SetupArgs A;
+    A.n_patches = P;
+    A.cn = cn;
+    A.coarse_uv = D.coarse_uv;
+    A.dims = D.p_dims;
+    A.node_off = D.p_node_off;
+    A.field_off = D.p_field_off;
+    A.nodes = D.p_nodes;
+    A.fields = D.p_fields;
+    const size_t per_xyz = 3 * static_cast<size_t>(cn) * cn, per_cell = 4 * static_cast<size_t>(nc) * nc;
+    double *cx = nullptr, *cc = nullptr;
+    if ((rc = s->alloc(per_xyz * P, cx))) return rc;
+    if ((rc = s->alloc(per_cell * P, cc))) return rc;
+    A.c_xyz = cx;
+    A.c_cell = cc;
+    DevBuf out, stats;
+    BBRT_CUDA(out.ensure(sizeof(double) * 10 * std::max(P, 1)));
+    A.patch_out = static_cast<double*>(out.p);
+    const bool cull = H.cfg.cull && P > 0;
+    int B = 4, NB = 0;
+    if (cull) {
+        B = std::max(4, static_cast<int>(std::ceil(std::sqrt(static_cast<double>(nc)))));
+        NB = (nc + B - 1) / B;
+        float *cb = nullptr, *bb = nullptr;
+        if ((rc = s->alloc(static_cast<size_t>(P) * nc * nc * 6, cb))) return rc;
+        if ((rc = s->alloc(static_cast<size_t>(P) * NB * NB * 6, bb))) return rc;
+        A.cell_box = cb;
+        A.block_box = bb;
+        A.block_cells = B;
+        A.n_blocks_side = NB;
+        BBRT_CUDA(stats.ensure(sizeof(double) * 3 * P));
+        A.cull_stats = static_cast<double*>(stats.p);
+    }
+    BBRT_CUDA(bbrt::launch_patch_setup(A, s->sm_count, s->stream));
+    std::vector<double> po(10 * static_cast<size_t>(P)), cs(cull ? 3 * static_cast<size_t>(P) : 0);
+    if (P > 0) BBRT_CUDA(cudaMemcpyAsync(po.data(), out.p, sizeof(double) * po.size(), cudaMemcpyDeviceToHost, s->stream));
+    if (cull) BBRT_CUDA(cudaMemcpyAsync(cs.data(), stats.p, sizeof(double) * cs.size(), cudaMemcpyDeviceToHost, s->stream));
+    BBRT_CUDA(cudaStreamSynchronize(s->stream));
+    for (int q = 0; q < P; ++q) {
+        const int k = H.patch_obj[q];
+        std::memcpy(&H.box[6 * static_cast<size_t>(k)], &po[10 * static_cast<size_t>(q)], sizeof(double) * 6);
+        std::memcpy(&H.centroid[3 * static_cast<size_t>(k)], &po[10 * static_cast<size_t>(q) + 6], sizeof(double) * 3);
+        H.padding[k] = po[10 * static_cast<size_t>(q) + 9];
+    }
+    bbrt::finish_host_scene(H);
+    D.c_xyz = cx;
+    D.c_cell = cc;
+    s->cull = bbrt::CullTables();
+    if (cull) {
+        double hmax = 0.0, cmax = 0.0;
+        bool finite = true;
+        for (int q = 0; q < P; ++q) {
+            hmax = std::max(hmax, cs[3 * static_cast<size_t>(q)]);
+            cmax = std::max(cmax, cs[3 * static_cast<size_t>(q) + 1]);
+            finite = finite && cs[3 * static_cast<size_t>(q) + 2] != 0.0;
+        }
+        s->cull.block_cells = B;
+        s->cull.n_blocks_side = NB;
+        bbrt::cull_constants(H, hmax, cmax, finite, s->cull);
+        D.c_cell_box = A.cell_box;
+        D.c_block_box = A.block_box;
+    }
+    s->setup_on_device = true;
+    return BBRT_OK;
+}
+
+int ensure_uploaded(bbrt_scene* s) {
+    if (s->uploaded) return BBRT_OK;
+    int rc0 = ensure_device(s);
+    if (rc0) return rc0;
+    if ((rc0 = upload_patch_tables(s))) return rc0;
+    const bbrt::HostScene& H = s->host;
+    bbrt::DScene& D = s->dev;
     D.n_objects = H.n_objects;
     D.n_nodes = static_cast<int>(H.nodes.size());
     D.coarse_n = H.coarse_n;
@@ -299,12 +421,7 @@ int ensure_uploaded(bbrt_scene* s) {
     // up to 3400 nodes (64 bytes each, 217 KB) in shared memory; launch shapes
     // with several blocks per SM stage fewer
     D.smem_nodes = static_cast<int>(std::min<size_t>(nn, 3400));
-    std::vector<int> dims(2 * static_cast<size_t>(H.n_patches));
-    for (int q = 0; q < H.n_patches; ++q) {
-        dims[2 * q] = H.p_imax[q];
-        dims[2 * q + 1] = H.p_jmax[q];
-        D.max_nodes = std::max(D.max_nodes, std::max(H.p_imax[q], H.p_jmax[q]));
-    }
+    for (int q = 0; q < H.n_patches; ++q) D.max_nodes = std::max(D.max_nodes, std::max(H.p_imax[q], H.p_jmax[q]));
     int rc;
     if ((rc = s->upload(nbox, D.node_box))) return rc;
     if ((rc = s->upload(nlink, D.node_link))) return rc;
@@ -312,11 +429,6 @@ int ensure_uploaded(bbrt_scene* s) {
     if ((rc = s->upload(H.kind, D.obj_kind))) return rc;
     if ((rc = s->upload(H.sub, D.obj_sub))) return rc;
     if ((rc = s->upload(H.padding, D.obj_pad))) return rc;
-    if ((rc = s->upload(dims, D.p_dims))) return rc;
-    if ((rc = s->upload(H.p_node_off, D.p_node_off))) return rc;
-    if ((rc = s->upload(H.p_field_off, D.p_field_off))) return rc;
-    if ((rc = s->upload(H.p_nodes, D.p_nodes))) return rc;
-    if ((rc = s->upload(H.p_fields, D.p_fields))) return rc;
     {
         const std::vector<float> n32(H.p_nodes.begin(), H.p_nodes.end());
         const std::vector<float> f32(H.p_fields.begin(), H.p_fields.end());
@@ -331,13 +443,16 @@ int ensure_uploaded(bbrt_scene* s) {
         if ((rc = s->upload(fr, s->guess.frame))) return rc;
     }
     D.precision = H.cfg.precision;
-    if ((rc = s->upload(H.coarse_uv, D.coarse_uv))) return rc;
-    if ((rc = s->upload(H.c_xyz, D.c_xyz))) return rc;
-    if ((rc = s->upload(H.c_cell, D.c_cell))) return rc;
+    if (!s->setup_on_device) {
+        if ((rc = s->upload(H.c_xyz, D.c_xyz))) return rc;
+        if ((rc = s->upload(H.c_cell, D.c_cell))) return rc;
+    }
     if ((rc = s->upload(H.tri, D.tri))) return rc;
     if (s->cull.enabled) {
-        if ((rc = s->upload(s->cull.cell_box, D.c_cell_box))) return rc;
-        if ((rc = s->upload(s->cull.block_box, D.c_block_box))) return rc;
+        if (!s->setup_on_device) {
+            if ((rc = s->upload(s->cull.cell_box, D.c_cell_box))) return rc;
+            if ((rc = s->upload(s->cull.block_box, D.c_block_box))) return rc;
+        }
         D.block_cells = s->cull.block_cells;
         D.n_blocks_side = s->cull.n_blocks_side;
         D.cull_enabled = 1;
@@ -366,16 +481,37 @@ int create_scene(const bbrt_object_desc* objects, int n, const bbrt_config* cfg,
     bbrt_config c;
     bbrt_config_init(&c);
     if (cfg) c = *cfg;
+    if (c.setup_on_device < -1 || c.setup_on_device > 1)
+        return fail(BBRT_ERR_ARG, "bbrt_scene_create: setup_on_device must be -1, 0 or 1");
+    bool on_device = c.setup_on_device == 1;
+    if (c.setup_on_device == -1) {
+        int ndev = 0;
+        on_device = cudaGetDeviceCount(&ndev) == cudaSuccess && ndev > 0;
+    }
     std::unique_ptr<bbrt_scene> s(new bbrt_scene());
     try {
-        bbrt::build_host_scene(objects, n, c, s->host);
-        bbrt::build_cull_tables(s->host, s->cull);
+        bbrt::build_host_tables(objects, n, c, s->host);
+        if (s->host.n_patches == 0) on_device = false;   // triangles only: nothing to compile
+        if (!on_device) {
+            bbrt::setup_patches_host(objects, s->host);
+            bbrt::finish_host_scene(s->host);
+            bbrt::build_cull_tables(s->host, s->cull);
+        }
     } catch (const std::invalid_argument& e) {
         return fail(BBRT_ERR_ARG, e.what());
     } catch (const std::runtime_error& e) {
         return fail(BBRT_ERR_FORMAT, e.what());
     } catch (const std::bad_alloc&) {
         return fail(BBRT_ERR_NOMEM, "bbrt_scene_create: out of host memory");
+    }
+    if (on_device) {
+        int rc = BBRT_OK;
+        try {
+            rc = device_setup(s.get());
+        } catch (const std::bad_alloc&) {
+            return fail(BBRT_ERR_NOMEM, "bbrt_scene_create: out of host memory");
+        }
+        if (rc) return rc;
     }
     *out = s.release();
     return BBRT_OK;
@@ -1059,6 +1195,7 @@ BBRT_API void bbrt_config_init(bbrt_config* c) {
     c->precision = BBRT_PREC_FP64;
     c->guess = BBRT_GUESS_TRIANGLE;
     c->cull = 1;
+    c->setup_on_device = -1;
 }
 
 BBRT_API int bbrt_device_count(void) {
@@ -1145,6 +1282,7 @@ BBRT_API int bbrt_scene_info_get(bbrt_scene_t s, bbrt_scene_info* out) {
     out->scene_diagonal = s->host.scene_diagonal;
     out->max_patch_sagitta = s->host.max_patch_sagitta;
     out->device_bytes = s->device_bytes;
+    out->setup_on_device = s->setup_on_device ? 1 : 0;
     return BBRT_OK;
 }
 
@@ -1173,11 +1311,88 @@ BBRT_API int bbrt_patch_coarse_grid(bbrt_scene_t s, int k, int* n, double* u, do
     if (n) *n = cn;
     if (u) std::memcpy(u, H.coarse_uv.data(), sizeof(double) * cn);
     if (v) std::memcpy(v, H.coarse_uv.data(), sizeof(double) * cn);
-    if (xyz) std::memcpy(xyz, &H.c_xyz[3 * static_cast<size_t>(cn) * cn * q], sizeof(double) * 3 * cn * cn);
-    const double* cc = &H.c_cell[4 * static_cast<size_t>(nc) * nc * q];
-    for (int c = 0; c < nc * nc; ++c) {
+    const size_t per_xyz = 3 * static_cast<size_t>(cn) * cn, per_cell = 4 * static_cast<size_t>(nc) * nc;
+    std::vector<double> dev_cell;
+    const double* cc = nullptr;
+    if (s->setup_on_device) {
+        // the set-up lives on the GPU only
+        std::lock_guard<std::mutex> g(s->mu);
+        if (xyz) BBRT_CUDA(cudaMemcpy(xyz, s->dev.c_xyz + per_xyz * q, sizeof(double) * per_xyz, cudaMemcpyDeviceToHost));
+        if (sag || nrm) {
+            dev_cell.resize(per_cell);
+            BBRT_CUDA(cudaMemcpy(dev_cell.data(), s->dev.c_cell + per_cell * q, sizeof(double) * per_cell,
+                                 cudaMemcpyDeviceToHost));
+            cc = dev_cell.data();
+        }
+    } else {
+        if (xyz) std::memcpy(xyz, &H.c_xyz[per_xyz * q], sizeof(double) * per_xyz);
+        cc = &H.c_cell[per_cell * q];
+    }
+    if (cc) for (int c = 0; c < nc * nc; ++c) {
         if (sag) sag[c] = cc[4 * c + 3];
         if (nrm) for (int a = 0; a < 3; ++a) nrm[3 * c + a] = cc[4 * c + a];
+    }
+    return BBRT_OK;
+}
+
+BBRT_API int bbrt_scene_setup_get(bbrt_scene_t s, int what, void* out, long long* count) {
+    if (!s || !count) return fail(BBRT_ERR_ARG, "bbrt_scene_setup_get: NULL argument");
+    const bbrt::HostScene& H = s->host;
+    const bbrt::CullTables& Cu = s->cull;
+    const long long P = H.n_patches, cn = H.coarse_n, nc = cn - 1;
+    const long long nb = Cu.enabled ? Cu.n_blocks_side : 0;
+    long long need = 0;
+    size_t elem = sizeof(double);
+    const void* host_src = nullptr;
+    const void* dev_src = nullptr;
+    double cull[11];
+    switch (what) {
+        case BBRT_SETUP_COARSE:
+            need = P * cn * cn * 3;
+            host_src = H.c_xyz.data();
+            dev_src = s->dev.c_xyz;
+            break;
+        case BBRT_SETUP_CELLS:
+            need = P * nc * nc * 4;
+            host_src = H.c_cell.data();
+            dev_src = s->dev.c_cell;
+            break;
+        case BBRT_SETUP_CELL_BOXES:
+            need = Cu.enabled ? P * nc * nc * 6 : 0;
+            elem = sizeof(float);
+            host_src = Cu.cell_box.data();
+            dev_src = s->dev.c_cell_box;
+            break;
+        case BBRT_SETUP_BLOCK_BOXES:
+            need = P * nb * nb * 6;
+            elem = sizeof(float);
+            host_src = Cu.block_box.data();
+            dev_src = s->dev.c_block_box;
+            break;
+        case BBRT_SETUP_CULL:
+            need = 11;
+            cull[0] = Cu.enabled ? 1.0 : 0.0;
+            cull[1] = Cu.block_cells;
+            cull[2] = static_cast<double>(nb);
+            cull[3] = Cu.a; cull[4] = Cu.h; cull[5] = Cu.b; cull[6] = Cu.coord; cull[7] = Cu.radius;
+            for (int a = 0; a < 3; ++a) cull[8 + a] = Cu.center[a];
+            host_src = cull;
+            dev_src = nullptr;
+            break;
+        default:
+            return fail(BBRT_ERR_ARG, "bbrt_scene_setup_get: unknown array");
+    }
+    if (!out) {
+        *count = need;
+        return BBRT_OK;
+    }
+    if (*count != need) return fail(BBRT_ERR_ARG, "bbrt_scene_setup_get: count must be " + std::to_string(need));
+    if (need == 0) return BBRT_OK;
+    if (s->setup_on_device && dev_src) {
+        std::lock_guard<std::mutex> g(s->mu);
+        BBRT_CUDA(cudaMemcpy(out, dev_src, elem * static_cast<size_t>(need), cudaMemcpyDeviceToHost));
+    } else {
+        std::memcpy(out, host_src, elem * static_cast<size_t>(need));
     }
     return BBRT_OK;
 }

@@ -127,10 +127,9 @@ struct PatchSetup {
     double max_sag;
 };
 
-// One patch: nodes/weights/fields copied into the flat tables, then the
-// centroid/box, the coarse grid and the per-cell padding.
-PatchSetup setup_patch(const bbrt_patch_desc& d, int cn, const std::vector<double>& cuv,
-                       double* nodes, double* fields, double* cxyz, double* ccell) {
+// One patch's flat tables: nodes un[I] vn[J] and their barycentric weights
+// uw[I] vw[J]; the kFields values of every node (i, j), node-major.
+void copy_patch_tables(const bbrt_patch_desc& d, double* nodes, double* fields) {
     const int I = d.imax, J = d.jmax;
     const size_t nn = static_cast<size_t>(I) * J;
     std::memcpy(nodes, d.u_nodes, sizeof(double) * I);
@@ -140,9 +139,17 @@ PatchSetup setup_patch(const bbrt_patch_desc& d, int cn, const std::vector<doubl
     std::memcpy(nodes + 2 * I + J, vw.data(), sizeof(double) * J);
     const double* src[kFields] = { d.x, d.y, d.z, d.dxdu, d.dydu, d.dzdu, d.dxdv, d.dydv, d.dzdv,
                                    d.nu_x, d.nu_y, d.nu_z };
-    // node-major: the kFields values of node (i, j) are contiguous
     for (size_t q = 0; q < nn; ++q)
         for (int k = 0; k < kFields; ++k) fields[q * kFields + k] = src[k][q];
+}
+
+// One patch: the centroid/box, the coarse grid and the per-cell padding.
+PatchSetup setup_patch(const bbrt_patch_desc& d, int cn, const std::vector<double>& cuv, double* cxyz, double* ccell) {
+    const int I = d.imax, J = d.jmax;
+    const size_t nn = static_cast<size_t>(I) * J;
+    const std::vector<double> uw = bary_weights(d.u_nodes, I), vw = bary_weights(d.v_nodes, J);
+    const double* src[kFields] = { d.x, d.y, d.z, d.dxdu, d.dydu, d.dzdu, d.dxdv, d.dydv, d.dzdv,
+                                   d.nu_x, d.nu_y, d.nu_z };
 
     PatchSetup s;
     // centroid = mean of the nodes; box = node AABB (later inflated)
@@ -266,7 +273,7 @@ private:
 
 }  // namespace
 
-void build_host_scene(const bbrt_object_desc* objects, int n_objects, const bbrt_config& cfg, HostScene& S) {
+void build_host_tables(const bbrt_object_desc* objects, int n_objects, const bbrt_config& cfg, HostScene& S) {
     if (n_objects <= 0 || objects == nullptr) throw std::invalid_argument("bbrt: a scene needs at least one object");
     if (cfg.coarse_grid_n < 2) throw std::invalid_argument("bbrt: coarse_grid_n must be >= 2");
     if (cfg.leaf_threshold < 1) throw std::invalid_argument("bbrt: leaf_threshold must be >= 1");
@@ -321,21 +328,11 @@ void build_host_scene(const bbrt_object_desc* objects, int n_objects, const bbrt
     }
     S.p_nodes.resize(static_cast<size_t>(node_total));
     S.p_fields.resize(static_cast<size_t>(field_total));
-    const size_t per_xyz = 3 * static_cast<size_t>(cn) * cn, per_cell = 4 * static_cast<size_t>(cn - 1) * (cn - 1);
-    S.c_xyz.resize(per_xyz * S.n_patches);
-    S.c_cell.resize(per_cell * S.n_patches);
-
-    // patch set-up, in parallel over patches
-    #pragma omp parallel for schedule(dynamic, 16)
-    for (int q = 0; q < S.n_patches; ++q) {
-        const int k = patch_obj[q];
-        const PatchSetup ps = setup_patch(*objects[k].patch, cn, S.coarse_uv, &S.p_nodes[S.p_node_off[q]],
-                                          &S.p_fields[S.p_field_off[q]], &S.c_xyz[per_xyz * q],
-                                          &S.c_cell[per_cell * q]);
-        std::memcpy(&S.box[6 * static_cast<size_t>(k)], ps.box, sizeof ps.box);
-        std::memcpy(&S.centroid[3 * static_cast<size_t>(k)], ps.centroid, sizeof ps.centroid);
-        S.padding[k] = ps.max_sag;
-    }
+    S.patch_obj = patch_obj;
+    // node tables (nodes and barycentric weights) and node-major fields
+    #pragma omp parallel for schedule(dynamic, 64)
+    for (int q = 0; q < S.n_patches; ++q)
+        copy_patch_tables(*objects[patch_obj[q]].patch, &S.p_nodes[S.p_node_off[q]], &S.p_fields[S.p_field_off[q]]);
     // triangles: exact AABB, centroid (a+b+c)/3, no padding
     for (int k = 0; k < n_objects; ++k) {
         if (S.kind[k] != BBRT_OBJ_TRIANGLE) continue;
@@ -347,13 +344,33 @@ void build_host_scene(const bbrt_object_desc* objects, int n_objects, const bbrt
         }
         S.padding[k] = 0.0;
     }
+}
 
+void setup_patches_host(const bbrt_object_desc* objects, HostScene& S) {
+    const int cn = S.coarse_n;
+    const size_t per_xyz = 3 * static_cast<size_t>(cn) * cn, per_cell = 4 * static_cast<size_t>(cn - 1) * (cn - 1);
+    S.c_xyz.resize(per_xyz * S.n_patches);
+    S.c_cell.resize(per_cell * S.n_patches);
+    // patch set-up, in parallel over patches
+    #pragma omp parallel for schedule(dynamic, 16)
+    for (int q = 0; q < S.n_patches; ++q) {
+        const int k = S.patch_obj[q];
+        const PatchSetup ps = setup_patch(*objects[k].patch, cn, S.coarse_uv, &S.c_xyz[per_xyz * q],
+                                          &S.c_cell[per_cell * q]);
+        std::memcpy(&S.box[6 * static_cast<size_t>(k)], ps.box, sizeof ps.box);
+        std::memcpy(&S.centroid[3 * static_cast<size_t>(k)], ps.centroid, sizeof ps.centroid);
+        S.padding[k] = ps.max_sag;
+    }
+}
+
+void finish_host_scene(HostScene& S) {
+    const int n_objects = S.n_objects;
     // BVH
     std::vector<int> ids(n_objects);
     for (int k = 0; k < n_objects; ++k) ids[k] = k;
     S.nodes.reserve(2 * static_cast<size_t>(n_objects));
     S.leaf_objects.reserve(n_objects);
-    BvhBuilder bb(S, S.nodes, S.leaf_objects, cfg.leaf_threshold);
+    BvhBuilder bb(S, S.nodes, S.leaf_objects, S.cfg.leaf_threshold);
     bb.build(std::move(ids), 0);
     S.max_depth = bb.max_depth;
 
@@ -368,6 +385,12 @@ void build_host_scene(const bbrt_object_desc* objects, int n_objects, const bbrt
     const double dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
     S.scene_diagonal = std::sqrt(dx * dx + dy * dy + dz * dz);
     S.max_patch_sagitta = ms;
+}
+
+void build_host_scene(const bbrt_object_desc* objects, int n_objects, const bbrt_config& cfg, HostScene& S) {
+    build_host_tables(objects, n_objects, cfg, S);
+    setup_patches_host(objects, S);
+    finish_host_scene(S);
 }
 
 void sample_grid(const bbrt_patch_desc& d, int n, double* xyz, double* normal, double* dxdu) {
@@ -518,6 +541,11 @@ void build_cull_tables(const HostScene& S, CullTables& C) {
             }
         }
     }
+    cull_constants(S, hmax, cmax, finite, C);
+}
+
+void cull_constants(const HostScene& S, double hmax, double cmax, bool finite, CullTables& C) {
+    C.enabled = false;
     const double eps64 = std::ldexp(1.0, -53), eps32 = std::ldexp(1.0, -24);
     if (!finite || cmax > 1e15 || 16.0 * eps64 * hmax * hmax > 1e-11) return;   // bound not small: no culling
     double lo[3], hi[3];

@@ -41,6 +41,7 @@ struct HostScene {
 
     // patches
     int n_patches = 0;
+    std::vector<int> patch_obj;       // object index of each patch
     int coarse_n = 0;
     std::vector<double> coarse_uv;    // [coarse_n] (the same for u and v, and every patch)
     std::vector<int> p_imax, p_jmax;
@@ -64,9 +65,18 @@ struct HostScene {
 
 // Builds every object's set-up, the BVH over objects in the given order and
 // the scene scale.  Throws std::invalid_argument / std::runtime_error with
-// the reference's wording on bad input.
+// the reference's wording on bad input.  The same in three steps:
+//   build_host_tables   validation, object tables, patch node / field tables,
+//                       triangle boxes and centroids
+//   setup_patches_host  per patch: coarse grid, cell normals and sagittas,
+//                       box, centroid, padding (the step the GPU can take over:
+//                       scene_compile.cu)
+//   finish_host_scene   BVH over the object boxes and centroids, scene scale
 void build_host_scene(const bbrt_object_desc* objects, int n_objects, const bbrt_config& cfg,
                       HostScene& out);
+void build_host_tables(const bbrt_object_desc* objects, int n_objects, const bbrt_config& cfg, HostScene& out);
+void setup_patches_host(const bbrt_object_desc* objects, HostScene& S);
+void finish_host_scene(HostScene& S);
 
 // SurfacePatch::sample_grid (SurfacePatch.hpp:199-242).
 void sample_grid(const bbrt_patch_desc& p, int n, double* xyz, double* normal, double* dxdu);
@@ -97,5 +107,10 @@ struct CullTables {
     double center[3] = { 0.0, 0.0, 0.0 };
 };
 void build_cull_tables(const HostScene& S, CullTables& out);
+// The per-ray inflation constants and the on/off decision of the cull tables,
+// from the longest triangle edge, the largest |coordinate| and whether every
+// offset corner is finite (build_cull_tables, or the GPU scene compile, which
+// computes those three per patch); sets C.enabled.
+void cull_constants(const HostScene& S, double hmax, double cmax, bool finite, CullTables& C);
 
 }  // namespace bbrt

@@ -99,6 +99,11 @@ typedef struct bbrt_config {
     int    guess;                      /* BBRT_GUESS_* (default TRIANGLE)                                 */
     int    cull;                       /* 1: conservative cell-box culling before Moller-Trumbore in
                                           stage 1; changes no result, only skips work (default 1)      */
+    int    setup_on_device;            /* where the per-patch set-up of scene creation runs (coarse grid,
+                                          cell normals and sagittas, boxes, centroids, cull tables;
+                                          SurfacePatch.hpp:380-492): -1 (default) on the GPU when a device
+                                          is present, else on the host; 0 host; 1 GPU (BBRT_ERR_CUDA
+                                          without one).  The values are the same bit for bit either way. */
 } bbrt_config;
 
 /* One patch file's numeric payload (SurfacePatch::Data, SurfacePatch.hpp:59-89).
@@ -139,6 +144,7 @@ typedef struct bbrt_scene_info {
     double scene_diagonal;       /* RayTracingDriver::compute_scene_scale, :386-396 */
     double max_patch_sagitta;
     long long device_bytes;
+    int setup_on_device;         /* 1: the per-patch set-up ran on the GPU */
 } bbrt_scene_info;
 
 typedef struct bbrt_object_info {
@@ -258,6 +264,19 @@ BBRT_API int  bbrt_object_info_get(bbrt_scene_t scene, int object, bbrt_object_i
 BBRT_API int  bbrt_patch_coarse_grid(bbrt_scene_t scene, int object, int* n,
                                      double* u, double* v, double* xyz,
                                      double* cell_sagitta, double* cell_normal);
+/* A scene's whole set-up arrays, from the host or the GPU scene compiler
+ * (no reference counterpart: for comparing the two).  `what`:
+ *   BBRT_SETUP_COARSE       double [n_patches][n * n][3]      coarse-grid vertices
+ *   BBRT_SETUP_CELLS        double [n_patches][(n-1)^2][4]    cell unit normal, sagitta
+ *   BBRT_SETUP_CELL_BOXES   float  [n_patches][(n-1)^2][6]    stage-1 cull boxes (0 when culling is off)
+ *   BBRT_SETUP_BLOCK_BOXES  float  [n_patches][blocks^2][6]   their block unions
+ *   BBRT_SETUP_CULL         double [11]  enabled, block cells, blocks per side, then the
+ *                                        inflation constants a, h, b, coord, radius, centre xyz
+ * With out == NULL the element count is written to *count; otherwise *count
+ * must equal it (BBRT_ERR_ARG if not). */
+enum { BBRT_SETUP_COARSE = 0, BBRT_SETUP_CELLS = 1, BBRT_SETUP_CELL_BOXES = 2, BBRT_SETUP_BLOCK_BOXES = 3,
+       BBRT_SETUP_CULL = 4 };
+BBRT_API int bbrt_scene_setup_get(bbrt_scene_t scene, int what, void* out, long long* count);
 /* RayTracingDriver::self_intersect_epsilon(leaving_object) (:260-265);
  * object < 0 means nullptr (scene-wide max sagitta). */
 BBRT_API int  bbrt_self_intersect_epsilon(bbrt_scene_t scene, int object, double* eps);
