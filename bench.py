@@ -152,15 +152,15 @@ class ClockSampler:
 
 
 def _hbm_peak():
-    """Measured copy bandwidth of this pool's B200 (MEASURED_PEAKS.json), else
-    the pool's earlier measurement."""
+    """Measured copy bandwidth of this pool's B200 (MEASURED_PEAKS.json) and
+    its source, else the pool's earlier measurement (the fallback)."""
     try:
-        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]), "measured"
     except (OSError, ValueError, KeyError):
-        return 6650.0
+        return 6650.0, "fallback"
 
 
-HBM_PEAK_GBS = _hbm_peak()
+HBM_PEAK_GBS, HBM_PEAK_SOURCE = _hbm_peak()
 PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "k_advance_traffic.json")
 
 
@@ -200,7 +200,8 @@ def advance_roofline(st, fp64_peak, fp32_peak, l2_peak):
             "pipes": {k: {"achieved": v[0], "peak": v[1], "unit": v[2], "frac": v[0] / v[1]} for k, v in pipes.items()},
             "note": "algorithmic work of the k_advance launches of one step (device counters) over their summed "
                     "CUDA-event time; peaks: FP64/FP32 FMA and L2-resident reads measured in this process "
-                    "(bbrt_measure_pipe_peak), HBM from MEASURED_PEAKS.json, all of measured; the exact FP64 "
+                    f"(bbrt_measure_pipe_peak), of measured; HBM {HBM_PEAK_GBS:.0f} GB/s, of {HBM_PEAK_SOURCE} "
+                    f"({'MEASURED_PEAKS.json' if HBM_PEAK_SOURCE == 'measured' else 'no MEASURED_PEAKS.json: the pool fallback'}); the exact FP64 "
                     "path runs unfused mul/add (half the FMA peak at most); traffic per launch from the ncu "
                     "capture in profiles/, scaled by node tests"}
 
@@ -369,8 +370,9 @@ def _accuracy(scene, o, d, maxb, C):
               "went_inside_plain": int((a["status"] == C.RAY_WENT_INSIDE).sum()),
               "went_inside_learned": int((b["status"] == C.RAY_WENT_INSIDE).sum()),
               "recorded_bounces": int(K),
-              "compared": "status, hit-object sequence and every recorded hit point, end point and exit direction "
-                          "vs the plain FP64 form"})
+              "compared": "status and hit-object sequence; every recorded hit point, its (u, v) and the exit "
+                          "direction held to 1e-10 vs the plain FP64 form; the end point (escaped rays: last hit + "
+                          "scene diagonal x exit direction) reported beside them"})
     return r
 
 

@@ -355,9 +355,13 @@ def compare_traces(ref: TraceResult, other: TraceResult, origins=None, bound: fl
     """Ray-by-ray agreement of two traces of the same rays, both recorded
     with every bounce (trace_recording_all): the share of rays with the same
     status, bounce count and hit-object sequence, and over those rays the
-    largest difference of any recorded hit point, of the end point and of the
-    exit direction.  With `origins`, the same share over the rays whose
-    incidence cosine (in `ref`) exceeds `grazing_cos` at every bounce."""
+    largest difference of any recorded hit point, of its patch parameters
+    (u, v) and of the exit direction — the quantities held to `bound`.  The
+    end point is reported beside them: for an escaped ray it is the tail
+    point last hit + scene diagonal * exit direction, so its difference is
+    the exit direction's scaled by the scene's size.  With `origins`, the
+    share of agreeing rays among those whose incidence cosine (in `ref`)
+    exceeds `grazing_cos` at every bounce."""
     K = ref["hit_object"].shape[1]
     if int(ref["bounce_count"].max(initial=0)) > K or int(other["bounce_count"].max(initial=0)) > other["hit_object"].shape[1]:
         raise ValueError("compare_traces: a trace did not record every bounce")
@@ -368,12 +372,17 @@ def compare_traces(ref: TraceResult, other: TraceResult, origins=None, bound: fl
     mask = np.arange(K)[None, :] < np.minimum(ref["bounce_count"], K)[:, None]
     diff = np.abs(ref["hit_point"] - other["hit_point"]).max(axis=2) if K else np.zeros((same.size, 0))
     err_hit = float(np.max(np.where(mask & same[:, None], diff, 0.0), initial=0.0))
+    err_uv = 0.0
+    if "hit_uv" in ref and "hit_uv" in other and K:
+        duv = np.abs(ref["hit_uv"] - other["hit_uv"]).max(axis=2)
+        err_uv = float(np.max(np.where(mask & same[:, None], duv, 0.0), initial=0.0))
     err_end = float(np.max(np.where(same[:, None], np.abs(ref["end_point"] - other["end_point"]), 0.0), initial=0.0))
     err_exit = float(np.max(np.where(same[:, None], np.abs(ref["exit_dir"] - other["exit_dir"]), 0.0), initial=0.0))
     out = {"rays": int(same.size), "sequence_agreement": float(np.mean(same)) if same.size else 1.0,
-           "max_hit_err_agreeing": err_hit, "max_end_point_err_agreeing": err_end,
-           "max_exit_dir_err_agreeing": err_exit, "bounces_compared": int(mask.sum()),
-           "hit_err_bound": bound, "within_bound": bool(max(err_hit, err_end, err_exit) <= bound)}
+           "max_hit_err_agreeing": err_hit, "max_uv_err_agreeing": err_uv,
+           "max_exit_dir_err_agreeing": err_exit, "max_end_point_err_agreeing": err_end,
+           "bounces_compared": int(mask.sum()), "hit_err_bound": bound,
+           "within_bound": bool(max(err_hit, err_uv, err_exit) <= bound)}
     if origins is not None:
         ok = min_incidence_cos(origins, ref) > grazing_cos
         out["non_grazing_rays"] = int(ok.sum())

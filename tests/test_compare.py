@@ -12,7 +12,8 @@ def _trace(n=4, K=3, seed=0):
     return {"status": np.zeros(n, np.int32), "bounce_count": np.array([0, 1, 2, 3][:n], np.int32),
             "hit_object": np.where(np.arange(K)[None, :] < np.array([0, 1, 2, 3][:n])[:, None],
                                    rng.integers(0, 9, (n, K)), -1).astype(np.int32),
-            "hit_point": rng.normal(size=(n, K, 3)), "exit_dir": rng.normal(size=(n, 3)),
+            "hit_point": rng.normal(size=(n, K, 3)), "hit_uv": rng.normal(size=(n, K, 2)),
+            "exit_dir": rng.normal(size=(n, 3)),
             "end_point": rng.normal(size=(n, 3))}
 
 
@@ -27,13 +28,19 @@ def test_compare_identical_and_every_bounce_counted():
     assert r["bounces_compared"] == 6
 
 
-def test_compare_sees_a_late_bounce_end_point_and_exit_direction():
+def test_compare_sees_a_late_bounce_its_parameters_and_the_exit_direction():
     a = _trace()
-    for key, idx in (("hit_point", (3, 2, 1)), ("end_point", (2, 0)), ("exit_dir", (1, 2))):
+    for key, idx in (("hit_point", (3, 2, 1)), ("hit_uv", (2, 1, 0)), ("exit_dir", (1, 2))):
         b = _copy(a)
         b[key][idx] += 1e-9
         r = api.compare_traces(a, b)
         assert r["sequence_agreement"] == 1.0 and not r["within_bound"], key
+    # the end point is reported, not held to the bound (an escaped ray's tail
+    # point scales the exit direction's difference by the scene's size)
+    b = _copy(a)
+    b["end_point"][2, 0] += 1e-9
+    r = api.compare_traces(a, b)
+    assert r["within_bound"] and r["max_end_point_err_agreeing"] > 0
     # a difference past a ray's last bounce is not a recorded hit
     b = _copy(a)
     b["hit_point"][1, 2, 0] += 1.0
