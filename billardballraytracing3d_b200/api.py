@@ -359,32 +359,60 @@ def compare_traces(ref: TraceResult, other: TraceResult, origins=None, bound: fl
     (u, v) and of the exit direction — the quantities held to `bound`.  The
     end point is reported beside them: for an escaped ray it is the tail
     point last hit + scene diagonal * exit direction, so its difference is
-    the exit direction's scaled by the scene's size.  With `origins`, the
-    share of agreeing rays among those whose incidence cosine (in `ref`)
-    exceeds `grazing_cos` at every bounce."""
+    the exit direction's scaled by the scene's size.
+
+    With `origins`, rays whose incidence cosine (in `ref`) falls to
+    `grazing_cos` or below at some bounce are set apart, as the accuracy bar
+    sets them apart: the bound is held over the other agreeing rays, and the
+    maxima over all agreeing rays are reported beside it."""
     K = ref["hit_object"].shape[1]
     if int(ref["bounce_count"].max(initial=0)) > K or int(other["bounce_count"].max(initial=0)) > other["hit_object"].shape[1]:
         raise ValueError("compare_traces: a trace did not record every bounce")
     if other["hit_object"].shape[1] != K:
         raise ValueError("compare_traces: the traces recorded different bounce counts")
+    n = ref["status"].size
     same = (ref["status"] == other["status"]) & (ref["bounce_count"] == other["bounce_count"])
     same &= np.all(ref["hit_object"] == other["hit_object"], axis=1)
     mask = np.arange(K)[None, :] < np.minimum(ref["bounce_count"], K)[:, None]
-    diff = np.abs(ref["hit_point"] - other["hit_point"]).max(axis=2) if K else np.zeros((same.size, 0))
-    err_hit = float(np.max(np.where(mask & same[:, None], diff, 0.0), initial=0.0))
-    err_uv = 0.0
+    # per-ray maxima
+    hit = np.where(mask, np.abs(ref["hit_point"] - other["hit_point"]).max(axis=2), 0.0).max(axis=1, initial=0.0) \
+        if K else np.zeros(n)
+    uv = np.zeros(n)
     if "hit_uv" in ref and "hit_uv" in other and K:
-        duv = np.abs(ref["hit_uv"] - other["hit_uv"]).max(axis=2)
-        err_uv = float(np.max(np.where(mask & same[:, None], duv, 0.0), initial=0.0))
-    err_end = float(np.max(np.where(same[:, None], np.abs(ref["end_point"] - other["end_point"]), 0.0), initial=0.0))
-    err_exit = float(np.max(np.where(same[:, None], np.abs(ref["exit_dir"] - other["exit_dir"]), 0.0), initial=0.0))
-    out = {"rays": int(same.size), "sequence_agreement": float(np.mean(same)) if same.size else 1.0,
-           "max_hit_err_agreeing": err_hit, "max_uv_err_agreeing": err_uv,
-           "max_exit_dir_err_agreeing": err_exit, "max_end_point_err_agreeing": err_end,
-           "bounces_compared": int(mask.sum()), "hit_err_bound": bound,
-           "within_bound": bool(max(err_hit, err_uv, err_exit) <= bound)}
+        uv = np.where(mask, np.abs(ref["hit_uv"] - other["hit_uv"]).max(axis=2), 0.0).max(axis=1, initial=0.0)
+    ext = np.abs(ref["exit_dir"] - other["exit_dir"]).max(axis=1)
+    end = np.abs(ref["end_point"] - other["end_point"]).max(axis=1)
+
+    def mx(v, sel):
+        return float(np.max(np.where(sel, v, 0.0), initial=0.0))
+
+    out = {"rays": int(n), "sequence_agreement": float(np.mean(same)) if n else 1.0,
+           "max_hit_err_agreeing": mx(hit, same), "max_uv_err_agreeing": mx(uv, same),
+           "max_exit_dir_err_agreeing": mx(ext, same), "max_end_point_err_agreeing": mx(end, same),
+           "bounces_compared": int(mask.sum()), "hit_err_bound": bound}
+    held = same
     if origins is not None:
-        ok = min_incidence_cos(origins, ref) > grazing_cos
+        cos = min_incidence_cos(origins, ref)
+        ok = cos > grazing_cos
+        held = same & ok
+        out["grazing_cos"] = grazing_cos
         out["non_grazing_rays"] = int(ok.sum())
         out["sequence_agreement_non_grazing"] = float(np.mean(same[ok])) if ok.any() else 1.0
+        out["max_hit_err_non_grazing"] = mx(hit, held)
+        out["max_uv_err_non_grazing"] = mx(uv, held)
+        out["max_exit_dir_err_non_grazing"] = mx(ext, held)
+        if same.any():
+            w = int(np.argmax(np.where(same, np.maximum(hit, np.maximum(uv, ext)), -1.0)))
+            out["largest_err_ray_min_incidence_cos"] = float(cos[w])
+    worst = np.maximum(hit, np.maximum(uv, ext))
+    out["within_bound"] = bool(mx(worst, held) <= bound)
+    # a ray agrees within the bound when its sequence agrees and every
+    # recorded hit point, (u, v) and its exit direction are within `bound`
+    # (differences of a few ulp at the first bounce grow by about twice the
+    # obstacle spacing over the radius per bounce, so a long chain can leave
+    # the bound although every bounce took the same patch)
+    base = np.ones(n, bool) if origins is None else (min_incidence_cos(origins, ref) > grazing_cos)
+    within = same & (worst <= bound)
+    out["agreement_within_bound"] = float(np.mean(within[base])) if base.any() else 1.0
+    out["rays_over_bound"] = int(np.sum(held & (worst > bound)))
     return out

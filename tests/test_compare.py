@@ -76,3 +76,12 @@ def test_min_incidence_cos_of_a_mirror_path():
     r = {"bounce_count": np.array([2]), "hit_point": np.array([[p1, p2]]), "exit_dir": np.array([d2])}
     cos = api.min_incidence_cos(o, r)
     assert np.isclose(cos[0], min(np.cos(np.pi / 3), abs(d1[0])))
+
+
+def test_agreement_within_bound_counts_rays():
+    a = _trace()
+    b = _copy(a)
+    b["hit_uv"][3, 2, 0] += 1e-9       # ray 3 agrees in sequence but not within the bound
+    r = api.compare_traces(a, b)
+    assert r["sequence_agreement"] == 1.0 and not r["within_bound"]
+    assert r["agreement_within_bound"] == 0.75 and r["rays_over_bound"] == 1

@@ -38,8 +38,8 @@ def test_watchdog_stops_the_round_and_the_next_call_is_clean(built, graph_rounds
 def test_tensor_core_wait_bound_reports_and_the_next_call_is_clean(built):
     patches = scenes.scene_tetra_spheres()
     sc = api.Scene(patches, config=C.default_config(coarse_grid_n=17, newton_tol=1e-12))
-    to, td = scenes.cone_rays(65536, 99, 5.0, 3.0, 10.0)
-    sc.guess_train(to, td, 200, epochs=1)
+    to, td = scenes.cone_rays(262144, 99, 5.0, 3.0, 10.0)
+    sc.guess_train(to, td, 200, epochs=4)
     o, d = scenes.cone_rays(65536, 1234, 5.0, 3.0, 10.0)
     sc.tuning(wave_tail=1024)   # wavefront rounds (which run the network) down to the last 1024 requests
     sc.set_modes(C.PREC_SPLIT, C.GUESS_LEARNED)
