@@ -567,19 +567,25 @@ def second_workload(args, dev, stream, flush):
 def multi_scene(k, steps, dev):
     """k independent scenes of uneven size (scenes.multi_scene_workload:
     1-32 obstacles of 96 or 384 patches at degree 4 or 6, 16k-1M rays each,
-    <= 100 bounces, plain FP64): device time of tracing them together in one
-    bbrt_trace_batch call vs one after another (the same call with one scene
-    at a time), best of `steps`."""
+    <= 100 bounces, plain FP64): device time of tracing them as one scene set
+    (bbrt_trace_set: one wavefront for all), together on their own streams
+    (bbrt_trace_batch), and one after another; best of `steps` after a warm-up
+    each.  Also the wall time of building the scenes (per-patch set-up on the
+    GPU) and of building the set."""
     import torch
     from billardballraytracing3d_b200 import _capi as C
     from billardballraytracing3d_b200 import api, scenes
     work = scenes.multi_scene_workload(k)
-    scs, tens = [], []
-    for patches, o, d, maxb, cn, tol in work:
-        sc = api.Scene(patches, config=C.default_config(coarse_grid_n=cn, newton_tol=tol))
+    t0 = time.perf_counter()
+    scs = [api.Scene(patches, config=C.default_config(coarse_grid_n=cn, newton_tol=tol))
+           for patches, o, d, maxb, cn, tol in work]
+    for sc in scs:
         sc.upload()
+    torch.cuda.synchronize(dev)
+    create_s = time.perf_counter() - t0
+    tens = []
+    for patches, o, d, maxb, cn, tol in work:
         n = o.shape[0]
-        scs.append(sc)
         tens.append(dict(o=torch.from_numpy(o).to(dev), d=torch.from_numpy(d).to(dev),
                          status=torch.zeros(n, dtype=torch.int32, device=dev),
                          bounce_count=torch.zeros(n, dtype=torch.int32, device=dev)))
@@ -587,19 +593,33 @@ def multi_scene(k, steps, dev):
     optr = [t["o"].data_ptr() for t in tens]
     dptr = [t["d"].data_ptr() for t in tens]
     outs = [dict(status=t["status"].data_ptr(), bounce_count=t["bounce_count"].data_ptr()) for t in tens]
-    st, _ = api.trace_batch_device(scs, optr, dptr, ns, 100, outs)   # warm-up
+    t0 = time.perf_counter()
+    ss = api.SceneSet(scs)
+    set_create_s = time.perf_counter() - t0
+    st, _ = ss.trace_device(optr, dptr, ns, 100, outs)   # warm-up (graph capture)
+    ss.trace_device(optr, dptr, ns, 100, outs, want_stats=False)
     bounces = st["bounces"]
+    set_ms = min(ss.trace_device(optr, dptr, ns, 100, outs, want_stats=False)[1] for _ in range(steps))
+    set_bc = [t["bounce_count"].clone() for t in tens]
+    api.trace_batch_device(scs, optr, dptr, ns, 100, outs)   # warm-up
     batch = min(api.trace_batch_device(scs, optr, dptr, ns, 100, outs, want_stats=False)[1] for _ in range(steps))
+    same = all(torch.equal(a, t["bounce_count"]) for a, t in zip(set_bc, tens))
     for j in range(k):   # warm-up one at a time
         api.trace_batch_device([scs[j]], [optr[j]], [dptr[j]], [ns[j]], 100, [outs[j]], want_stats=False)
     seq = min(sum(api.trace_batch_device([scs[j]], [optr[j]], [dptr[j]], [ns[j]], 100, [outs[j]],
                                          want_stats=False)[1] for j in range(k)) for _ in range(steps))
     return {"scenes": k, "rays": int(sum(ns)), "patches": int(sum(len(w[0]) for w in work)),
-            "bounces": int(bounces), "batched_ms": batch, "sequential_ms": seq,
-            "batched_value": bounces / (batch / 1e3), "sequential_value": bounces / (seq / 1e3),
-            "unit": UNIT, "speedup": seq / batch,
-            "note": "device time of one bbrt_trace_batch call over all scenes vs the sum over one-scene calls; "
-                    "plain FP64 form, default schedule"}
+            "bounces": int(bounces), "set_ms": set_ms, "batched_ms": batch, "sequential_ms": seq,
+            "set_value": bounces / (set_ms / 1e3), "batched_value": bounces / (batch / 1e3),
+            "sequential_value": bounces / (seq / 1e3), "unit": UNIT,
+            "set_over_sequential": seq / set_ms, "set_over_batched": batch / set_ms,
+            "set_results_equal_batched": bool(same),
+            "scene_build_s": create_s, "set_build_s": set_create_s, "set_rounds": st["rounds"],
+            "set_launches": st["launches"],
+            "note": "device time of one bbrt_trace_set call (the set: one wavefront over all scenes, rays in and "
+                    "results out included) vs one bbrt_trace_batch call (a wavefront per scene, scenes on their "
+                    "own streams) vs the sum of one-scene calls; plain FP64 form, default schedule; scene_build_s: "
+                    "wall time of creating and uploading the scenes (per-patch set-up on the GPU, BVH on the host)"}
 
 
 def main():

@@ -297,6 +297,12 @@ def _declare(lib):
     lib.bbrt_scene_set_modes.argtypes = [V, I, I]
     lib.bbrt_trace_batch.argtypes = [ctypes.POINTER(V), I, ctypes.POINTER(V), ctypes.POINTER(V), c_ll_p, I,
                                      ctypes.POINTER(TraceOut), ctypes.POINTER(TraceStats), c_double_p]
+    lib.bbrt_scene_set_create.argtypes = [ctypes.POINTER(V), I, ctypes.POINTER(V)]
+    lib.bbrt_scene_set_destroy.argtypes = [V]
+    lib.bbrt_scene_set_destroy.restype = None
+    lib.bbrt_scene_set_configure.argtypes = [V, I, ctypes.POINTER(Tuning)]
+    lib.bbrt_trace_set.argtypes = [V, ctypes.POINTER(V), ctypes.POINTER(V), c_ll_p, I, ctypes.POINTER(TraceOut),
+                                   ctypes.POINTER(TraceStats), c_double_p, V]
     lib.bbrt_scene_get_tuning.argtypes = [V, ctypes.POINTER(Tuning)]
     lib.bbrt_scene_set_tuning.argtypes = [V, ctypes.POINTER(Tuning)]
     lib.bbrt_scene_autotune.argtypes = [V, c_double_p, c_double_p, LL, I, I, ctypes.POINTER(Tuning), c_double_p, V]

@@ -291,6 +291,71 @@ def trace_batch_device(scenes: Sequence["Scene"], origin_ptrs, dir_ptrs, ns, max
     return (st.as_dict() if want_stats else None), ms.value
 
 
+def _trace_outs(outs, k):
+    """Per-scene dicts of device pointers (+ 'record') as a bbrt_trace_out array."""
+    if outs is None:
+        return None
+    to = (C.TraceOut * k)()
+    for j, od in enumerate(outs):
+        if not od:
+            continue
+        to[j].record_bounces = int(od.get("record", 0))
+        for key, v in od.items():
+            if key == "record":
+                continue
+            ct = {"status": ctypes.c_int, "bounce_count": ctypes.c_int, "hit_object": ctypes.c_int,
+                  "err_object": ctypes.c_int, "ray_work": ctypes.c_longlong}.get(key, ctypes.c_double)
+            setattr(to[j], key, ctypes.cast(ctypes.c_void_p(v), ctypes.POINTER(ct)))
+    return to
+
+
+class SceneSet:
+    """bbrt_scene_set: several scenes traced as one wavefront (one launch
+    sequence for all members); results per member, in its own numbering."""
+
+    def __init__(self, scenes: Sequence["Scene"]):
+        self.lib = C.load_library()
+        self.k = len(scenes)
+        hs = (ctypes.c_void_p * self.k)(*[s.h for s in scenes])
+        h = ctypes.c_void_p()
+        C.check(self.lib, self.lib.bbrt_scene_set_create(hs, self.k, ctypes.byref(h)), "bbrt_scene_set_create")
+        self.h = h
+
+    def configure(self, precision: int = C.PREC_FP64, **tuning):
+        t = None
+        if tuning:
+            t = C.Tuning()
+            for k, v in tuning.items():
+                setattr(t, k, v)
+        C.check(self.lib, self.lib.bbrt_scene_set_configure(self.h, int(precision), ctypes.byref(t) if t else None),
+                "bbrt_scene_set_configure")
+
+    def trace_device(self, origin_ptrs, dir_ptrs, ns, max_bounces: int, outs=None, want_stats: bool = True,
+                     stream: int = 0):
+        """Every member's rays (device pointers) in one trace; returns (stats, set_ms)."""
+        k = self.k
+        op = (ctypes.c_void_p * k)(*[ctypes.c_void_p(p) for p in origin_ptrs])
+        dp = (ctypes.c_void_p * k)(*[ctypes.c_void_p(p) for p in dir_ptrs])
+        nn = (ctypes.c_longlong * k)(*[int(v) for v in ns])
+        st = C.TraceStats()
+        ms = ctypes.c_double()
+        C.check(self.lib, self.lib.bbrt_trace_set(self.h, op, dp, nn, int(max_bounces), _trace_outs(outs, k),
+                                                  ctypes.byref(st) if want_stats else None, ctypes.byref(ms),
+                                                  ctypes.c_void_p(stream) if stream else None), "bbrt_trace_set")
+        return (st.as_dict() if want_stats else None), ms.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.bbrt_scene_set_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def sample_grid(patch, n: int):
     """SurfacePatch::sample_grid(n) through the C ABI: (xyz, normal, dX/du)."""
     lib = C.load_library()

@@ -30,6 +30,7 @@
 #include "dscene.h"
 #include "guess.h"
 #include "scene_compile.h"
+#include "scene_set.h"
 #include "scene_host.hpp"
 
 namespace bbrt {
@@ -51,7 +52,7 @@ int request_sort_max_objects();
 cudaError_t sort_requests(const NewtonRequest* req, long long n, const unsigned* n_dev, int n_objects, int side,
                           int coarse_cells, void* ws, NewtonRequest* out, cudaStream_t stream);
 cudaError_t ray_order(const double* o, const double* d, long long n, const double center[3], double radius,
-                      void* ws, int* order, cudaStream_t stream, bool entry);
+                      void* ws, int* order, cudaStream_t stream, bool entry, long long base);
 cudaError_t launch_query(const DScene& S, const QueryArgs& Q, cudaStream_t stream);
 cudaError_t noalloc_prepare();
 cudaError_t launch_trace_noalloc(const DScene& S, TraceArgs A, bool count_hits, long long* hit_counts_out,
@@ -150,6 +151,12 @@ struct bbrt_scene {
     // Launch schedule of this scene (library defaults until set or autotuned).
     bool tune_set = false;
     bbrt_tuning tune{};
+    // Scene set (bbrt_scene_set): the members' ray ranges of the current call
+    // ([M + 1] offsets), each member's ordering sphere ([M][4] centre, radius)
+    // and the member of every ray; empty / null for a single scene.
+    std::vector<long long> member_rays;
+    std::vector<double> member_sphere;
+    const int* ray_member = nullptr;
     // Training-sample recording, set only inside bbrt_guess_train.
     bbrt::GuessSample* rec_samples = nullptr;
     unsigned long long* rec_count = nullptr;
@@ -696,6 +703,27 @@ bool sort_round_requests(const bbrt_scene* s) {
     return tuning().sort_requests && s->host.n_objects >= 1 && s->host.n_objects <= bbrt::request_sort_max_objects();
 }
 
+// Round 0's processing order (s->order): rays bucketed by where they enter
+// the scene's sphere; in a scene set, each member's rays among themselves
+// in its own range, so that warps keep to one member's tree.
+cudaError_t order_rays(bbrt_scene* s, const bbrt::TraceArgs& A, cudaStream_t st) {
+    int* order = static_cast<int*>(s->order.p);
+    const bool entry = tuning().order_entry != 0;
+    if (s->member_rays.empty()) {
+        const double radius = s->cull.radius > 0.0 ? s->cull.radius : s->host.scene_diagonal;
+        return bbrt::ray_order(A.origins, A.dirs, A.n, s->cull.center, radius, s->order_ws.p, order, st, entry, 0);
+    }
+    for (size_t m = 0; m + 1 < s->member_rays.size(); ++m) {
+        const long long off = s->member_rays[m], cnt = s->member_rays[m + 1] - off;
+        if (cnt <= 0) continue;
+        const double* sp = &s->member_sphere[4 * m];
+        const cudaError_t e = bbrt::ray_order(A.origins + 3 * off, A.dirs + 3 * off, cnt, sp, sp[3], s->order_ws.p,
+                                              order + off, st, entry, off);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 // ---- the wavefront trace as one CUDA graph ------------------------------------
 
 // Values a captured graph depends on, flattened (pointers and integers by
@@ -800,11 +828,7 @@ int build_wave_graph(bbrt_scene* s, const bbrt::TraceArgs& A, const bbrt_tuning&
     cudaGraphConditionalHandle loop = 0;
     cudaError_t e = cudaStreamGetCaptureInfo(cs, &cst, nullptr, &cg, nullptr, nullptr);
     if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&loop, cg, 0, cudaGraphCondAssignDefault);
-    if (e == cudaSuccess && T.order_rays) {
-        const double radius = s->cull.radius > 0.0 ? s->cull.radius : s->host.scene_diagonal;
-        e = bbrt::ray_order(A.origins, A.dirs, n, s->cull.center, radius, s->order_ws.p,
-                            static_cast<int*>(s->order.p), cs, tuning().order_entry != 0);
-    }
+    if (e == cudaSuccess && T.order_rays) e = order_rays(s, A, cs);
     if (e == cudaSuccess) e = cudaMemsetAsync(c, 0, bbrt::kWaveCounters * sizeof(unsigned int), cs);
     if (e == cudaSuccess) e = round(cs, W0, loop);
     if (e == cudaSuccess) {
@@ -892,6 +916,8 @@ int launch_wave_graph(bbrt_scene* s, const bbrt::TraceArgs& A, const bbrt_tuning
         k.put(x);
     k.put(s->guess.min_logit);
     k.put(s->guess.t_window);
+    k.put(static_cast<const void*>(A.ray_member));
+    for (long long r : s->member_rays) k.put(r);
     auto& gs = s->wgraphs;
     auto it = std::find_if(gs.begin(), gs.end(), [&](const bbrt_scene::WaveGraph& g) { return g.key == k.v; });
     if (it == gs.end()) {
@@ -963,11 +989,7 @@ struct WaveRun {
         if (T.order_rays) {
             BBRT_CUDA(s->order_ws.ensure(bbrt::ray_order_workspace_bytes(n)));
             BBRT_CUDA(s->order.ensure(sizeof(int) * static_cast<size_t>(n)));
-            const double radius = s->cull.radius > 0.0 ? s->cull.radius : s->host.scene_diagonal;
-            BBRT_CUDA(timed(s, K_ORDER, st, [&] {
-                return bbrt::ray_order(A.origins, A.dirs, n, s->cull.center, radius, s->order_ws.p,
-                                       static_cast<int*>(s->order.p), st, tuning().order_entry != 0);
-            }));
+            BBRT_CUDA(timed(s, K_ORDER, st, [&] { return order_rays(s, A, st); }));
             W.order = static_cast<const int*>(s->order.p);
         }
         BBRT_CUDA(cudaMemsetAsync(W.counters, 0, bbrt::kWaveCounters * sizeof(unsigned int), st));
@@ -1121,6 +1143,7 @@ int prepare_trace(bbrt_scene* s, const double* d_o, const double* d_d, long long
     A.sample_count = s->rec_count;
     A.sample_cap_pos = s->rec_cap_pos;
     A.sample_cap_neg = s->rec_cap_neg;
+    A.ray_member = s->ray_member;
     if (want_stats) BBRT_CUDA(cudaMemsetAsync(s->stats.p, 0, sizeof(long long) * bbrt::ST_COUNT, st));
     BBRT_CUDA(cudaMemsetAsync(s->work.p, 0, sizeof(unsigned long long), st));
     if (learned_trace(s)) {
@@ -2466,3 +2489,408 @@ BBRT_API int bbrt_trace_batch(const bbrt_scene_t* scenes, int n_scenes, const do
     cleanup();
     return rc;
 }
+
+// ---- several scenes as one trace (scene set) --------------------------------
+//
+// A set copies its members' device arrays side by side into one scene: the
+// objects, patch tables, coarse grids, cell data and cull boxes are
+// concatenated (member m's object k becomes object obj_off[m] + k), and the
+// BVH trees form one forest renumbered breadth-first across all trees, so
+// that the top levels of every member land in the shared-memory node copy
+// the trace kernels stage.  Each ray carries its member: its query starts at
+// the member's root and uses the member's scale and cull constants.  Every
+// per-object computation is the member's own, so the results equal a trace
+// of each member alone, bit for bit.
+
+struct bbrt_scene_set {
+    bbrt_scene merged;
+    int n_members = 0;
+    std::vector<int> obj_off;              // [M + 1]
+    std::vector<bbrt::MemberIO> io;        // per-call member table (host copy of io_dev)
+    DevBuf io_dev, ray_member, set_o, set_d, o_status, o_bounce, o_dir, o_end, o_hobj, o_hpt, o_huv, o_eobj,
+        o_eval, o_work;
+    cudaEvent_t ev[2] = { nullptr, nullptr };
+    ~bbrt_scene_set() {
+        for (DevBuf* b : { &io_dev, &ray_member, &set_o, &set_d, &o_status, &o_bounce, &o_dir, &o_end, &o_hobj,
+                           &o_hpt, &o_huv, &o_eobj, &o_eval, &o_work })
+            b->release();
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+    }
+};
+
+namespace {
+
+// Device arrays of several members joined into one (device-to-device copies;
+// a member without the array contributes zeros).
+template <class T>
+int join_device(bbrt_scene& S, const std::vector<std::pair<const T*, size_t>>& parts, const T*& dst) {
+    size_t total = 0;
+    for (const auto& pr : parts) total += pr.second;
+    T* p = nullptr;
+    int rc = S.alloc(total, p);
+    if (rc) return rc;
+    size_t at = 0;
+    for (const auto& pr : parts) {
+        if (pr.second) {
+            if (pr.first) BBRT_CUDA(cudaMemcpyAsync(p + at, pr.first, sizeof(T) * pr.second, cudaMemcpyDeviceToDevice, S.stream));
+            else BBRT_CUDA(cudaMemsetAsync(p + at, 0, sizeof(T) * pr.second, S.stream));
+        }
+        at += pr.second;
+    }
+    dst = p;
+    return BBRT_OK;
+}
+
+int build_scene_set(const std::vector<bbrt_scene*>& mem, bbrt_scene_set* set) {
+    const int M = static_cast<int>(mem.size());
+    const bbrt::HostScene& H0 = mem[0]->host;
+    for (bbrt_scene* m : mem) {
+        const bbrt::HostScene& H = m->host;
+        const bbrt_config &a = H.cfg, &b = H0.cfg;
+        if (H.coarse_n != H0.coarse_n || a.newton_max_iters != b.newton_max_iters || a.newton_tol != b.newton_tol ||
+            a.self_intersect_eps_factor != b.self_intersect_eps_factor ||
+            a.sagitta_clearance_factor != b.sagitta_clearance_factor || a.backface_tol != b.backface_tol ||
+            a.cull != b.cull || m->dev.precision != mem[0]->dev.precision || m->device != mem[0]->device)
+            return fail(BBRT_ERR_ARG, "bbrt_scene_set_create: the member scenes must share the coarse grid size, "
+                                      "the Newton and epsilon constants, culling, precision and device");
+    }
+    bbrt_scene& S = set->merged;
+    int dev = -1;
+    BBRT_CUDA(cudaGetDevice(&dev));
+    if (dev != mem[0]->device) return fail(BBRT_ERR_STATE, "bbrt_scene_set_create: the current device is not the scenes' device");
+    int rc = ensure_device(&S);
+    if (rc) return rc;
+    bbrt::HostScene& HM = S.host;
+    HM.cfg = H0.cfg;
+    HM.cfg.guess = BBRT_GUESS_TRIANGLE;
+    HM.coarse_n = H0.coarse_n;
+    HM.coarse_uv = H0.coarse_uv;
+    std::vector<long long> obj_off(M + 1, 0), patch_off(M + 1, 0), tri_off(M + 1, 0), leaf_off(M + 1, 0),
+        node_off(M + 1, 0), ntab_off(M + 1, 0), ftab_off(M + 1, 0);
+    for (int m = 0; m < M; ++m) {
+        const bbrt::HostScene& H = mem[m]->host;
+        obj_off[m + 1] = obj_off[m] + H.n_objects;
+        patch_off[m + 1] = patch_off[m] + H.n_patches;
+        tri_off[m + 1] = tri_off[m] + static_cast<long long>(H.tri.size() / 9);
+        leaf_off[m + 1] = leaf_off[m] + static_cast<long long>(H.leaf_objects.size());
+        node_off[m + 1] = node_off[m] + static_cast<long long>(H.nodes.size());
+        ntab_off[m + 1] = ntab_off[m] + static_cast<long long>(H.p_nodes.size());
+        ftab_off[m + 1] = ftab_off[m] + static_cast<long long>(H.p_fields.size());
+    }
+    if (obj_off[M] > (1LL << 30) || node_off[M] >= (1LL << 24))
+        return fail(BBRT_ERR_UNSUPPORTED, "bbrt_scene_set_create: too many objects or BVH nodes in the set");
+    HM.n_objects = static_cast<int>(obj_off[M]);
+    HM.n_patches = static_cast<int>(patch_off[M]);
+    set->obj_off.assign(obj_off.begin(), obj_off.end());
+    std::vector<int> pdims;
+    for (int m = 0; m < M; ++m) {
+        const bbrt::HostScene& H = mem[m]->host;
+        for (int k = 0; k < H.n_objects; ++k) {
+            HM.kind.push_back(H.kind[k]);
+            HM.sub.push_back(H.sub[k] + static_cast<int>(H.kind[k] == BBRT_OBJ_PATCH ? patch_off[m] : tri_off[m]));
+            HM.padding.push_back(H.padding[k]);
+        }
+        for (int q = 0; q < H.n_patches; ++q) {
+            HM.p_imax.push_back(H.p_imax[q]);
+            HM.p_jmax.push_back(H.p_jmax[q]);
+            HM.p_node_off.push_back(H.p_node_off[q] + ntab_off[m]);
+            HM.p_field_off.push_back(H.p_field_off[q] + ftab_off[m]);
+            pdims.push_back(H.p_imax[q]);
+            pdims.push_back(H.p_jmax[q]);
+        }
+        for (int o : H.leaf_objects) HM.leaf_objects.push_back(o + static_cast<int>(obj_off[m]));
+    }
+    // the forest, breadth-first across all trees (children explicit)
+    const size_t NN = static_cast<size_t>(node_off[M]);
+    std::vector<std::pair<int, int>> order;
+    order.reserve(NN);
+    std::vector<std::vector<int>> newid(M);
+    for (int m = 0; m < M; ++m) {
+        newid[m].assign(mem[m]->host.nodes.size(), -1);
+        if (!mem[m]->host.nodes.empty()) order.push_back({ m, 0 });
+    }
+    for (size_t h = 0; h < order.size(); ++h) {
+        const int m = order[h].first, idx = order[h].second;
+        newid[m][idx] = static_cast<int>(h);
+        const bbrt::BvhNode& nd = mem[m]->host.nodes[idx];
+        if (nd.right >= 0) {
+            order.push_back({ m, idx + 1 });
+            order.push_back({ m, nd.right });
+        }
+    }
+    std::vector<double> nbox(6 * NN);
+    std::vector<int> nlink(4 * NN), roots(M, 0);
+    std::vector<double> params(static_cast<size_t>(M) * bbrt::kMemberParams, 0.0);
+    for (size_t h = 0; h < order.size(); ++h) {
+        const int m = order[h].first, idx = order[h].second;
+        const bbrt::BvhNode& nd = mem[m]->host.nodes[idx];
+        std::memcpy(&nbox[6 * h], nd.box, sizeof(double) * 6);
+        if (nd.right >= 0) {
+            nlink[4 * h] = newid[m][idx + 1];
+            nlink[4 * h + 1] = newid[m][nd.right];
+            nlink[4 * h + 2] = 0;
+            nlink[4 * h + 3] = nd.axis;
+        } else {
+            nlink[4 * h] = nd.start + static_cast<int>(leaf_off[m]);
+            nlink[4 * h + 1] = -1;
+            nlink[4 * h + 2] = nd.count;
+            nlink[4 * h + 3] = 0;
+        }
+    }
+    bbrt::DScene& D = S.dev;
+    S.member_sphere.assign(4 * static_cast<size_t>(M), 0.0);
+    double diag_max = 0.0, sag_max = 0.0;
+    int cull_block_cells = 4, cull_blocks = 0;
+    for (int m = 0; m < M; ++m) {
+        const bbrt_scene* ms = mem[m];
+        roots[m] = newid[m].empty() ? 0 : newid[m][0];
+        double* pr = &params[static_cast<size_t>(m) * bbrt::kMemberParams];
+        pr[0] = ms->host.scene_diagonal;
+        pr[1] = ms->cull.enabled ? 1.0 : 0.0;
+        pr[2] = ms->cull.a; pr[3] = ms->cull.h; pr[4] = ms->cull.b; pr[5] = ms->cull.coord; pr[6] = ms->cull.radius;
+        for (int a = 0; a < 3; ++a) pr[7 + a] = ms->cull.center[a];
+        for (int a = 0; a < 3; ++a) S.member_sphere[4 * m + a] = ms->cull.center[a];
+        S.member_sphere[4 * m + 3] = ms->cull.radius > 0.0 ? ms->cull.radius : ms->host.scene_diagonal;
+        diag_max = std::max(diag_max, ms->host.scene_diagonal);
+        sag_max = std::max(sag_max, ms->host.max_patch_sagitta);
+        if (ms->cull.enabled) {
+            cull_block_cells = ms->cull.block_cells;
+            cull_blocks = ms->cull.n_blocks_side;
+        }
+        D.max_nodes = std::max(D.max_nodes, ms->dev.max_nodes);
+    }
+    HM.scene_diagonal = diag_max;
+    HM.max_patch_sagitta = sag_max;
+    D.n_objects = HM.n_objects;
+    D.n_nodes = static_cast<int>(NN);
+    D.coarse_n = HM.coarse_n;
+    D.newton_max_iters = H0.cfg.newton_max_iters;
+    D.newton_tol = H0.cfg.newton_tol;
+    D.scene_diagonal = diag_max;
+    D.max_patch_sagitta = sag_max;
+    D.eps_factor = H0.cfg.self_intersect_eps_factor;
+    D.sag_factor = H0.cfg.sagitta_clearance_factor;
+    D.backface_tol = H0.cfg.backface_tol;
+    D.precision = mem[0]->dev.precision;
+    D.smem_nodes = static_cast<int>(std::min<size_t>(NN, 3400));
+    D.block_cells = cull_block_cells;
+    D.n_blocks_side = cull_blocks;
+    D.cull_enabled = 0;   // per member (m_param); a ray without a member never occurs in a set
+    D.n_members = M;
+    if ((rc = S.upload(nbox, D.node_box))) return rc;
+    if ((rc = S.upload(nlink, D.node_link))) return rc;
+    if ((rc = S.upload(HM.leaf_objects, D.leaf_objects))) return rc;
+    if ((rc = S.upload(HM.kind, D.obj_kind))) return rc;
+    if ((rc = S.upload(HM.sub, D.obj_sub))) return rc;
+    if ((rc = S.upload(HM.padding, D.obj_pad))) return rc;
+    if ((rc = S.upload(pdims, D.p_dims))) return rc;
+    if ((rc = S.upload(HM.p_node_off, D.p_node_off))) return rc;
+    if ((rc = S.upload(HM.p_field_off, D.p_field_off))) return rc;
+    if ((rc = S.upload(HM.coarse_uv, D.coarse_uv))) return rc;
+    if ((rc = S.upload(roots, D.m_root))) return rc;
+    if ((rc = S.upload(params, D.m_param))) return rc;
+    const int cn = HM.coarse_n, nc = cn - 1;
+    std::vector<std::pair<const double*, size_t>> pn, pf, cx, cc, tr;
+    std::vector<std::pair<const float*, size_t>> pn32, pf32, cb, bb;
+    for (int m = 0; m < M; ++m) {
+        const bbrt_scene* ms = mem[m];
+        const bbrt::DScene& Dm = ms->dev;
+        const size_t P = static_cast<size_t>(ms->host.n_patches);
+        pn.push_back({ Dm.p_nodes, ms->host.p_nodes.size() });
+        pf.push_back({ Dm.p_fields, ms->host.p_fields.size() });
+        pn32.push_back({ Dm.p_nodes32, ms->host.p_nodes.size() });
+        pf32.push_back({ Dm.p_fields32, ms->host.p_fields.size() });
+        cx.push_back({ Dm.c_xyz, P * 3 * cn * cn });
+        cc.push_back({ Dm.c_cell, P * 4 * nc * nc });
+        tr.push_back({ Dm.tri, ms->host.tri.size() });
+        const bool on = ms->cull.enabled;
+        cb.push_back({ on ? Dm.c_cell_box : nullptr, cull_blocks ? P * 6 * nc * nc : 0 });
+        bb.push_back({ on ? Dm.c_block_box : nullptr, cull_blocks ? P * 6 * cull_blocks * cull_blocks : 0 });
+    }
+    if ((rc = join_device(S, pn, D.p_nodes))) return rc;
+    if ((rc = join_device(S, pf, D.p_fields))) return rc;
+    if ((rc = join_device(S, pn32, D.p_nodes32))) return rc;
+    if ((rc = join_device(S, pf32, D.p_fields32))) return rc;
+    if ((rc = join_device(S, cx, D.c_xyz))) return rc;
+    if ((rc = join_device(S, cc, D.c_cell))) return rc;
+    if ((rc = join_device(S, tr, D.tri))) return rc;
+    if (cull_blocks) {
+        if ((rc = join_device(S, cb, D.c_cell_box))) return rc;
+        if ((rc = join_device(S, bb, D.c_block_box))) return rc;
+    }
+    BBRT_CUDA(cudaStreamSynchronize(S.stream));
+    BBRT_CUDA(S.stats.ensure(sizeof(long long) * bbrt::ST_COUNT));
+    BBRT_CUDA(S.work.ensure(sizeof(unsigned long long)));
+    S.tables_uploaded = true;
+    S.setup_on_device = true;
+    S.uploaded = true;
+    set->n_members = M;
+    BBRT_CUDA(cudaEventCreate(&set->ev[0]));
+    BBRT_CUDA(cudaEventCreate(&set->ev[1]));
+    return BBRT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+BBRT_API int bbrt_scene_set_create(const bbrt_scene_t* scenes, int n_scenes, bbrt_scene_set_t* out) {
+    if (!out) return fail(BBRT_ERR_ARG, "bbrt_scene_set_create: out is NULL");
+    *out = nullptr;
+    if (!scenes || n_scenes < 1) return fail(BBRT_ERR_ARG, "bbrt_scene_set_create: no scenes");
+    std::vector<bbrt_scene*> mem(scenes, scenes + n_scenes), sorted;
+    for (bbrt_scene* m : mem)
+        if (!m) return fail(BBRT_ERR_ARG, "bbrt_scene_set_create: NULL scene");
+    sorted = mem;
+    std::sort(sorted.begin(), sorted.end());
+    if (std::adjacent_find(sorted.begin(), sorted.end()) != sorted.end())
+        return fail(BBRT_ERR_ARG, "bbrt_scene_set_create: a scene appears twice in the set");
+    std::vector<std::unique_lock<std::mutex>> locks;
+    for (bbrt_scene* m : sorted) locks.emplace_back(m->mu);   // address order: no lock cycles
+    for (bbrt_scene* m : mem) {
+        const int rc = ensure_uploaded(m);
+        if (rc) return rc;
+    }
+    std::unique_ptr<bbrt_scene_set> set(new bbrt_scene_set());
+    int rc = BBRT_OK;
+    try {
+        rc = build_scene_set(mem, set.get());
+    } catch (const std::bad_alloc&) {
+        return fail(BBRT_ERR_NOMEM, "bbrt_scene_set_create: out of host memory");
+    }
+    if (rc) return rc;
+    *out = set.release();
+    return BBRT_OK;
+}
+
+BBRT_API void bbrt_scene_set_destroy(bbrt_scene_set_t set) { delete set; }
+
+BBRT_API int bbrt_scene_set_configure(bbrt_scene_set_t set, int precision, const bbrt_tuning* tuning) {
+    if (!set) return fail(BBRT_ERR_ARG, "bbrt_scene_set_configure: NULL set");
+    if (precision != BBRT_PREC_FP64 && precision != BBRT_PREC_SPLIT)
+        return fail(BBRT_ERR_ARG, "bbrt_scene_set_configure: unknown precision");
+    if (tuning) {
+        const int rc = bbrt_scene_set_tuning(&set->merged, tuning);
+        if (rc) return rc;
+    }
+    std::lock_guard<std::mutex> g(set->merged.mu);
+    set->merged.host.cfg.precision = precision;
+    set->merged.dev.precision = precision;
+    return BBRT_OK;
+}
+
+BBRT_API int bbrt_trace_set(bbrt_scene_set_t set, const double* const* origins, const double* const* dirs,
+                            const long long* n, int max_bounces, const bbrt_trace_out* outs,
+                            bbrt_trace_stats* stats, double* set_ms, void* stream) {
+    if (!set || !origins || !dirs || !n) return fail(BBRT_ERR_ARG, "bbrt_trace_set: NULL argument");
+    if (max_bounces < 0) return fail(BBRT_ERR_ARG, "bbrt_trace_set: max_bounces < 0");
+    const int M = set->n_members;
+    std::vector<long long> off(M + 1, 0);
+    for (int m = 0; m < M; ++m) {
+        if (n[m] < 0 || (n[m] > 0 && (!origins[m] || !dirs[m])))
+            return fail(BBRT_ERR_ARG, "bbrt_trace_set: bad rays of member " + std::to_string(m));
+        off[m + 1] = off[m] + n[m];
+    }
+    const long long N = off[M];
+    if (N >= (1LL << 31)) return fail(BBRT_ERR_UNSUPPORTED, "bbrt_trace_set: more than 2^31 - 1 rays");
+    // the outputs' shape comes from the first member with rays (members without
+    // rays may leave theirs empty)
+    int first = 0;
+    while (first < M - 1 && n[first] == 0) ++first;
+    const int K = outs ? outs[first].record_bounces : 0;
+    if (K < 0) return fail(BBRT_ERR_ARG, "bbrt_trace_set: record_bounces < 0");
+    auto same_shape = [&](const bbrt_trace_out& a, const bbrt_trace_out& b) {
+        return a.record_bounces == b.record_bounces && !a.status == !b.status && !a.bounce_count == !b.bounce_count &&
+               !a.exit_dir == !b.exit_dir && !a.end_point == !b.end_point && !a.hit_object == !b.hit_object &&
+               !a.hit_point == !b.hit_point && !a.hit_uv == !b.hit_uv && !a.err_object == !b.err_object &&
+               !a.err_value == !b.err_value && !a.ray_work == !b.ray_work;
+    };
+    if (outs)
+        for (int m = 0; m < M; ++m)
+            if (n[m] > 0 && !same_shape(outs[first], outs[m]))
+                return fail(BBRT_ERR_ARG, "bbrt_trace_set: every member must ask for the same outputs and record length");
+    bbrt_scene* s = &set->merged;
+    std::lock_guard<std::mutex> g(s->mu);
+    cudaStream_t st = pick_stream(s, stream);
+    long long hs[bbrt::ST_COUNT] = { 0 };
+    if (N == 0) {
+        if (stats) fill_stats(s, hs, 0, 0.0f, 0.0f, stats);
+        if (set_ms) *set_ms = 0.0;
+        return BBRT_OK;
+    }
+    const size_t NS = static_cast<size_t>(N), KS = static_cast<size_t>(K);
+    BBRT_CUDA(set->set_o.ensure(sizeof(double) * 3 * NS));
+    BBRT_CUDA(set->set_d.ensure(sizeof(double) * 3 * NS));
+    BBRT_CUDA(set->ray_member.ensure(sizeof(int) * NS));
+    bbrt_trace_out dev{};
+    bbrt::SetIO io;
+    if (outs) {
+        const bbrt_trace_out& o0 = outs[first];
+        dev.record_bounces = K;
+        auto bind = [&](const void* want, DevBuf& b, size_t bytes, auto*& field, auto*& io_field) -> int {
+            using T = std::remove_pointer_t<std::remove_reference_t<decltype(field)>>;
+            if (!want || bytes == 0) return BBRT_OK;
+            BBRT_CUDA(b.ensure(bytes));
+            field = static_cast<T*>(b.p);
+            io_field = static_cast<T*>(b.p);
+            return BBRT_OK;
+        };
+        int rc;
+        if ((rc = bind(o0.status, set->o_status, sizeof(int) * NS, dev.status, io.status))) return rc;
+        if ((rc = bind(o0.bounce_count, set->o_bounce, sizeof(int) * NS, dev.bounce_count, io.bounce_count))) return rc;
+        if ((rc = bind(o0.exit_dir, set->o_dir, sizeof(double) * 3 * NS, dev.exit_dir, io.exit_dir))) return rc;
+        if ((rc = bind(o0.end_point, set->o_end, sizeof(double) * 3 * NS, dev.end_point, io.end_point))) return rc;
+        if ((rc = bind(o0.hit_object, set->o_hobj, sizeof(int) * NS * KS, dev.hit_object, io.hit_object))) return rc;
+        if ((rc = bind(o0.hit_point, set->o_hpt, sizeof(double) * 3 * NS * KS, dev.hit_point, io.hit_point))) return rc;
+        if ((rc = bind(o0.hit_uv, set->o_huv, sizeof(double) * 2 * NS * KS, dev.hit_uv, io.hit_uv))) return rc;
+        if ((rc = bind(o0.err_object, set->o_eobj, sizeof(int) * NS, dev.err_object, io.err_object))) return rc;
+        if ((rc = bind(o0.err_value, set->o_eval, sizeof(double) * 2 * NS, dev.err_value, io.err_value))) return rc;
+        if ((rc = bind(o0.ray_work, set->o_work, sizeof(long long) * 4 * NS, dev.ray_work, io.ray_work))) return rc;
+    }
+    set->io.assign(M, bbrt::MemberIO());
+    for (int m = 0; m < M; ++m) {
+        bbrt::MemberIO& x = set->io[m];
+        x.o = origins[m];
+        x.d = dirs[m];
+        x.off = off[m];
+        x.n = n[m];
+        x.obj_off = set->obj_off[m];
+        if (outs) {
+            const bbrt_trace_out& om = outs[m];
+            x.status = om.status; x.bounce_count = om.bounce_count; x.exit_dir = om.exit_dir;
+            x.end_point = om.end_point; x.hit_object = om.hit_object; x.hit_point = om.hit_point;
+            x.hit_uv = om.hit_uv; x.err_object = om.err_object; x.err_value = om.err_value;
+            x.ray_work = om.ray_work;
+        }
+    }
+    BBRT_CUDA(set->io_dev.ensure(sizeof(bbrt::MemberIO) * M));
+    BBRT_CUDA(cudaEventRecord(set->ev[0], st));
+    BBRT_CUDA(cudaMemcpyAsync(set->io_dev.p, set->io.data(), sizeof(bbrt::MemberIO) * M, cudaMemcpyHostToDevice, st));
+    io.m = static_cast<const bbrt::MemberIO*>(set->io_dev.p);
+    io.n_members = M;
+    io.n = N;
+    io.K = K;
+    io.o = static_cast<double*>(set->set_o.p);
+    io.d = static_cast<double*>(set->set_d.p);
+    io.ray_member = static_cast<int*>(set->ray_member.p);
+    BBRT_CUDA(bbrt::set_gather(io, st));
+    s->member_rays = off;
+    s->ray_member = io.ray_member;
+    float kms = 0.0f;
+    int rc = run_trace_device(s, io.o, io.d, N, max_bounces, outs ? &dev : nullptr, nullptr, 1, st, stats != nullptr,
+                              hs, stats ? &kms : nullptr);
+    s->member_rays.clear();
+    s->ray_member = nullptr;
+    if (rc) return rc;
+    if (outs) BBRT_CUDA(bbrt::set_scatter(io, st));
+    BBRT_CUDA(cudaEventRecord(set->ev[1], st));
+    BBRT_CUDA(cudaEventSynchronize(set->ev[1]));
+    float tot = 0.0f;
+    BBRT_CUDA(cudaEventElapsedTime(&tot, set->ev[0], set->ev[1]));
+    if (set_ms) *set_ms = tot;
+    if (stats) fill_stats(s, hs, N, kms, tot, stats);
+    return BBRT_OK;
+}
+
+}  // extern "C"

@@ -66,7 +66,20 @@ struct DScene {
 
     // triangles
     const double* tri = nullptr;           // [n_tri][9]
+
+    // Several scenes traced as one (a scene set): the member scenes' objects,
+    // patches and BVH trees live in the arrays above side by side; member m's
+    // tree starts at node m_root[m], and its scale and cull constants are
+    // m_param[m * kMemberParams + ...] (see kMemberParams).  n_members == 0
+    // for a single scene, whose tree starts at node 0.
+    int n_members = 0;
+    const int* m_root = nullptr;
+    const double* m_param = nullptr;
 };
+
+// Per-member values of a scene set: scene diagonal, cull on (1) / off (0),
+// cull_a, cull_h, cull_b, cull_coord, cull_radius, cull_center xyz.
+constexpr int kMemberParams = 10;
 
 // Counter slots of the per-launch statistics buffer (long long each).
 enum StatSlot {
@@ -115,6 +128,8 @@ struct TraceArgs {
     // stands).  Off (0) in the plain and split forms, which keep the
     // reference's failure.
     int off_patch_miss = 0;
+    // Scene set: the member scene of every ray ([n]); null for one scene.
+    const int* ray_member = nullptr;
 };
 
 // Network outputs (u, v, t, logit) that place a confident hit well inside

@@ -128,21 +128,22 @@ __global__ void __launch_bounds__(kScanBlock) k_order_scan_add(unsigned* __restr
 }
 
 __global__ void k_order_scatter(const unsigned* __restrict__ keys, long long n, unsigned* __restrict__ cursor,
-                                int* __restrict__ order) {
+                                int* __restrict__ order, long long base) {
     const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
     if (i >= n) return;
     const unsigned pos = atomicAdd(cursor + keys[i], 1u);
-    order[pos] = static_cast<int>(i);
+    order[pos] = static_cast<int>(base + i);
 }
 
 size_t ray_order_workspace_bytes(long long n) {
     return sizeof(unsigned) * (static_cast<size_t>(n) + kOrderBuckets + kScanBlocks) + 512;
 }
 
-// order[n] receives the processing order.  `ws` holds ray_order_workspace_bytes(n).
-// entry: key on the point where each ray enters the scene's sphere (else on its origin).
+// order[n] receives the processing order (ray indices plus `base`).  `ws`
+// holds ray_order_workspace_bytes(n).  entry: key on the point where each ray
+// enters the scene's sphere (else on its origin).
 cudaError_t ray_order(const double* o, const double* d, long long n, const double center[3], double radius,
-                      void* ws, int* order, cudaStream_t stream, bool entry) {
+                      void* ws, int* order, cudaStream_t stream, bool entry, long long base) {
     if (n <= 0) return cudaSuccess;
     unsigned* hist = static_cast<unsigned*>(ws);
     unsigned* block_sums = hist + kOrderBuckets;
@@ -156,7 +157,7 @@ cudaError_t ray_order(const double* o, const double* d, long long n, const doubl
                                              entry && radius > 0.0 ? radius : 0.0, keys, hist);
     k_order_scan_local<<<kScanBlocks, kScanBlock, 0, stream>>>(hist, block_sums);
     k_order_scan_add<<<kScanBlocks, kScanBlock, 0, stream>>>(hist, block_sums);
-    k_order_scatter<<<blocks, 256, 0, stream>>>(keys, n, hist, order);
+    k_order_scatter<<<blocks, 256, 0, stream>>>(keys, n, hist, order, base);
     return cudaGetLastError();
 }
 

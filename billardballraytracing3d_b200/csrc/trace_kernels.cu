@@ -40,19 +40,31 @@ __device__ __forceinline__ bool finite3(const V3& a) {
     return isfinite(a.x) && isfinite(a.y) && isfinite(a.z);
 }
 
+// Scene values of a ray's scene: the scene itself, or member m of a scene set.
+__device__ __forceinline__ double scene_diag(const DScene& S, int m) {
+    return m < 0 ? S.scene_diagonal : S.m_param[m * kMemberParams];
+}
+__device__ __forceinline__ int root_node(const DScene& S, int m) { return m < 0 ? 0 : S.m_root[m]; }
+
 // The cull inflation bound is derived for |d| <= 1 (the trace loop always
 // normalises d); single queries with longer or non-finite rays skip culling.
-__device__ __forceinline__ bool cull_ok(const DScene& S, int cull_flag, const V3& o, const V3& d) {
-    return cull_flag && S.cull_enabled && finite3(o) && finite3(d) &&
-           d.x * d.x + d.y * d.y + d.z * d.z <= 1.0 + 1e-6;
+__device__ __forceinline__ bool cull_ok(const DScene& S, int m, int cull_flag, const V3& o, const V3& d) {
+    const bool on = m < 0 ? S.cull_enabled != 0 : S.m_param[m * kMemberParams + 1] != 0.0;
+    return cull_flag && on && finite3(o) && finite3(d) && d.x * d.x + d.y * d.y + d.z * d.z <= 1.0 + 1e-6;
 }
 
-__device__ __forceinline__ CullRay make_cull_ray(const DScene& S, const V3& o, const V3& d) {
+__device__ __forceinline__ CullRay make_cull_ray(const DScene& S, int m, const V3& o, const V3& d) {
     CullRay c;
-    const double cx = o.x - S.cull_center[0], cy = o.y - S.cull_center[1], cz = o.z - S.cull_center[2];
-    const double L = sqrt(cx * cx + cy * cy + cz * cz) + S.cull_radius;
+    double ca = S.cull_a, ch = S.cull_h, cb = S.cull_b, cc = S.cull_coord, cr = S.cull_radius;
+    double c0 = S.cull_center[0], c1 = S.cull_center[1], c2 = S.cull_center[2];
+    if (m >= 0) {
+        const double* p = S.m_param + m * kMemberParams;
+        ca = p[2]; ch = p[3]; cb = p[4]; cc = p[5]; cr = p[6]; c0 = p[7]; c1 = p[8]; c2 = p[9];
+    }
+    const double cx = o.x - c0, cy = o.y - c1, cz = o.z - c2;
+    const double L = sqrt(cx * cx + cy * cy + cz * cz) + cr;
     const double on = sqrt(o.x * o.x + o.y * o.y + o.z * o.z);
-    const double delta = S.cull_a * (L + S.cull_h) + S.cull_b * (L + on + S.cull_coord);
+    const double delta = ca * (L + ch) + cb * (L + on + cc);
     c.ox = static_cast<float>(o.x);
     c.oy = static_cast<float>(o.y);
     c.oz = static_cast<float>(o.z);
@@ -215,20 +227,20 @@ __device__ __forceinline__ int object_intersect(const DScene& S, int obj, const 
 // a miss (obj < 0, err 0), or the first Newton failure met (err != 0).
 // off_patch_miss (learned form): a Newton root outside its patch is a miss.
 __device__ QHit bvh_query(const DScene& S, const V3& o, const V3& d, int cull_flag, Counters& ctr,
-                          bool off_patch_miss = false) {
+                          bool off_patch_miss = false, int member = -1) {
     QHit best;
     best.obj = -1;
     best.err = 0;
     best.t = CUDART_INF;
     const double inv[3] = { 1.0 / d.x, 1.0 / d.y, 1.0 / d.z };
     const bool neg[3] = { inv[0] < 0.0, inv[1] < 0.0, inv[2] < 0.0 };
-    const bool use_cull = cull_ok(S, cull_flag, o, d);
+    const bool use_cull = cull_ok(S, member, cull_flag, o, d);
     CullRay cr;
-    if (use_cull) cr = make_cull_ray(S, o, d);
+    if (use_cull) cr = make_cull_ray(S, member, o, d);
     double best_t = CUDART_INF;
     int stack[64];
     int sp = 0;
-    stack[sp++] = 0;
+    stack[sp++] = root_node(S, member);
     while (sp > 0) {
         const int idx = stack[--sp];
         ++ctr.node_tests;
@@ -279,6 +291,7 @@ __device__ __forceinline__ void warp_add(long long* dst, long long v) {
 // Registers of one ray between queries.
 struct RayCtx {
     V3 o, d, end;
+    int member;      // scene-set member of the ray, -1 for a single scene
     int bounces;
     int status;      // final status once set; -1 while the ray is running
     int err_obj;
@@ -299,6 +312,7 @@ __device__ __forceinline__ void init_outputs(const TraceArgs& A, long long i) {
 __device__ __forceinline__ RayCtx start_ray(const TraceArgs& A, long long i) {
     RayCtx r;
     r.o = load3(A.origins + 3 * i);
+    r.member = A.ray_member ? A.ray_member[i] : -1;
     const V3 dir_in = load3(A.dirs + 3 * i);
     r.end = r.o;
     r.d = v3(0.0, 0.0, 0.0);
@@ -329,7 +343,8 @@ __device__ __forceinline__ bool step_ray(const DScene& S, const TraceArgs& A, lo
     }
     if (h.obj < 0) {
         r.status = BBRT_RAY_ESCAPED;
-        r.end = v3(r.o.x + r.d.x * S.scene_diagonal, r.o.y + r.d.y * S.scene_diagonal, r.o.z + r.d.z * S.scene_diagonal);
+        const double diag = scene_diag(S, r.member);
+        r.end = v3(r.o.x + r.d.x * diag, r.o.y + r.d.y * diag, r.o.z + r.d.z * diag);
         return false;
     }
     if (vdot(r.d, h.n) > S.backface_tol) { r.status = BBRT_RAY_WENT_INSIDE; return false; }
@@ -345,7 +360,7 @@ __device__ __forceinline__ bool step_ray(const DScene& S, const TraceArgs& A, lo
     const V3 d = r.d;
     const double dn = d.x * h.n.x + d.y * h.n.y + d.z * h.n.z;
     r.d = v3(d.x - 2.0 * dn * h.n.x, d.y - 2.0 * dn * h.n.y, d.z - 2.0 * dn * h.n.z);
-    const double eps = smax(S.eps_factor * S.scene_diagonal, S.sag_factor * S.obj_pad[h.obj]);
+    const double eps = smax(S.eps_factor * scene_diag(S, r.member), S.sag_factor * S.obj_pad[h.obj]);
     r.o = v3(h.p.x + r.d.x * eps, h.p.y + r.d.y * eps, h.p.z + r.d.z * eps);
     return true;
 }
@@ -365,7 +380,7 @@ __device__ __forceinline__ void run_ray(const DScene& S, const TraceArgs& A, lon
     while (r.status < 0) {
         if (r.bounces >= A.max_bounces) { r.status = BBRT_RAY_MAX_BOUNCES; break; }
         ++queries;
-        const QHit h = bvh_query(S, r.o, r.d, A.cull, ctr, A.off_patch_miss != 0);
+        const QHit h = bvh_query(S, r.o, r.d, A.cull, ctr, A.off_patch_miss != 0, r.member);
         if (!step_ray(S, A, i, r, h)) break;
     }
 }
@@ -451,8 +466,9 @@ __device__ __forceinline__ void save_ray(const WaveArgs& W, long long i, const R
     W.nres[i] = nres;
 }
 
-__device__ __forceinline__ RayCtx load_ray(const WaveArgs& W, long long i, int& nres) {
+__device__ __forceinline__ RayCtx load_ray(const TraceArgs& A, const WaveArgs& W, long long i, int& nres) {
     RayCtx r;
+    r.member = A.ray_member ? A.ray_member[i] : -1;
     r.o = load3(W.o + 3 * i);
     r.d = load3(W.d + 3 * i);
     r.end = load3(W.end + 3 * i);
@@ -722,8 +738,8 @@ __device__ __forceinline__ void adv_start_query(const DScene& S, const TraceArgs
     q.neg[0] = q.inv[0] < 0.0;
     q.neg[1] = q.inv[1] < 0.0;
     q.neg[2] = q.inv[2] < 0.0;
-    q.use_cull = cull_ok(S, A.cull, r.o, r.d);
-    if (q.use_cull) q.cr = make_cull_ray(S, r.o, r.d);
+    q.use_cull = cull_ok(S, r.member, A.cull, r.o, r.d);
+    if (q.use_cull) q.cr = make_cull_ray(S, r.member, r.o, r.d);
     q.best_t = CUDART_INF;
     q.best_ver = 0;
     q.best_obj = -1;
@@ -732,7 +748,7 @@ __device__ __forceinline__ void adv_start_query(const DScene& S, const TraceArgs
     q.err_obj = -1;
     q.ev0 = q.ev1 = 0.0;
     q.sp = 0;
-    stack[q.sp++] = stack_entry(0, kStackAlways);
+    stack[q.sp++] = stack_entry(root_node(S, r.member), kStackAlways);
 }
 
 // Keeps the traversal state of a query that suspends for a Newton solve
@@ -1175,7 +1191,7 @@ __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, Wav
                     r = start_ray(A, i);
                 } else {
                     i = W.runnable[fs].ray;
-                    r = load_ray(W, i, nres);
+                    r = load_ray(A, W, i, nres);
                 }
                 mode = M_FINISH;
                 if (r.status < 0) {
@@ -1359,7 +1375,7 @@ __global__ void __launch_bounds__(128) k_resume(DScene S, TraceArgs A, WaveArgs 
     if (slot < n) {
         const long long i = reqs ? reqs[slot].ray : rays[slot];
         int nres;
-        RayCtx r = load_ray(W, i, nres);
+        RayCtx r = load_ray(A, W, i, nres);
         run_ray(S, A, i, r, ctr, tally.queries);
         add_ray_work(A, i, ctr);
         finish_ray(A, i, r);
@@ -1382,20 +1398,20 @@ __global__ void __launch_bounds__(128) k_resume(DScene S, TraceArgs A, WaveArgs 
 // BVH::intersect for one ray with a whole warp (every lane returns the same result).
 // Nodes [0, staged) are read from the shared-memory copy (sbox, slink).
 __device__ QHit warp_bvh_query(const DScene& S, const V3& o, const V3& d, int cull_flag, int lane, Counters& ctr,
-                               const double* sbox, const int* slink, int staged, bool off_patch_miss) {
+                               const double* sbox, const int* slink, int staged, bool off_patch_miss, int member) {
     QHit best;
     best.obj = -1;
     best.err = 0;
     best.t = CUDART_INF;
     const double inv[3] = { 1.0 / d.x, 1.0 / d.y, 1.0 / d.z };
     const bool neg[3] = { inv[0] < 0.0, inv[1] < 0.0, inv[2] < 0.0 };
-    const bool use_cull = cull_ok(S, cull_flag, o, d);
+    const bool use_cull = cull_ok(S, member, cull_flag, o, d);
     CullRay cr;
-    if (use_cull) cr = make_cull_ray(S, o, d);
+    if (use_cull) cr = make_cull_ray(S, member, o, d);
     double best_t = CUDART_INF;
     int stack[64];
     int sp = 0;
-    stack[sp++] = 0;
+    stack[sp++] = root_node(S, member);
     while (sp > 0) {
         const int idx = stack[--sp];
         if (lane == 0) ++ctr.node_tests;
@@ -1488,13 +1504,13 @@ __global__ void __launch_bounds__(128, MINB) k_resume_warp(DScene S, TraceArgs A
     for (long long slot = take(warp); slot < n; slot = take(slot + n_warps)) {
         const long long i = reqs ? reqs[slot].ray : rays[slot];
         int nres;
-        RayCtx r = load_ray(W, i, nres);
+        RayCtx r = load_ray(A, W, i, nres);
         Counters c1;
         while (r.status < 0) {
             if (r.bounces >= A.max_bounces) { r.status = BBRT_RAY_MAX_BOUNCES; break; }
             if (lane == 0) ++tally.queries;
             const QHit h = warp_bvh_query(S, r.o, r.d, A.cull, lane, c1, sbox, slink, S.smem_nodes,
-                                          A.off_patch_miss != 0);
+                                          A.off_patch_miss != 0, r.member);
             if (!step_ray(S, A, i, r, h, lane == 0)) break;
         }
         if (lane == 0) {
@@ -1526,9 +1542,9 @@ __global__ void __launch_bounds__(128) k_query(DScene S, QueryArgs Q) {
     r.t = 0.0;
     r.p = r.n = v3(0.0, 0.0, 0.0);
     r.u = r.v = r.ev0 = r.ev1 = 0.0;
-    const bool use_cull = cull_ok(S, Q.cull, o, d);
+    const bool use_cull = cull_ok(S, -1, Q.cull, o, d);
     CullRay cr;
-    if (use_cull) cr = make_cull_ray(S, o, d);
+    if (use_cull) cr = make_cull_ray(S, -1, o, d);
     if (Q.mode == BBRT_QUERY_BVH) {
         r = bvh_query(S, o, d, Q.cull, ctr);
     } else if (Q.mode == BBRT_QUERY_BRUTE) {

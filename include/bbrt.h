@@ -451,6 +451,36 @@ BBRT_API int bbrt_scene_autotune(bbrt_scene_t scene, const double* origins, cons
                                  int max_bounces, int trials, bbrt_tuning* best, double* best_ms,
                                  void* stream);
 
+/* ---- several scenes in one trace: scene sets (no reference counterpart) ----
+ *
+ * Many independent scenes of uneven sizes traced as ONE wavefront: one
+ * ordering, one set of advance / Newton rounds (one CUDA graph launch with
+ * graph_rounds), one tail, however many scenes.  bbrt_scene_set_create copies
+ * the members' device arrays side by side into one device scene (objects,
+ * patch tables, coarse grids, cell data, cull boxes; the BVH trees as one
+ * forest renumbered breadth-first across the trees, so the top levels of every
+ * member share the trace kernels' shared-memory node copy); the members stay
+ * valid and independent, and may be destroyed while the set lives.  Members
+ * must share the coarse grid size, the Newton and epsilon constants, culling,
+ * precision and device (BBRT_ERR_ARG otherwise).  The set traces with the
+ * stage-1 triangle start (its members' learned networks are not used).
+ *
+ * bbrt_trace_set takes every member's rays as device arrays (origins[m],
+ * dirs[m], n[m]) and writes every member's results to outs[m] (device
+ * arrays; every member asks for the same outputs and record length) in the
+ * member's own object numbering: each member's results equal a bbrt_trace of
+ * that member alone, bit for bit.  set_ms (optional): device time of the
+ * call, from copying the rays in to copying the results out.  stream: a
+ * cudaStream_t, or NULL for the set's own stream. */
+typedef struct bbrt_scene_set* bbrt_scene_set_t;
+BBRT_API int bbrt_scene_set_create(const bbrt_scene_t* scenes, int n_scenes, bbrt_scene_set_t* out);
+BBRT_API void bbrt_scene_set_destroy(bbrt_scene_set_t set);
+/* Precision (BBRT_PREC_*) and, when tuning is not NULL, the launch schedule of the set's traces. */
+BBRT_API int bbrt_scene_set_configure(bbrt_scene_set_t set, int precision, const bbrt_tuning* tuning);
+BBRT_API int bbrt_trace_set(bbrt_scene_set_t set, const double* const* origins, const double* const* dirs,
+                            const long long* n, int max_bounces, const bbrt_trace_out* outs,
+                            bbrt_trace_stats* stats, double* set_ms, void* stream);
+
 /* ---- diagnostics ------------------------------------------------------ */
 enum {
     BBRT_PIPE_FP64 = 0,   /* FP64 FMA throughput, TFLOP/s (2 FLOP per FMA) */
