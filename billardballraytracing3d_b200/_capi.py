@@ -300,7 +300,10 @@ def _declare(lib):
     lib.bbrt_scene_set_create.argtypes = [ctypes.POINTER(V), I, ctypes.POINTER(V)]
     lib.bbrt_scene_set_destroy.argtypes = [V]
     lib.bbrt_scene_set_destroy.restype = None
-    lib.bbrt_scene_set_configure.argtypes = [V, I, ctypes.POINTER(Tuning)]
+    lib.bbrt_scene_set_configure.argtypes = [V, I, I, ctypes.POINTER(Tuning)]
+    lib.bbrt_scene_set_guess_train.argtypes = [V, ctypes.POINTER(V), ctypes.POINTER(V), c_ll_p, I,
+                                               ctypes.POINTER(GuessTrainConfig), ctypes.POINTER(GuessTrainReport)]
+    lib.bbrt_scene_set_guess_export.argtypes = [V, I, V]
     lib.bbrt_trace_set.argtypes = [V, ctypes.POINTER(V), ctypes.POINTER(V), c_ll_p, I, ctypes.POINTER(TraceOut),
                                    ctypes.POINTER(TraceStats), c_double_p, V]
     lib.bbrt_scene_get_tuning.argtypes = [V, ctypes.POINTER(Tuning)]

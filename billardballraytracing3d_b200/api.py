@@ -321,14 +321,36 @@ class SceneSet:
         C.check(self.lib, self.lib.bbrt_scene_set_create(hs, self.k, ctypes.byref(h)), "bbrt_scene_set_create")
         self.h = h
 
-    def configure(self, precision: int = C.PREC_FP64, **tuning):
+    def configure(self, precision: int = C.PREC_FP64, guess: int = C.GUESS_TRIANGLE, **tuning):
         t = None
         if tuning:
             t = C.Tuning()
             for k, v in tuning.items():
                 setattr(t, k, v)
-        C.check(self.lib, self.lib.bbrt_scene_set_configure(self.h, int(precision), ctypes.byref(t) if t else None),
-                "bbrt_scene_set_configure")
+        C.check(self.lib, self.lib.bbrt_scene_set_configure(self.h, int(precision), int(guess),
+                                                            ctypes.byref(t) if t else None), "bbrt_scene_set_configure")
+
+    def guess_train(self, origins, dirs, max_bounces: int, **kw) -> Dict:
+        """One network for every member (host ray arrays per member), trained on the GPU."""
+        os_ = [np.ascontiguousarray(o, dtype=np.float64).reshape(-1, 3) for o in origins]
+        ds_ = [np.ascontiguousarray(d, dtype=np.float64).reshape(-1, 3) for d in dirs]
+        k = self.k
+        op = (ctypes.c_void_p * k)(*[ctypes.c_void_p(a.ctypes.data) for a in os_])
+        dp = (ctypes.c_void_p * k)(*[ctypes.c_void_p(a.ctypes.data) for a in ds_])
+        nn = (ctypes.c_longlong * k)(*[a.shape[0] for a in os_])
+        cfg = C.GuessTrainConfig()
+        self.lib.bbrt_guess_train_config_init(ctypes.byref(cfg))
+        for key, v in kw.items():
+            setattr(cfg, key, v)
+        rep = C.GuessTrainReport()
+        C.check(self.lib, self.lib.bbrt_scene_set_guess_train(self.h, op, dp, nn, int(max_bounces), ctypes.byref(cfg),
+                                                              ctypes.byref(rep)), "bbrt_scene_set_guess_train")
+        return {key: getattr(rep, key) for key, _ in rep._fields_}
+
+    def guess_export(self, member: int, scene: "Scene"):
+        """Member `member`'s share of the set's network into `scene`."""
+        C.check(self.lib, self.lib.bbrt_scene_set_guess_export(self.h, int(member), scene.h),
+                "bbrt_scene_set_guess_export")
 
     def trace_device(self, origin_ptrs, dir_ptrs, ns, max_bounces: int, outs=None, want_stats: bool = True,
                      stream: int = 0):

@@ -2015,6 +2015,11 @@ BBRT_API int bbrt_guess_params(bbrt_scene_t s, float* params, long long n, int s
     return BBRT_OK;
 }
 
+namespace {
+int guess_train_core(bbrt_scene* s, const double* d_o, const double* d_d, long long n, int max_bounces,
+                     const bbrt_guess_train_config& cfg, bbrt_guess_train_report* rep, cudaStream_t st);
+}  // namespace
+
 BBRT_API int bbrt_guess_train(bbrt_scene_t s, const double* origins, const double* dirs, long long n, int max_bounces,
                               const bbrt_guess_train_config* cfg_in, bbrt_guess_train_report* rep, void* stream) {
     if (!s || !origins || !dirs) return fail(BBRT_ERR_ARG, "bbrt_guess_train: NULL argument");
@@ -2030,16 +2035,27 @@ BBRT_API int bbrt_guess_train(bbrt_scene_t s, const double* origins, const doubl
     if (rc) return rc;
     if (s->host.n_patches == 0) return fail(BBRT_ERR_ARG, "bbrt_guess_train: the scene has no patches");
     cudaStream_t st = pick_stream(s, stream);
+    BBRT_CUDA(s->in_o.ensure(sizeof(double) * 3 * n));
+    BBRT_CUDA(s->in_d.ensure(sizeof(double) * 3 * n));
+    BBRT_CUDA(cudaMemcpyAsync(s->in_o.p, origins, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, st));
+    BBRT_CUDA(cudaMemcpyAsync(s->in_d.p, dirs, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, st));
+    return guess_train_core(s, static_cast<const double*>(s->in_o.p), static_cast<const double*>(s->in_d.p), n,
+                            max_bounces, cfg, rep, st);
+}
+
+namespace {
+
+// The training of bbrt_guess_train on device rays (scene locked and on the
+// device): samples from a plain FP64 trace of the rays, then Adam epochs.
+int guess_train_core(bbrt_scene* s, const double* d_o, const double* d_d, long long n, int max_bounces,
+                     const bbrt_guess_train_config& cfg, bbrt_guess_train_report* rep, cudaStream_t st) {
+    int rc = BBRT_OK;
     // ---- 1. samples from a plain FP64 trace of the rays
     const long long cap_p = cfg.max_positive, cap_n = cfg.max_negative;
     DevBuf samples, counters, rows;
     BBRT_CUDA(samples.ensure(sizeof(bbrt::GuessSample) * static_cast<size_t>(cap_p + cap_n)));
     BBRT_CUDA(counters.ensure(2 * sizeof(unsigned long long)));
     BBRT_CUDA(cudaMemsetAsync(counters.p, 0, 2 * sizeof(unsigned long long), st));
-    BBRT_CUDA(s->in_o.ensure(sizeof(double) * 3 * n));
-    BBRT_CUDA(s->in_d.ensure(sizeof(double) * 3 * n));
-    BBRT_CUDA(cudaMemcpyAsync(s->in_o.p, origins, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, st));
-    BBRT_CUDA(cudaMemcpyAsync(s->in_d.p, dirs, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, st));
     const int save_prec = s->dev.precision, save_guess = s->host.cfg.guess;
     s->dev.precision = BBRT_PREC_FP64;
     s->host.cfg.guess = BBRT_GUESS_TRIANGLE;
@@ -2048,8 +2064,7 @@ BBRT_API int bbrt_guess_train(bbrt_scene_t s, const double* origins, const doubl
     s->rec_cap_pos = cap_p;
     s->rec_cap_neg = cap_n;
     float collect_ms = 0.0f;
-    rc = run_trace_device(s, static_cast<const double*>(s->in_o.p), static_cast<const double*>(s->in_d.p), n,
-                          max_bounces, nullptr, nullptr, 1, st, false, nullptr, &collect_ms);
+    rc = run_trace_device(s, d_o, d_d, n, max_bounces, nullptr, nullptr, 1, st, false, nullptr, &collect_ms);
     s->rec_samples = nullptr;
     s->rec_count = nullptr;
     s->dev.precision = save_prec;
@@ -2148,8 +2163,6 @@ BBRT_API int bbrt_guess_train(bbrt_scene_t s, const double* origins, const doubl
     }
     return BBRT_OK;
 }
-
-namespace {
 
 // Standalone network buffers for the check entry points.
 struct CheckNet {
@@ -2506,6 +2519,7 @@ struct bbrt_scene_set {
     bbrt_scene merged;
     int n_members = 0;
     std::vector<int> obj_off;              // [M + 1]
+    std::vector<long long> patch_off;      // [M + 1]
     std::vector<bbrt::MemberIO> io;        // per-call member table (host copy of io_dev)
     DevBuf io_dev, ray_member, set_o, set_d, o_status, o_bounce, o_dir, o_end, o_hobj, o_hpt, o_huv, o_eobj,
         o_eval, o_work;
@@ -2583,6 +2597,7 @@ int build_scene_set(const std::vector<bbrt_scene*>& mem, bbrt_scene_set* set) {
     HM.n_objects = static_cast<int>(obj_off[M]);
     HM.n_patches = static_cast<int>(patch_off[M]);
     set->obj_off.assign(obj_off.begin(), obj_off.end());
+    set->patch_off = patch_off;
     std::vector<int> pdims;
     for (int m = 0; m < M; ++m) {
         const bbrt::HostScene& H = mem[m]->host;
@@ -2690,6 +2705,15 @@ int build_scene_set(const std::vector<bbrt_scene*>& mem, bbrt_scene_set* set) {
     if ((rc = S.upload(HM.coarse_uv, D.coarse_uv))) return rc;
     if ((rc = S.upload(roots, D.m_root))) return rc;
     if ((rc = S.upload(params, D.m_param))) return rc;
+    {
+        // the learned guess's patch frames, member after member
+        std::vector<double> fr;
+        for (int m = 0; m < M; ++m) {
+            const std::vector<double> f = patch_frames(mem[m]->host);
+            fr.insert(fr.end(), f.begin(), f.end());
+        }
+        if ((rc = S.upload(fr, S.guess.frame))) return rc;
+    }
     const int cn = HM.coarse_n, nc = cn - 1;
     std::vector<std::pair<const double*, size_t>> pn, pf, cx, cc, tr;
     std::vector<std::pair<const float*, size_t>> pn32, pf32, cb, bb;
@@ -2766,17 +2790,101 @@ BBRT_API int bbrt_scene_set_create(const bbrt_scene_t* scenes, int n_scenes, bbr
 
 BBRT_API void bbrt_scene_set_destroy(bbrt_scene_set_t set) { delete set; }
 
-BBRT_API int bbrt_scene_set_configure(bbrt_scene_set_t set, int precision, const bbrt_tuning* tuning) {
+BBRT_API int bbrt_scene_set_configure(bbrt_scene_set_t set, int precision, int guess, const bbrt_tuning* tuning) {
     if (!set) return fail(BBRT_ERR_ARG, "bbrt_scene_set_configure: NULL set");
     if (precision != BBRT_PREC_FP64 && precision != BBRT_PREC_SPLIT)
         return fail(BBRT_ERR_ARG, "bbrt_scene_set_configure: unknown precision");
+    if (guess != BBRT_GUESS_TRIANGLE && guess != BBRT_GUESS_LEARNED)
+        return fail(BBRT_ERR_ARG, "bbrt_scene_set_configure: unknown guess");
     if (tuning) {
         const int rc = bbrt_scene_set_tuning(&set->merged, tuning);
         if (rc) return rc;
     }
     std::lock_guard<std::mutex> g(set->merged.mu);
+    if (guess == BBRT_GUESS_LEARNED && !set->merged.guess.trained)
+        return fail(BBRT_ERR_STATE, "bbrt_scene_set_configure: the set has no trained network (bbrt_scene_set_guess_train)");
     set->merged.host.cfg.precision = precision;
     set->merged.dev.precision = precision;
+    set->merged.host.cfg.guess = guess;
+    return BBRT_OK;
+}
+
+BBRT_API int bbrt_scene_set_guess_train(bbrt_scene_set_t set, const double* const* origins, const double* const* dirs,
+                                        const long long* n, int max_bounces, const bbrt_guess_train_config* cfg_in,
+                                        bbrt_guess_train_report* rep) {
+    if (!set || !origins || !dirs || !n) return fail(BBRT_ERR_ARG, "bbrt_scene_set_guess_train: NULL argument");
+    if (max_bounces < 0) return fail(BBRT_ERR_ARG, "bbrt_scene_set_guess_train: max_bounces < 0");
+    bbrt_guess_train_config cfg;
+    bbrt_guess_train_config_init(&cfg);
+    if (cfg_in) cfg = *cfg_in;
+    if (cfg.epochs < 1 || cfg.batch < 128 || cfg.max_positive < 1 || cfg.max_negative < 0 || !(cfg.lr > 0.0f))
+        return fail(BBRT_ERR_ARG, "bbrt_scene_set_guess_train: bad training configuration");
+    const int M = set->n_members;
+    std::vector<long long> off(M + 1, 0);
+    for (int m = 0; m < M; ++m) {
+        if (n[m] < 0 || (n[m] > 0 && (!origins[m] || !dirs[m])))
+            return fail(BBRT_ERR_ARG, "bbrt_scene_set_guess_train: bad rays of member " + std::to_string(m));
+        off[m + 1] = off[m] + n[m];
+    }
+    const long long N = off[M];
+    if (N <= 0) return fail(BBRT_ERR_ARG, "bbrt_scene_set_guess_train: no rays");
+    if (N >= (1LL << 31)) return fail(BBRT_ERR_UNSUPPORTED, "bbrt_scene_set_guess_train: more than 2^31 - 1 rays");
+    bbrt_scene* s = &set->merged;
+    std::lock_guard<std::mutex> g(s->mu);
+    cudaStream_t st = s->stream;
+    BBRT_CUDA(set->set_o.ensure(sizeof(double) * 3 * static_cast<size_t>(N)));
+    BBRT_CUDA(set->set_d.ensure(sizeof(double) * 3 * static_cast<size_t>(N)));
+    BBRT_CUDA(set->ray_member.ensure(sizeof(int) * static_cast<size_t>(N)));
+    double* so = static_cast<double*>(set->set_o.p);
+    double* sd = static_cast<double*>(set->set_d.p);
+    set->io.assign(M, bbrt::MemberIO());
+    for (int m = 0; m < M; ++m) {
+        set->io[m].off = off[m];
+        set->io[m].n = n[m];
+        set->io[m].obj_off = set->obj_off[m];
+        if (n[m] == 0) continue;
+        BBRT_CUDA(cudaMemcpyAsync(so + 3 * off[m], origins[m], sizeof(double) * 3 * n[m], cudaMemcpyHostToDevice, st));
+        BBRT_CUDA(cudaMemcpyAsync(sd + 3 * off[m], dirs[m], sizeof(double) * 3 * n[m], cudaMemcpyHostToDevice, st));
+    }
+    BBRT_CUDA(set->io_dev.ensure(sizeof(bbrt::MemberIO) * M));
+    BBRT_CUDA(cudaMemcpyAsync(set->io_dev.p, set->io.data(), sizeof(bbrt::MemberIO) * M, cudaMemcpyHostToDevice, st));
+    bbrt::SetIO io;
+    io.m = static_cast<const bbrt::MemberIO*>(set->io_dev.p);
+    io.n_members = M;
+    io.n = N;
+    io.ray_member = static_cast<int*>(set->ray_member.p);
+    BBRT_CUDA(bbrt::set_members(io, st));
+    BBRT_CUDA(cudaStreamSynchronize(st));   // the host copies of the rays and the table outlive the uploads
+    s->member_rays = off;
+    s->ray_member = io.ray_member;
+    const int rc = guess_train_core(s, so, sd, N, max_bounces, cfg, rep, st);
+    s->member_rays.clear();
+    s->ray_member = nullptr;
+    return rc;
+}
+
+BBRT_API int bbrt_scene_set_guess_export(bbrt_scene_set_t set, int member, bbrt_scene_t scene) {
+    if (!set || !scene) return fail(BBRT_ERR_ARG, "bbrt_scene_set_guess_export: NULL argument");
+    if (member < 0 || member >= set->n_members) return fail(BBRT_ERR_ARG, "bbrt_scene_set_guess_export: no such member");
+    const long long np_member = set->patch_off[member + 1] - set->patch_off[member];
+    if (scene->host.n_patches != np_member)
+        return fail(BBRT_ERR_ARG, "bbrt_scene_set_guess_export: the scene's patch count is not the member's");
+    std::vector<float> P;
+    {
+        bbrt_scene* s = &set->merged;
+        std::lock_guard<std::mutex> g(s->mu);
+        if (!s->guess.trained) return fail(BBRT_ERR_STATE, "bbrt_scene_set_guess_export: the set has no trained network");
+        P.resize(static_cast<size_t>(bbrt::oE + bbrt::kEmb * np_member));
+        BBRT_CUDA(cudaMemcpy(P.data(), s->guess.P.p, sizeof(float) * bbrt::oE, cudaMemcpyDeviceToHost));
+        BBRT_CUDA(cudaMemcpy(P.data() + bbrt::oE,
+                             static_cast<const float*>(s->guess.P.p) + bbrt::oE + bbrt::kEmb * set->patch_off[member],
+                             sizeof(float) * bbrt::kEmb * np_member, cudaMemcpyDeviceToHost));
+    }
+    const int rc = bbrt_guess_params(scene, P.data(), static_cast<long long>(P.size()), 1);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> g(scene->mu);
+    scene->guess.min_logit = set->merged.guess.min_logit;
+    scene->guess.t_window = set->merged.guess.t_window;
     return BBRT_OK;
 }
 

@@ -32,6 +32,12 @@ __global__ void k_set_gather(SetIO io) {
     io.ray_member[i] = k;
 }
 
+__global__ void k_set_members(SetIO io) {
+    const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (i >= io.n) return;
+    io.ray_member[i] = member_of(io.m, io.n_members, i);
+}
+
 __global__ void k_set_scatter(SetIO io) {
     const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
     if (i >= io.n) return;
@@ -62,6 +68,12 @@ __global__ void k_set_scatter(SetIO io) {
 cudaError_t set_gather(const SetIO& io, cudaStream_t st) {
     if (io.n <= 0) return cudaSuccess;
     k_set_gather<<<static_cast<unsigned>((io.n + 255) / 256), 256, 0, st>>>(io);
+    return cudaGetLastError();
+}
+
+cudaError_t set_members(const SetIO& io, cudaStream_t st) {
+    if (io.n <= 0) return cudaSuccess;
+    k_set_members<<<static_cast<unsigned>((io.n + 255) / 256), 256, 0, st>>>(io);
     return cudaGetLastError();
 }
 

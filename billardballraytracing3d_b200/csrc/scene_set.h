@@ -48,6 +48,8 @@ struct SetIO {
 
 // Copies every member's rays into the set's arrays and records each ray's member.
 cudaError_t set_gather(const SetIO& io, cudaStream_t st);
+// Records each set ray's member only (the rays are already in place).
+cudaError_t set_members(const SetIO& io, cudaStream_t st);
 // Copies the set's per-ray results to every member's outputs; object indices
 // (hit and error objects) go back to the member's own numbering.
 cudaError_t set_scatter(const SetIO& io, cudaStream_t st);

@@ -462,8 +462,9 @@ BBRT_API int bbrt_scene_autotune(bbrt_scene_t scene, const double* origins, cons
  * member share the trace kernels' shared-memory node copy); the members stay
  * valid and independent, and may be destroyed while the set lives.  Members
  * must share the coarse grid size, the Newton and epsilon constants, culling,
- * precision and device (BBRT_ERR_ARG otherwise).  The set traces with the
- * stage-1 triangle start (its members' learned networks are not used).
+ * precision and device (BBRT_ERR_ARG otherwise).  The set's Newton start is
+ * the stage-1 triangle unless the set is configured for its own learned
+ * network (the members' networks are not used).
  *
  * bbrt_trace_set takes every member's rays as device arrays (origins[m],
  * dirs[m], n[m]) and writes every member's results to outs[m] (device
@@ -475,8 +476,21 @@ BBRT_API int bbrt_scene_autotune(bbrt_scene_t scene, const double* origins, cons
 typedef struct bbrt_scene_set* bbrt_scene_set_t;
 BBRT_API int bbrt_scene_set_create(const bbrt_scene_t* scenes, int n_scenes, bbrt_scene_set_t* out);
 BBRT_API void bbrt_scene_set_destroy(bbrt_scene_set_t set);
-/* Precision (BBRT_PREC_*) and, when tuning is not NULL, the launch schedule of the set's traces. */
-BBRT_API int bbrt_scene_set_configure(bbrt_scene_set_t set, int precision, const bbrt_tuning* tuning);
+/* Precision (BBRT_PREC_*), Newton start (BBRT_GUESS_*; LEARNED needs the
+ * set's own network, bbrt_scene_set_guess_train) and, when tuning is not
+ * NULL, the launch schedule of the set's traces. */
+BBRT_API int bbrt_scene_set_configure(bbrt_scene_set_t set, int precision, int guess, const bbrt_tuning* tuning);
+/* One learned-guess network for the whole set (shared weights, one embedding
+ * per patch of every member), trained like bbrt_guess_train on samples that a
+ * plain FP64 trace of every member's rays (HOST arrays) records: the network
+ * of several scenes at once.  bbrt_scene_set_guess_export gives member
+ * `member`'s share (the weights and its patches' embeddings) to `scene`, a
+ * scene with the member's patches (e.g. the member itself), which then traces
+ * its learned form with it. */
+BBRT_API int bbrt_scene_set_guess_train(bbrt_scene_set_t set, const double* const* origins, const double* const* dirs,
+                                        const long long* n, int max_bounces, const bbrt_guess_train_config* cfg,
+                                        bbrt_guess_train_report* report);
+BBRT_API int bbrt_scene_set_guess_export(bbrt_scene_set_t set, int member, bbrt_scene_t scene);
 BBRT_API int bbrt_trace_set(bbrt_scene_set_t set, const double* const* origins, const double* const* dirs,
                             const long long* n, int max_bounces, const bbrt_trace_out* outs,
                             bbrt_trace_stats* stats, double* set_ms, void* stream);

@@ -56,7 +56,7 @@ def test_scene_set_equals_each_scene_alone(built, schedule):
     if schedule:
         t = scs[0].tuning()
         t.update(schedule)
-        ss.configure(C.PREC_FP64, **t)
+        ss.configure(C.PREC_FP64, C.GUESS_TRIANGLE, **t)
     tens, outs = _device_io(torch, work, K)
     for call in range(2):   # the second call reuses the captured graph
         for t in tens:
@@ -111,3 +111,45 @@ def test_scene_set_rejects_mismatched_members(built):
     assert b"must share the coarse grid size" in lib.bbrt_last_error()
     hs = (ctypes.c_void_p * 2)(a.h, a.h)
     assert lib.bbrt_scene_set_create(hs, 2, ctypes.byref(h)) == C.BBRT_ERR_ARG
+
+
+def test_scene_set_learned_network_of_two_scenes(built):
+    """One network trained on the four-sphere and the ellipsoid scenes
+    together (a set of the two): the set's learned form agrees with the plain
+    form on >= 99.9% of each member's rays within 1e-10, and each member,
+    given its share of the network, traces its learned form exactly as the set
+    traced that member."""
+    import torch
+    tet = api.Scene(scenes.scene_tetra_spheres(), config=C.default_config(coarse_grid_n=17, newton_tol=1e-12))
+    ell = api.Scene(scenes.scene_ellipsoids(), config=C.default_config(coarse_grid_n=17, newton_tol=1e-12))
+    ss = api.SceneSet([tet, ell])
+    src = [(5.0, 3.0, 10.0), (8.0, 6.0, 20.0)]
+    train = [scenes.cone_rays(200000, 99 + j, *src[j]) for j in range(2)]
+    rep = ss.guess_train([t[0] for t in train], [t[1] for t in train], 100, epochs=4)
+    assert rep["positives"] > 50000 and rep["last_loss"] < rep["first_loss"]
+    rays = [scenes.cone_rays(65536, 1234 + j, *src[j]) for j in range(2)]
+    K = 100   # every bounce recorded
+    runs = {}
+    for name, guess in (("plain", C.GUESS_TRIANGLE), ("learned", C.GUESS_LEARNED)):
+        ss.configure(C.PREC_SPLIT if guess == C.GUESS_LEARNED else C.PREC_FP64, guess, wave_tail=1024,
+                     **{k: v for k, v in tet.tuning().items() if k != "wave_tail"})
+        work = [(None, o, d, 100, 17, 1e-12) for o, d in rays]
+        tens, outs = _device_io(torch, work, K)
+        st, _ = ss.trace_device([t["o"].data_ptr() for t in tens], [t["d"].data_ptr() for t in tens],
+                                [o.shape[0] for o, _ in rays], 100, outs)
+        torch.cuda.synchronize()
+        runs[name] = [{k: t[k].cpu().numpy() for k in OUTS} for t in tens]
+        if guess == C.GUESS_LEARNED:
+            assert st["guess_used"] > 0
+    for j in range(2):
+        assert int(runs["plain"][j]["bounce_count"].max()) <= K
+        cmp = api.compare_traces(runs["plain"][j], runs["learned"][j], rays[j][0])
+        assert cmp["sequence_agreement"] >= 0.999 and cmp["agreement_within_bound"] >= 0.999, (j, cmp)
+        assert cmp["max_hit_err_non_grazing"] <= 1e-10, (j, cmp)
+    for j, sc in enumerate((tet, ell)):
+        ss.guess_export(j, sc)
+        sc.set_modes(C.PREC_SPLIT, C.GUESS_LEARNED)
+        sc.tuning(wave_tail=1024)
+        alone = sc.trace(rays[j][0], rays[j][1], 100, record=K, outputs=tuple(OUTS))
+        for k in OUTS:
+            assert np.array_equal(alone[k], runs["learned"][j][k]), (j, k)
