@@ -62,11 +62,14 @@ def parse():
     ap.add_argument("--cull", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=8.0, help="target wall time of the CPU sample")
-    ap.add_argument("--train-rays", type=int, default=1 << 20, help="rays traced to record training samples")
-    ap.add_argument("--train-epochs", type=int, default=20)
+    ap.add_argument("--train-rays", type=int, default=16 << 20,
+                    help="rays of each scene traced to record training samples")
+    ap.add_argument("--train-epochs", type=int, default=6)
+    ap.add_argument("--train-positives", type=int, default=16 << 20, help="converged Newton solves kept for training")
+    ap.add_argument("--train-negatives", type=int, default=4 << 20, help="stage-1 misses kept for training")
     ap.add_argument("--accuracy-rays", type=int, default=262144, help="0 skips the accuracy comparison")
     ap.add_argument("--autotune", type=int, default=1, help="pick the launch schedule on the workload first")
-    ap.add_argument("--multi-scene", type=int, default=0,
+    ap.add_argument("--multi-scene", type=int, default=64,
                     help="also time K uneven scenes traced together (bbrt_trace_batch) vs one after another")
     ap.add_argument("--forms", default="plain,split,learned",
                     help="forms to time besides the headline (learned); e.g. 'learned' alone for profiling")
@@ -416,8 +419,31 @@ def run_ours(args, rank, world, local_rank):
     # launch schedule picked on the workload itself (plain form; results do not depend on it)
     tuned = scene.autotune(o, d, maxb, trials=2) if args.autotune else scene.tuning()
     # the learned guess: trained on this GPU on a separately seeded ray set of the same source
-    train_o, train_d = scenes.cone_rays(args.train_rays, 99 + rank, *TRAIN_SOURCE.get(args.workload, (5.0, 3.0, 10.0)))
-    training = scene.guess_train(train_o, train_d, maxb, epochs=args.train_epochs)
+    # the learned guess: trained on this GPU by the project's own kernels on
+    # samples that a plain trace of separately seeded rays records; with a
+    # second workload, one network for both scenes (a scene set of the two),
+    # each scene then given its share
+    second = None
+    train_src = TRAIN_SOURCE.get(args.workload, (5.0, 3.0, 10.0))
+    train_o, train_d = scenes.cone_rays(args.train_rays, 99 + rank, *train_src)
+    tcfg = dict(epochs=args.train_epochs, max_positive=args.train_positives, max_negative=args.train_negatives)
+    if args.second:
+        s_patches, s_o, s_d, s_maxb, s_cn, s_tol = scenes.workload(args.second, args.second_rays)
+        s_scene = api.Scene(s_patches, config=C.default_config(coarse_grid_n=s_cn, newton_tol=s_tol, cull=args.cull))
+        s_scene.upload()
+        s_to, s_td = scenes.cone_rays(args.train_rays, 199 + rank, *TRAIN_SOURCE.get(args.second, (5.0, 3.0, 10.0)))
+        pair = api.SceneSet([scene, s_scene])
+        training = pair.guess_train([train_o, s_to], [train_d, s_td], max(maxb, s_maxb), **tcfg)
+        training["scenes"] = [args.workload, args.second]
+        training["rays_per_scene"] = int(args.train_rays)
+        pair.guess_export(0, scene)
+        pair.guess_export(1, s_scene)
+        pair.close()
+        del s_to, s_td
+        second = (s_scene, s_o, s_d, s_maxb, s_cn, s_tol, training)
+    else:
+        training = scene.guess_train(train_o, train_d, maxb, **tcfg)
+    del train_o, train_d
 
     to = torch.from_numpy(np.ascontiguousarray(o)).to(dev)
     td = torch.from_numpy(np.ascontiguousarray(d)).to(dev)
@@ -513,30 +539,25 @@ def run_ours(args, rank, world, local_rank):
             "wall_s_timed_region": wall,
             "counters_per_step": {k: v for k, v in (stats or {}).items() if k not in ("kernel_ms", "total_ms")}}
     if args.second:
-        line["second_workload"] = second_workload(args, dev, stream, flush)
-    if args.multi_scene > 0:
+        line["second_workload"] = second_workload(args, second, dev, stream, flush)
+    if args.multi_scene > 0 and world == 1:
         line["multi_scene"] = multi_scene(args.multi_scene, args.steps, dev)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(patches, o, d, maxb, cn, tol, args.cpu_seconds)
     print(json.dumps(line), flush=True)
 
 
-def second_workload(args, dev, stream, flush):
+def second_workload(args, second, dev, stream, flush):
     """The second workload (default: the random-ellipsoid scene, 16 ellipsoids
     x 384 patches, 4,194,304 rays in a 20-degree cone, <= 100 bounces) traced
-    in the plain FP64 form, the split form and the learned-guess form (network
-    trained on this GPU on a separately seeded ray set of the same source),
-    each timed like the headline; with Newton failure rates, Newton iterations
-    per hit, and the learned form's accuracy against the plain one."""
+    in the plain FP64 form, the split form and the learned-guess form (the
+    network trained for both scenes together), each timed like the headline;
+    with Newton failure rates, Newton iterations per hit, and the learned
+    form's accuracy against the plain one."""
     import torch
     from billardballraytracing3d_b200 import _capi as C
-    from billardballraytracing3d_b200 import api, scenes
-    patches, o, d, maxb, cn, tol = scenes.workload(args.second, args.second_rays)
+    sc, o, d, maxb, cn, tol, training = second
     n = o.shape[0]
-    sc = api.Scene(patches, config=C.default_config(coarse_grid_n=cn, newton_tol=tol, cull=args.cull))
-    sc.upload()
-    train_o, train_d = scenes.cone_rays(args.train_rays, 99, *TRAIN_SOURCE.get(args.second, (5.0, 3.0, 10.0)))
-    training = sc.guess_train(train_o, train_d, maxb, epochs=args.train_epochs)
     to = torch.from_numpy(np.ascontiguousarray(o)).to(dev)
     td = torch.from_numpy(np.ascontiguousarray(d)).to(dev)
     st_ = torch.empty(n, dtype=torch.int32, device=dev)
@@ -558,7 +579,7 @@ def second_workload(args, dev, stream, flush):
         acc = _accuracy(sc, o[:m], d[:m], maxb, C)
     sc.set_modes(C.PREC_FP64, C.GUESS_TRIANGLE)
     return {"config": workload_config(args.second, n, maxb, cn, tol), "steps": steps, "warmup": warmup,
-            "forms": forms, "accuracy": acc, "guess_training": training,
+            "forms": forms, "accuracy": acc, "guess_training": "the headline's (one network for both scenes)",
             "note": "device time per step (CUDA events, L2 flushed before each step), default launch schedule; "
                     "newton_failure_rate = rays failed by Newton / rays; newton_iters_per_hit = FP32 + FP64 "
                     "Newton iterations / ray-bounces"}
@@ -570,7 +591,8 @@ def multi_scene(k, steps, dev):
     <= 100 bounces, plain FP64): device time of tracing them as one scene set
     (bbrt_trace_set: one wavefront for all), together on their own streams
     (bbrt_trace_batch), and one after another; best of `steps` after a warm-up
-    each.  Also the wall time of building the scenes (per-patch set-up on the
+    each; and the set's learned form (one network for all scenes, trained on
+    this GPU) against its plain one.  Also the wall time of building the scenes (per-patch set-up on the
     GPU) and of building the set."""
     import torch
     from billardballraytracing3d_b200 import _capi as C
@@ -601,6 +623,17 @@ def multi_scene(k, steps, dev):
     bounces = st["bounces"]
     set_ms = min(ss.trace_device(optr, dptr, ns, 100, outs, want_stats=False)[1] for _ in range(steps))
     set_bc = [t["bounce_count"].clone() for t in tens]
+    # the learned form of the set: one network for all 64 scenes, trained on
+    # separately seeded rays of every scene's source
+    train = [scenes.cone_rays(min(n, 1 << 17), 7000 + j, 8.0, 6.0, 20.0) for j, n in enumerate(ns)]
+    set_training = ss.guess_train([t[0] for t in train], [t[1] for t in train], 100, epochs=4)
+    del train
+    ss.configure(C.PREC_SPLIT, C.GUESS_LEARNED)
+    lst, _ = ss.trace_device(optr, dptr, ns, 100, outs)   # warm-up (graph capture)
+    ss.trace_device(optr, dptr, ns, 100, outs, want_stats=False)
+    learned_ms = min(ss.trace_device(optr, dptr, ns, 100, outs, want_stats=False)[1] for _ in range(steps))
+    agree = float(sum(int((a == t["bounce_count"]).sum().item()) for a, t in zip(set_bc, tens)) / sum(ns))
+    ss.configure(C.PREC_FP64, C.GUESS_TRIANGLE)
     api.trace_batch_device(scs, optr, dptr, ns, 100, outs)   # warm-up
     batch = min(api.trace_batch_device(scs, optr, dptr, ns, 100, outs, want_stats=False)[1] for _ in range(steps))
     same = all(torch.equal(a, t["bounce_count"]) for a, t in zip(set_bc, tens))
@@ -614,6 +647,10 @@ def multi_scene(k, steps, dev):
             "sequential_value": bounces / (seq / 1e3), "unit": UNIT,
             "set_over_sequential": seq / set_ms, "set_over_batched": batch / set_ms,
             "set_results_equal_batched": bool(same),
+            "learned_set_ms": learned_ms, "learned_set_value": lst["bounces"] / (learned_ms / 1e3),
+            "learned_over_plain": (lst["bounces"] / learned_ms) / (bounces / set_ms),
+            "learned_bounce_count_agreement": agree, "learned_newton_failed_rays": int(sum(lst["status_hist"][2:5])),
+            "plain_newton_failed_rays": int(sum(st["status_hist"][2:5])), "learned_training": set_training,
             "scene_build_s": create_s, "set_build_s": set_create_s, "set_rounds": st["rounds"],
             "set_launches": st["launches"],
             "note": "device time of one bbrt_trace_set call (the set: one wavefront over all scenes, rays in and "
