@@ -309,14 +309,20 @@ def _trace_form(scene, to, td, n, maxb, outs, stream, flush, steps, warmup, dev,
     wall = time.perf_counter() - wall0
     if world > 1:
         dist.barrier()
-    if stats is not None and scene.tuning()["graph_rounds"]:
-        scene.tuning(graph_rounds=0)
+    if stats is not None:
+        # per-kernel device times of the timed kernels (the instances that
+        # keep no counters): one host-driven-rounds step with kernel events only
+        graph = scene.tuning()["graph_rounds"]
+        if graph:
+            scene.tuning(graph_rounds=0)
         host = scene.trace_device(to.data_ptr(), td.data_ptr(), n, maxb, outs, stream=stream.cuda_stream,
-                                  want_stats=True)
-        scene.tuning(graph_rounds=1)
+                                  want_stats=True, times_only=True)
+        if graph:
+            scene.tuning(graph_rounds=1)
         torch.cuda.synchronize(dev)
         stats = dict(stats, **{k: host[k] for k in ("order_ms", "advance_ms", "guess_ms", "newton_ms", "tail_ms")},
-                     kernel_ms_from="one host-driven-rounds step after the timed region")
+                     kernel_ms_from="one host-driven-rounds step after the timed region, kernel events only (the "
+                                    "counters above come from a statistics step, whose kernels also count)")
     return sum(a.elapsed_time(b) for a, b in evs) / 1e3, wall, stats
 
 

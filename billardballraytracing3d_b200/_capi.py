@@ -52,6 +52,7 @@ QUERY_BVH = 0
 QUERY_BRUTE = 1
 QUERY_OBJECT = 2
 DEVICE_PTRS = 1
+TIMES_ONLY = 2
 PIPE_FP64 = 0
 PIPE_FP32 = 1
 PIPE_L2 = 2

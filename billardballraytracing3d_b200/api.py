@@ -147,8 +147,10 @@ class Scene:
         return r
 
     def trace_device(self, origins_ptr: int, dirs_ptr: int, n: int, max_bounces: int, out_ptrs: Dict[str, int],
-                     record: int = 0, stream: int = 0, want_stats: bool = False) -> Optional[Dict]:
-        """bbrt_trace on device pointers (e.g. torch tensors' data_ptr())."""
+                     record: int = 0, stream: int = 0, want_stats: bool = False,
+                     times_only: bool = False) -> Optional[Dict]:
+        """bbrt_trace on device pointers (e.g. torch tensors' data_ptr()); with
+        times_only the statistics hold the device times only (BBRT_TIMES_ONLY)."""
         out = C.TraceOut()
         out.record_bounces = record
         for k, v in out_ptrs.items():
@@ -156,7 +158,8 @@ class Scene:
             setattr(out, k, ctypes.cast(ctypes.c_void_p(v), ctypes.POINTER(ct)))
         st = C.TraceStats()
         C.check(self.lib, self.lib.bbrt_trace(self.h, ctypes.c_void_p(origins_ptr), ctypes.c_void_p(dirs_ptr), n,
-                                              max_bounces, C.DEVICE_PTRS, ctypes.byref(out),
+                                              max_bounces, C.DEVICE_PTRS | (C.TIMES_ONLY if times_only else 0),
+                                              ctypes.byref(out),
                                               ctypes.byref(st) if want_stats else None,
                                               ctypes.c_void_p(stream) if stream else None), "bbrt_trace")
         return st.as_dict() if want_stats else None

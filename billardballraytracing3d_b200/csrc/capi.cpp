@@ -157,6 +157,8 @@ struct bbrt_scene {
     std::vector<long long> member_rays;
     std::vector<double> member_sphere;
     const int* ray_member = nullptr;
+    // Per-kernel event timing without device counters (bbrt_trace BBRT_TIMES_ONLY).
+    bool time_kernels = false;
     // Training-sample recording, set only inside bbrt_guess_train.
     bbrt::GuessSample* rec_samples = nullptr;
     unsigned long long* rec_count = nullptr;
@@ -1150,7 +1152,7 @@ int prepare_trace(bbrt_scene* s, const double* d_o, const double* d_d, long long
         BBRT_CUDA(cudaMemsetAsync(s->guess.err.p, 0, sizeof(int), st));
         A.off_patch_miss = 1;
     }
-    s->timing = want_stats;
+    s->timing = want_stats || s->time_kernels;
     s->kev_used = 0;
     s->kspans.clear();
     s->rounds = 0;
@@ -1486,9 +1488,12 @@ BBRT_API int bbrt_trace(bbrt_scene_t s, const double* origins, const double* dir
         if (stats) fill_stats(s, hs, 0, 0.0f, 0.0f, stats);
         return BBRT_OK;
     }
+    const bool counters = stats != nullptr && !(flags & BBRT_TIMES_ONLY);
     if (flags & BBRT_DEVICE_PTRS) {
-        rc = run_trace_device(s, origins, dirs, n, max_bounces, out, nullptr, 1, st, stats != nullptr, hs,
+        s->time_kernels = stats != nullptr;
+        rc = run_trace_device(s, origins, dirs, n, max_bounces, out, nullptr, 1, st, counters, hs,
                               stats ? &kms : nullptr);
+        s->time_kernels = false;
         if (rc) return rc;
         if (stats) {
             BBRT_CUDA(cudaStreamSynchronize(st));
@@ -1527,8 +1532,10 @@ BBRT_API int bbrt_trace(bbrt_scene_t s, const double* origins, const double* dir
         if ((rc = bind(out->err_value, s->o_eval, sizeof(double) * 2 * N, dev.err_value))) return rc;
         if ((rc = bind(out->ray_work, s->o_work, sizeof(long long) * 4 * N, dev.ray_work))) return rc;
     }
+    s->time_kernels = stats != nullptr;
     rc = run_trace_device(s, static_cast<const double*>(s->in_o.p), static_cast<const double*>(s->in_d.p), n,
-                          max_bounces, out ? &dev : nullptr, nullptr, 1, st, stats != nullptr, hs, nullptr);
+                          max_bounces, out ? &dev : nullptr, nullptr, 1, st, counters, hs, nullptr);
+    s->time_kernels = false;
     if (rc) return rc;
     for (const Map& m : maps)
         BBRT_CUDA(cudaMemcpyAsync(m.host, m.buf->p, m.bytes, cudaMemcpyDeviceToHost, st));

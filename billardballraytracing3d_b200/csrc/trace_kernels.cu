@@ -26,10 +26,29 @@
 
 namespace bbrt {
 
-struct Counters {
+// Work counters of the statistics, per thread (summed per warp at the end of
+// a launch).  CountersT<false> holds nothing: a launch that collects no
+// statistics (and no per-ray work profile) uses it, so the counting, its
+// 64-bit registers and their spills compile away.
+struct NoCount {
+    __device__ __forceinline__ NoCount& operator++() { return *this; }
+    __device__ __forceinline__ NoCount operator++(int) { return *this; }
+    __device__ __forceinline__ NoCount& operator+=(long long) { return *this; }
+    __device__ __forceinline__ operator long long() const { return 0; }
+};
+
+template <bool ON>
+struct CountersT {
+    static constexpr bool kOn = true;
     long long node_tests = 0, patch_tests = 0, cell_tests = 0, tri_tests = 0, newton_iters = 0;
     long long off_patch = 0;   // learned form: Newton roots outside their patch taken as misses
 };
+template <>
+struct CountersT<false> {
+    static constexpr bool kOn = false;
+    NoCount node_tests, patch_tests, cell_tests, tri_tests, newton_iters, off_patch;
+};
+using Counters = CountersT<true>;
 
 // Per-ray data of the FP32 cull test (computed once per query).
 struct CullRay {
@@ -134,8 +153,9 @@ __device__ __forceinline__ void stage1_cell(const double* __restrict__ X, const 
 
 // SurfacePatch::intersect stage 1: the winning (t, key) over the coarse
 // triangulation (all cells, or only cells whose inflated box the ray crosses).
+template <class Ctr>
 __device__ __forceinline__ Stage1 patch_stage1(const DScene& S, int pidx, const V3& o, const V3& d, bool use_cull,
-                                               const CullRay& cr, Counters& ctr) {
+                                               const CullRay& cr, Ctr& ctr) {
     const int n = S.coarse_n, nc = n - 1;
     const double* X = S.c_xyz + static_cast<long long>(pidx) * n * n * 3;
     const double* CC = S.c_cell + static_cast<long long>(pidx) * nc * nc * 4;
@@ -182,19 +202,24 @@ __device__ __forceinline__ void key_to_uv(const DScene& S, int key, double& u0, 
 
 // SurfacePatch::intersect: stage 1, then Newton from the winning triangle's
 // (u, v) centroid and its t.
+template <class Ctr>
 __device__ __forceinline__ int patch_intersect(const DScene& S, int pidx, const V3& o, const V3& d, bool use_cull,
-                                               const CullRay& cr, QHit& h, Counters& ctr) {
+                                               const CullRay& cr, QHit& h, Ctr& ctr) {
     const Stage1 best = patch_stage1(S, pidx, o, d, use_cull, cr, ctr);
     if (!best.have) return 0;
     double u0, v0;
     key_to_uv(S, best.key, u0, v0);
-    return newton_exact(S, pidx, o, d, u0, v0, best.t, h, ctr.newton_iters);
+    long long it = 0;
+    const int r = newton_exact(S, pidx, o, d, u0, v0, best.t, h, it);
+    ctr.newton_iters += it;
+    return r;
 }
 
 // Triangle::intersect (Triangle.hpp:26-28): Moller-Trumbore, point o + t d,
 // normal normalize(e1 x e2).
+template <class Ctr>
 __device__ __forceinline__ int triangle_intersect(const DScene& S, int sub, const V3& o, const V3& d, QHit& h,
-                                                  Counters& ctr) {
+                                                  Ctr& ctr) {
     h.err = 0;
     h.ev0 = 0.0;
     h.ev1 = 0.0;
@@ -213,8 +238,9 @@ __device__ __forceinline__ int triangle_intersect(const DScene& S, int sub, cons
 
 // ScatObject::intersect for object `obj`: 1 hit, 0 miss (h.err set on a
 // Newton failure).
+template <class Ctr>
 __device__ __forceinline__ int object_intersect(const DScene& S, int obj, const V3& o, const V3& d, bool use_cull,
-                                                const CullRay& cr, QHit& h, Counters& ctr) {
+                                                const CullRay& cr, QHit& h, Ctr& ctr) {
     h.err = 0;
     h.ev0 = 0.0;
     h.ev1 = 0.0;
@@ -226,7 +252,8 @@ __device__ __forceinline__ int object_intersect(const DScene& S, int obj, const 
 // BVH::intersect with a 64-entry stack.  Returns the closest hit (obj >= 0),
 // a miss (obj < 0, err 0), or the first Newton failure met (err != 0).
 // off_patch_miss (learned form): a Newton root outside its patch is a miss.
-__device__ QHit bvh_query(const DScene& S, const V3& o, const V3& d, int cull_flag, Counters& ctr,
+template <class Ctr>
+__device__ QHit bvh_query(const DScene& S, const V3& o, const V3& d, int cull_flag, Ctr& ctr,
                           bool off_patch_miss = false, int member = -1) {
     QHit best;
     best.obj = -1;
@@ -375,7 +402,8 @@ __device__ __forceinline__ void finish_ray(const TraceArgs& A, long long i, cons
 }
 
 // Runs the bounce loop of one ray to the end with inline queries.
-__device__ __forceinline__ void run_ray(const DScene& S, const TraceArgs& A, long long i, RayCtx& r, Counters& ctr,
+template <class Ctr>
+__device__ __forceinline__ void run_ray(const DScene& S, const TraceArgs& A, long long i, RayCtx& r, Ctr& ctr,
                                         long long& queries) {
     while (r.status < 0) {
         if (r.bounces >= A.max_bounces) { r.status = BBRT_RAY_MAX_BOUNCES; break; }
@@ -387,7 +415,9 @@ __device__ __forceinline__ void run_ray(const DScene& S, const TraceArgs& A, lon
 
 // Adds one thread's work counters for ray i to the optional per-ray profile
 // (a ray is owned by one thread at a time, so no atomics are needed).
-__device__ __forceinline__ void add_ray_work(const TraceArgs& A, long long i, const Counters& c) {
+template <class Ctr>
+__device__ __forceinline__ void add_ray_work(const TraceArgs& A, long long i, const Ctr& c) {
+    if constexpr (!Ctr::kOn) return;
     if (!A.ray_work || i < 0) return;
     long long* w = A.ray_work + 4 * i;
     w[0] += c.node_tests;
@@ -396,13 +426,21 @@ __device__ __forceinline__ void add_ray_work(const TraceArgs& A, long long i, co
     w[3] += c.newton_iters;
 }
 
-struct RayTally {
+template <bool ON>
+struct RayTallyT {
     long long bounces = 0, queries = 0;
     long long hist[BBRT_RAY_STATUS_COUNT] = { 0, 0, 0, 0, 0, 0, 0, 0 };
 };
+template <>
+struct RayTallyT<false> {
+    NoCount bounces, queries;
+    NoCount hist[BBRT_RAY_STATUS_COUNT];
+};
+using RayTally = RayTallyT<true>;
 
-__device__ __forceinline__ void flush_stats(const TraceArgs& A, const Counters& ctr, const RayTally& t,
-                                            bool tail = false) {
+template <class Ctr, class Tally>
+__device__ __forceinline__ void flush_stats(const TraceArgs& A, const Ctr& ctr, const Tally& t, bool tail = false) {
+    if constexpr (!Ctr::kOn) return;
     if (!A.stats) return;
     if (tail) {
         long long rays = 0;
@@ -562,8 +600,9 @@ __device__ __forceinline__ void warp_cell_tris(const double* X, const double* CC
     }
 }
 
+template <class Ctr>
 __device__ Stage1 warp_patch_stage1(const DScene& S, int pidx, const V3& o, const V3& d, bool use_cull,
-                                    const CullRay& cr, int lane, Counters& ctr) {
+                                    const CullRay& cr, int lane, Ctr& ctr) {
     const int n = S.coarse_n, nc = n - 1;
     const double* X = S.c_xyz + static_cast<long long>(pidx) * n * n * 3;
     const double* CC = S.c_cell + static_cast<long long>(pidx) * nc * nc * 4;
@@ -571,7 +610,7 @@ __device__ Stage1 warp_patch_stage1(const DScene& S, int pidx, const V3& o, cons
     if (lane == 0) ++ctr.patch_tests;
     if (!(finite3(o) && finite3(d))) {
         // ordered loop on every lane (same result everywhere)
-        Counters dummy;
+        CountersT<false> dummy;
         best = patch_stage1(S, pidx, o, d, false, cr, dummy);
         if (lane == 0) ctr.tri_tests += 6LL * nc * nc;
         return best;
@@ -613,8 +652,9 @@ __device__ Stage1 warp_patch_stage1(const DScene& S, int pidx, const V3& o, cons
 // the half.  With at most 16 blocks per patch and 16 cells per block each
 // level is still one ballot, so two halves take two patches in the time the
 // whole warp takes one.  The half's test counts (uniform over it) go to c.
+template <class Ctr>
 __device__ Stage1 half_patch_stage1(const DScene& S, int pidx, const V3& o, const V3& d, bool use_cull,
-                                    const CullRay& cr, int hl, unsigned hmask, int hbase, Counters& c) {
+                                    const CullRay& cr, int hl, unsigned hmask, int hbase, Ctr& c) {
     constexpr int WH = 16;
     const int n = S.coarse_n, nc = n - 1;
     const double* X = S.c_xyz + static_cast<long long>(pidx) * n * n * 3;
@@ -622,7 +662,7 @@ __device__ Stage1 half_patch_stage1(const DScene& S, int pidx, const V3& o, cons
     Stage1 best;
     ++c.patch_tests;
     if (!(finite3(o) && finite3(d))) {
-        Counters dummy;
+        CountersT<false> dummy;
         best = patch_stage1(S, pidx, o, d, false, cr, dummy);
         c.tri_tests += 6LL * nc * nc;
         return best;
@@ -808,10 +848,10 @@ __device__ __forceinline__ bool resume_query(const DScene& S, const TraceArgs& A
 // children are tested with it (see the traversal stack tags); HALF: the
 // warp's queued stage 1s are taken two at a time by half-warps (patches of at
 // most 16 blocks of at most 16 cells).
-template <int NT, int MINB, bool CHILD, bool HALF>
+template <int NT, int MINB, bool CHILD, bool HALF, bool STATS>
 __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, WaveArgs W) {
-    Counters ctr, cray;
-    RayTally tally;
+    CountersT<STATS> ctr, cray;
+    RayTallyT<STATS> tally;
     NewtonRequest rq;
     rq.ray = -1;
     long long i = -1;
@@ -1092,7 +1132,7 @@ __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, Wav
                 scr.iy = __shfl_sync(kFull, q.cr.iy, src);
                 scr.iz = __shfl_sync(kFull, q.cr.iz, src);
                 scr.delta = __shfl_sync(kFull, q.cr.delta, src);
-                Counters c2;
+                CountersT<STATS> c2;
                 const Stage1 res = half_patch_stage1(S, spidx, so, sd, scull, scr, lane & 15, 0xFFFFu << (16 * hh),
                                                      16 * hh, c2);
                 __syncwarp();
@@ -1102,9 +1142,12 @@ __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, Wav
                     const int have = __shfl_sync(kFull, res.have ? 1 : 0, leader);
                     const double st = __shfl_sync(kFull, res.t, leader);
                     const int sk = __shfl_sync(kFull, res.key, leader);
-                    const long long pt = __shfl_sync(kFull, c2.patch_tests, leader);
-                    const long long ct = __shfl_sync(kFull, c2.cell_tests, leader);
-                    const long long tt = __shfl_sync(kFull, c2.tri_tests, leader);
+                    long long pt = 0, ct = 0, tt = 0;
+                    if constexpr (STATS) {
+                        pt = __shfl_sync(kFull, c2.patch_tests, leader);
+                        ct = __shfl_sync(kFull, c2.cell_tests, leader);
+                        tt = __shfl_sync(kFull, c2.tri_tests, leader);
+                    }
                     const int owner = hv == 0 ? src0 : src1;
                     if (lane == owner) {
                         q.s1.have = have != 0;
@@ -1139,11 +1182,14 @@ __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, Wav
                 scr.iy = __shfl_sync(kFull, q.cr.iy, src);
                 scr.iz = __shfl_sync(kFull, q.cr.iz, src);
                 scr.delta = __shfl_sync(kFull, q.cr.delta, src);
-                Counters c2;
+                CountersT<STATS> c2;
                 const Stage1 res = warp_patch_stage1(S, spidx, so, sd, scull, scr, lane, c2);
-                const long long pt = __shfl_sync(kFull, c2.patch_tests, 0);
-                const long long ct = __shfl_sync(kFull, c2.cell_tests, 0);
-                const long long tt = __shfl_sync(kFull, c2.tri_tests, 0);
+                long long pt = 0, ct = 0, tt = 0;
+                if constexpr (STATS) {
+                    pt = __shfl_sync(kFull, c2.patch_tests, 0);
+                    ct = __shfl_sync(kFull, c2.cell_tests, 0);
+                    tt = __shfl_sync(kFull, c2.tri_tests, 0);
+                }
                 if (lane == src) {
                     q.s1 = res;
                     cray.patch_tests += pt;
@@ -1183,7 +1229,7 @@ __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, Wav
         const long long fs = warp_append(&W.counters[2], need);
         if (need) {
             if (fs < n_run) {
-                cray = Counters();
+                cray = CountersT<STATS>();
                 nres = 0;
                 if (W.runnable == nullptr) {
                     i = W.order ? W.order[fs] : fs;
@@ -1397,7 +1443,8 @@ __global__ void __launch_bounds__(128) k_resume(DScene S, TraceArgs A, WaveArgs 
 
 // BVH::intersect for one ray with a whole warp (every lane returns the same result).
 // Nodes [0, staged) are read from the shared-memory copy (sbox, slink).
-__device__ QHit warp_bvh_query(const DScene& S, const V3& o, const V3& d, int cull_flag, int lane, Counters& ctr,
+template <class Ctr>
+__device__ QHit warp_bvh_query(const DScene& S, const V3& o, const V3& d, int cull_flag, int lane, Ctr& ctr,
                                const double* sbox, const int* slink, int staged, bool off_patch_miss, int member) {
     QHit best;
     best.obj = -1;
@@ -1442,7 +1489,7 @@ __device__ QHit warp_bvh_query(const DScene& S, const V3& o, const V3& d, int cu
                         if (lane == 0) ctr.newton_iters += it;
                     }
                 } else {
-                    Counters dummy;
+                    CountersT<false> dummy;
                     r = triangle_intersect(S, S.obj_sub[obj], o, d, h, dummy);
                 }
                 if (off_patch_miss && h.err == BBRT_RAY_NEWTON_DOMAIN) {
@@ -1476,7 +1523,7 @@ __device__ QHit warp_bvh_query(const DScene& S, const V3& o, const V3& d, int cu
 // Finishes rays from their saved state, one warp per ray.
 // MINB blocks of 128 threads per SM requested from the register allocator;
 // the first S.smem_nodes BVH nodes are staged in shared memory.
-template <int MINB>
+template <int MINB, bool STATS>
 __global__ void __launch_bounds__(128, MINB) k_resume_warp(DScene S, TraceArgs A, WaveArgs W,
                                                            const NewtonRequest* reqs, const int* rays, long long n) {
     extern __shared__ __align__(16) double smem_tail[];
@@ -1489,8 +1536,8 @@ __global__ void __launch_bounds__(128, MINB) k_resume_warp(DScene S, TraceArgs A
     const int lane = threadIdx.x & 31;
     const long long warp = (blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x) >> 5;
     const long long n_warps = (static_cast<long long>(gridDim.x) * blockDim.x) >> 5;
-    Counters ctr;
-    RayTally tally;
+    CountersT<STATS> ctr;
+    RayTallyT<STATS> tally;
     // The tail's time is that of its slowest warp: rays are handed out one
     // at a time from a counter, so a warp that drew a long chain takes no
     // further rays while others do (a fixed stride when no counter is given).
@@ -1505,7 +1552,7 @@ __global__ void __launch_bounds__(128, MINB) k_resume_warp(DScene S, TraceArgs A
         const long long i = reqs ? reqs[slot].ray : rays[slot];
         int nres;
         RayCtx r = load_ray(A, W, i, nres);
-        Counters c1;
+        CountersT<STATS> c1;
         while (r.status < 0) {
             if (r.bounces >= A.max_bounces) { r.status = BBRT_RAY_MAX_BOUNCES; break; }
             if (lane == 0) ++tally.queries;
@@ -1705,15 +1752,15 @@ void wave_layout(void* ws, long long n, WaveArgs& W, NewtonRequest*& req_a, Newt
 
 size_t wave_workspace_bytes(long long n) { return wave_bytes_per_ray() * n + 20 * 256; }
 
-template <int NT, int MINB, bool CHILD, bool HALF>
-static cudaError_t launch_advance_variant(const DScene& Sl, const TraceArgs& A, const WaveArgs& W, int sm_count,
-                                          cudaStream_t stream) {
+template <int NT, int MINB, bool CHILD, bool HALF, bool STATS>
+static cudaError_t launch_advance_stats(const DScene& Sl, const TraceArgs& A, const WaveArgs& W, int sm_count,
+                                        cudaStream_t stream) {
     const size_t smem = static_cast<size_t>(Sl.smem_nodes) * (6 * sizeof(double) + 4 * sizeof(int));
-    cudaError_t e = cudaFuncSetAttribute(k_advance<NT, MINB, CHILD, HALF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(k_advance<NT, MINB, CHILD, HALF, STATS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_advance<NT, MINB, CHILD, HALF>, NT, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_advance<NT, MINB, CHILD, HALF, STATS>, NT, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
     // A small round (the late ones) is spread over every SM with smaller
@@ -1725,8 +1772,16 @@ static cudaError_t launch_advance_variant(const DScene& Sl, const TraceArgs& A, 
     long long blocks = static_cast<long long>(per_sm) * sm_count;
     const long long need = (W.n_runnable + threads - 1) / threads;
     if (blocks > need) blocks = need;
-    k_advance<NT, MINB, CHILD, HALF><<<static_cast<unsigned>(blocks), threads, smem, stream>>>(Sl, A, W);
+    k_advance<NT, MINB, CHILD, HALF, STATS><<<static_cast<unsigned>(blocks), threads, smem, stream>>>(Sl, A, W);
     return cudaGetLastError();
+}
+
+// The statistics-free instance unless the call collects statistics or a per-ray work profile.
+template <int NT, int MINB, bool CHILD, bool HALF>
+static cudaError_t launch_advance_variant(const DScene& Sl, const TraceArgs& A, const WaveArgs& W, int sm_count,
+                                          cudaStream_t stream) {
+    if (A.stats || A.ray_work) return launch_advance_stats<NT, MINB, CHILD, HALF, true>(Sl, A, W, sm_count, stream);
+    return launch_advance_stats<NT, MINB, CHILD, HALF, false>(Sl, A, W, sm_count, stream);
 }
 
 template <int NT, int MINB>
@@ -1816,25 +1871,35 @@ cudaError_t launch_resume(const DScene& S, const TraceArgs& A, const WaveArgs& W
     return cudaGetLastError();
 }
 
-template <int MINB>
-static cudaError_t launch_resume_warp_shape(const DScene& S, const TraceArgs& A, const WaveArgs& W,
+template <int MINB, bool STATS>
+static cudaError_t launch_resume_warp_stats(const DScene& S, const TraceArgs& A, const WaveArgs& W,
                                             const NewtonRequest* reqs, const int* rays, long long n, int sm_count,
                                             int max_smem_nodes, cudaStream_t stream) {
     DScene Sl = S;
     if (Sl.smem_nodes > max_smem_nodes) Sl.smem_nodes = max_smem_nodes;
     const size_t smem = static_cast<size_t>(Sl.smem_nodes) * (6 * sizeof(double) + 4 * sizeof(int));
-    cudaError_t e = cudaFuncSetAttribute(k_resume_warp<MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(k_resume_warp<MINB, STATS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_resume_warp<MINB>, 128, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_resume_warp<MINB, STATS>, 128, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
     long long blocks = static_cast<long long>(per_sm) * sm_count;
     const long long need = (n + 3) / 4;   // four warps (rays) per block
     if (blocks > need) blocks = need;
-    k_resume_warp<MINB><<<static_cast<unsigned>(blocks), 128, smem, stream>>>(Sl, A, W, reqs, rays, n);
+    k_resume_warp<MINB, STATS><<<static_cast<unsigned>(blocks), 128, smem, stream>>>(Sl, A, W, reqs, rays, n);
     return cudaGetLastError();
+}
+
+// The statistics-free instance unless the call collects statistics or a per-ray work profile.
+template <int MINB>
+static cudaError_t launch_resume_warp_shape(const DScene& S, const TraceArgs& A, const WaveArgs& W,
+                                            const NewtonRequest* reqs, const int* rays, long long n, int sm_count,
+                                            int max_smem_nodes, cudaStream_t stream) {
+    if (A.stats || A.ray_work)
+        return launch_resume_warp_stats<MINB, true>(S, A, W, reqs, rays, n, sm_count, max_smem_nodes, stream);
+    return launch_resume_warp_stats<MINB, false>(S, A, W, reqs, rays, n, sm_count, max_smem_nodes, stream);
 }
 
 // Tail launch shapes (blocks of 128 threads per SM, BVH nodes staged in

@@ -176,7 +176,10 @@ enum {
 
 /* Flags for bbrt_trace / bbrt_intersect. */
 enum {
-    BBRT_DEVICE_PTRS = 1    /* all array arguments are device pointers (else host pointers) */
+    BBRT_DEVICE_PTRS = 1,   /* all array arguments are device pointers (else host pointers) */
+    BBRT_TIMES_ONLY = 2     /* with stats: fill only the call's and the per-kernel device times
+                               (no device counters are kept, and the trace kernels run the
+                               instances that keep none, as a call without stats does) */
 };
 
 /* Per-ray outputs of bbrt_trace.  Arrays the caller does not want may be NULL. */
