@@ -62,7 +62,7 @@ def parse():
     ap.add_argument("--cull", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=8.0, help="target wall time of the CPU sample")
-    ap.add_argument("--train-rays", type=int, default=16 << 20,
+    ap.add_argument("--train-rays", type=int, default=32 << 20,
                     help="rays of each scene traced to record training samples")
     ap.add_argument("--train-epochs", type=int, default=6)
     ap.add_argument("--train-positives", type=int, default=16 << 20, help="converged Newton solves kept for training")

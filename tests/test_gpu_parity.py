@@ -302,3 +302,37 @@ def test_trace_batch_equals_single_scene_traces(built):
         for k in ("status", "bounce_count", "exit_dir", "hit_object", "hit_point"):
             assert np.array_equal(ref[k], t[k].cpu().numpy()), k
     assert st["bounces"] == sum(int(r["bounce_count"].sum()) for r in refs)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("graph_rounds", [1, 0])
+def test_statistics_free_kernels_give_the_same_results(built, workloads, graph_rounds):
+    """A call without statistics runs the k_advance and tail instances that
+    keep no counters: the same results bit for bit as a call with them."""
+    import torch
+    patches, o, d, maxb, cn, tol = workloads("tetra_spheres", 65536)
+    sc = api.Scene(patches, config=C.default_config(coarse_grid_n=cn, newton_tol=tol))
+    sc.tuning(graph_rounds=graph_rounds)
+    n, K = o.shape[0], 8
+    to = torch.from_numpy(np.ascontiguousarray(o)).cuda()
+    td = torch.from_numpy(np.ascontiguousarray(d)).cuda()
+    res = []
+    for want_stats in (True, False):
+        bufs = {"status": torch.full((n,), -1, dtype=torch.int32, device="cuda"),
+                "bounce_count": torch.full((n,), -1, dtype=torch.int32, device="cuda"),
+                "exit_dir": torch.zeros((n, 3), dtype=torch.float64, device="cuda"),
+                "end_point": torch.zeros((n, 3), dtype=torch.float64, device="cuda"),
+                "hit_object": torch.full((n, K), -9, dtype=torch.int32, device="cuda"),
+                "hit_point": torch.zeros((n, K, 3), dtype=torch.float64, device="cuda")}
+        st = sc.trace_device(to.data_ptr(), td.data_ptr(), n, maxb, {k: v.data_ptr() for k, v in bufs.items()},
+                             record=K, want_stats=want_stats)
+        torch.cuda.synchronize()
+        res.append({k: v.cpu().numpy() for k, v in bufs.items()})
+        if want_stats:
+            assert st["node_tests"] > 0
+    for k in res[0]:
+        assert np.array_equal(res[0][k], res[1][k]), k
+    # times only: kernel times, no counters
+    sc.tuning(graph_rounds=0)
+    st = sc.trace_device(to.data_ptr(), td.data_ptr(), n, maxb, {}, want_stats=True, times_only=True)
+    assert st["node_tests"] == 0 and st["advance_ms"] > 0
