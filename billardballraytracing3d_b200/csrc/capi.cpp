@@ -80,10 +80,14 @@ int fail(int code, const std::string& msg) {
             return fail(BBRT_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
     } while (0)
 
-// A grow-only device buffer.
+// A grow-only device buffer, freed when it goes out of scope.
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
     cudaError_t ensure(size_t n) {
         if (n <= bytes) return cudaSuccess;
         if (p) cudaFree(p);
