@@ -604,6 +604,20 @@ def multi_scene(k, steps, dev):
     from billardballraytracing3d_b200 import _capi as C
     from billardballraytracing3d_b200 import api, scenes
     work = scenes.multi_scene_workload(k)
+    # scene creation with the per-patch set-up on the GPU vs on the host, on
+    # the first eight scenes (each created, uploaded and released in turn)
+    setup_cmp = {}
+    for where in (1, 0):
+        t0 = time.perf_counter()
+        for patches, o, d, maxb, cn, tol in work[:8]:
+            sc = api.Scene(patches, config=C.default_config(coarse_grid_n=cn, newton_tol=tol, setup_on_device=where))
+            sc.upload()
+            sc.close()
+        torch.cuda.synchronize(dev)
+        setup_cmp["gpu_s" if where else "host_s"] = time.perf_counter() - t0
+    setup_cmp["scenes"] = 8
+    setup_cmp["patches"] = int(sum(len(w[0]) for w in work[:8]))
+    setup_cmp["host_threads"] = os.cpu_count()
     t0 = time.perf_counter()
     scs = [api.Scene(patches, config=C.default_config(coarse_grid_n=cn, newton_tol=tol))
            for patches, o, d, maxb, cn, tol in work]
@@ -657,7 +671,7 @@ def multi_scene(k, steps, dev):
             "learned_over_plain": (lst["bounces"] / learned_ms) / (bounces / set_ms),
             "learned_bounce_count_agreement": agree, "learned_newton_failed_rays": int(sum(lst["status_hist"][2:5])),
             "plain_newton_failed_rays": int(sum(st["status_hist"][2:5])), "learned_training": set_training,
-            "scene_build_s": create_s, "set_build_s": set_create_s, "set_rounds": st["rounds"],
+            "scene_build_s": create_s, "set_build_s": set_create_s, "setup_compare": setup_cmp, "set_rounds": st["rounds"],
             "set_launches": st["launches"],
             "note": "device time of one bbrt_trace_set call (the set: one wavefront over all scenes, rays in and "
                     "results out included) vs one bbrt_trace_batch call (a wavefront per scene, scenes on their "
