@@ -604,20 +604,6 @@ def multi_scene(k, steps, dev):
     from billardballraytracing3d_b200 import _capi as C
     from billardballraytracing3d_b200 import api, scenes
     work = scenes.multi_scene_workload(k)
-    # scene creation with the per-patch set-up on the GPU vs on the host, on
-    # the first eight scenes (each created, uploaded and released in turn)
-    setup_cmp = {}
-    for where in (1, 0):
-        t0 = time.perf_counter()
-        for patches, o, d, maxb, cn, tol in work[:8]:
-            sc = api.Scene(patches, config=C.default_config(coarse_grid_n=cn, newton_tol=tol, setup_on_device=where))
-            sc.upload()
-            sc.close()
-        torch.cuda.synchronize(dev)
-        setup_cmp["gpu_s" if where else "host_s"] = time.perf_counter() - t0
-    setup_cmp["scenes"] = 8
-    setup_cmp["patches"] = int(sum(len(w[0]) for w in work[:8]))
-    setup_cmp["host_threads"] = os.cpu_count()
     t0 = time.perf_counter()
     scs = [api.Scene(patches, config=C.default_config(coarse_grid_n=cn, newton_tol=tol))
            for patches, o, d, maxb, cn, tol in work]
@@ -625,6 +611,19 @@ def multi_scene(k, steps, dev):
         sc.upload()
     torch.cuda.synchronize(dev)
     create_s = time.perf_counter() - t0
+    # the C ABI's scene creation alone (descriptors already built): the
+    # per-patch set-up on the GPU vs on the host, every scene created,
+    # uploaded and released in turn
+    setup_cmp = {"scenes": k, "patches": int(sum(len(w[0]) for w in work)), "host_threads": os.cpu_count()}
+    for where in (1, 0):
+        t0 = time.perf_counter()
+        for sc0, (patches, o, d, maxb, cn, tol) in zip(scs, work):
+            sc = api.Scene(table=sc0.table, config=C.default_config(coarse_grid_n=cn, newton_tol=tol,
+                                                                    setup_on_device=where))
+            sc.upload()
+            sc.close()
+        torch.cuda.synchronize(dev)
+        setup_cmp["gpu_s" if where else "host_s"] = time.perf_counter() - t0
     tens = []
     for patches, o, d, maxb, cn, tol in work:
         n = o.shape[0]

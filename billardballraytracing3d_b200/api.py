@@ -26,7 +26,7 @@ class Scene:
     (scenes.Patch), triangles (9 floats each), or a patch directory."""
 
     def __init__(self, patches: Sequence = (), triangles: Sequence = (), config: C.Config = None,
-                 directory: str = None, _handle=None):
+                 directory: str = None, _handle=None, table: C.ObjectTable = None):
         self.lib = C.load_library()
         self.config = config if config is not None else C.default_config()
         h = ctypes.c_void_p()
@@ -36,7 +36,8 @@ class Scene:
             C.check(self.lib, self.lib.bbrt_scene_create_from_dir(directory.encode(), ctypes.byref(self.config),
                                                                    ctypes.byref(h)), "bbrt_scene_create_from_dir")
         else:
-            self.table = C.ObjectTable(patches, triangles)
+            # `table`: descriptors already built (another scene's), reused as they are
+            self.table = table if table is not None else C.ObjectTable(patches, triangles)
             C.check(self.lib, self.lib.bbrt_scene_create(self.table.descs, self.table.n, ctypes.byref(self.config),
                                                          ctypes.byref(h)), "bbrt_scene_create")
         self.h = h
