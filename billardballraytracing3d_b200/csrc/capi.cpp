@@ -625,6 +625,7 @@ struct Tuning {
     int order_entry = 1;              // round-0 order keyed on the scene-sphere entry point (else the origin)
     int child_test = -1;              // k_advance child tests: -1 when the BVH exceeds the staged nodes, 0 / 1
     int half_stage1 = 1;              // k_advance stage 1 of two patches at a time by half-warps
+    int quarter_stage1 = 0;           // ... four at a time by quarter-warps
 };
 
 // Launch-shape knobs; defaults tuned on B200, overridable for experiments by
@@ -649,6 +650,7 @@ const Tuning& tuning() {
         if (const char* e = std::getenv("BBRT_ORDER_ENTRY")) v.order_entry = std::atoi(e);
         if (const char* e = std::getenv("BBRT_CHILD_TEST")) v.child_test = std::atoi(e);
         if (const char* e = std::getenv("BBRT_HALF_S1")) v.half_stage1 = std::atoi(e);
+        if (const char* e = std::getenv("BBRT_QUARTER_S1")) v.quarter_stage1 = std::atoi(e);
         return v;
     }();
     return t;
@@ -790,6 +792,7 @@ int build_wave_graph(bbrt_scene* s, const bbrt::TraceArgs& A, const bbrt_tuning&
     W.resume_queries = tuning().resume_queries;
     W.child_test = tuning().child_test;
     W.half_stage1 = tuning().half_stage1;
+        W.quarter_stage1 = tuning().quarter_stage1;
     W.group_newton = tuning().group_newton;
     W.watchdog_cycles = watchdog_cycles(T);
     W.n_runnable = n;   // sizes the persistent grid; later rounds read their count
@@ -916,7 +919,8 @@ int launch_wave_graph(bbrt_scene* s, const bbrt::TraceArgs& A, const bbrt_tuning
                          static_cast<long long>(T.advance_shape), static_cast<long long>(T.warp_stage1),
                          static_cast<long long>(T.order_rays), static_cast<long long>(T.warp_tail), T.wave_tail,
                          static_cast<long long>(tuning().resume_queries), static_cast<long long>(tuning().group_newton),
-                         static_cast<long long>(tuning().tail_shape), max_rounds,
+                         static_cast<long long>(tuning().tail_shape), static_cast<long long>(tuning().quarter_stage1),
+                         max_rounds,
                          static_cast<long long>(sort_round_requests(s)), watchdog_cycles(T), mma_wait_cycles(T),
                          static_cast<long long>(A.off_patch_miss) })
         k.put(x);
@@ -987,6 +991,7 @@ struct WaveRun {
         W.resume_queries = tuning().resume_queries;
         W.child_test = tuning().child_test;
         W.half_stage1 = tuning().half_stage1;
+        W.quarter_stage1 = tuning().quarter_stage1;
         W.group_newton = tuning().group_newton;
         W.watchdog_cycles = watchdog_cycles(T);
         W.runnable = nullptr;

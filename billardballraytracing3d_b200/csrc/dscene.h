@@ -176,6 +176,7 @@ struct WaveArgs {
     double guess_t_window = 0.5;               // accepted |t - t_stage1| in units of L
     int warp_stage1 = 1;                       // stage 1 of k_advance by the whole warp (else per lane)
     int half_stage1 = 1;                       // ... two patches at a time by half-warps where they fit
+    int quarter_stage1 = 0;                    // ... four at a time by quarter-warps instead
     // Traversal state of a query suspended for a Newton solve, so that the
     // next round resumes it instead of replaying it from the root:
     // qs_int[ray][kQsInt] = stack depth (-1: none saved), leaf start, leaf

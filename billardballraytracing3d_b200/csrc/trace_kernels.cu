@@ -646,16 +646,18 @@ __device__ Stage1 warp_patch_stage1(const DScene& S, int pidx, const V3& o, cons
     return best;
 }
 
-// Stage 1 of one patch by a half-warp (lane hl of the half whose lanes are
-// hmask, the first being hbase): warp_patch_stage1's block, cell and
-// triangle tests over 16 lanes, and the same (t, key) winner on every lane of
-// the half.  With at most 16 blocks per patch and 16 cells per block each
-// level is still one ballot, so two halves take two patches in the time the
-// whole warp takes one.  The half's test counts (uniform over it) go to c.
-template <class Ctr>
-__device__ Stage1 half_patch_stage1(const DScene& S, int pidx, const V3& o, const V3& d, bool use_cull,
-                                    const CullRay& cr, int hl, unsigned hmask, int hbase, Ctr& c) {
-    constexpr int WH = 16;
+// Stage 1 of one patch by a group of WH lanes, 16 (a half-warp) or 8 (a
+// quarter; lane hl of the group whose lanes are hmask, the first being
+// hbase): warp_patch_stage1's block, cell and triangle tests over WH lanes,
+// and the same (t, key) winner on every lane of the group.  With at most 16
+// blocks per patch and 16 cells per block each level is one ballot for a
+// half-warp (two for a quarter), so two halves take two patches, four
+// quarters four, in about the time the whole warp takes one.  The group's
+// test counts (uniform over it) go to c.
+template <int WH, class Ctr>
+__device__ Stage1 group_patch_stage1(const DScene& S, int pidx, const V3& o, const V3& d, bool use_cull,
+                                     const CullRay& cr, int hl, unsigned hmask, int hbase, Ctr& c) {
+    constexpr unsigned kGroupBits = (1u << WH) - 1u;
     const int n = S.coarse_n, nc = n - 1;
     const double* X = S.c_xyz + static_cast<long long>(pidx) * n * n * 3;
     const double* CC = S.c_cell + static_cast<long long>(pidx) * nc * nc * 4;
@@ -673,7 +675,7 @@ __device__ Stage1 half_patch_stage1(const DScene& S, int pidx, const V3& o, cons
         const float* CB = S.c_cell_box + static_cast<long long>(pidx) * nc * nc * 6;
         for (int b0 = 0; b0 < NB2; b0 += WH) {
             const int b = b0 + hl;
-            unsigned bm = (__ballot_sync(hmask, b < NB2 && cull_box(BB + b * 6, cr)) >> hbase) & 0xFFFFu;
+            unsigned bm = (__ballot_sync(hmask, b < NB2 && cull_box(BB + b * 6, cr)) >> hbase) & kGroupBits;
             c.cell_tests += min(WH, NB2 - b0);
             while (bm) {
                 const int bl = __ffs(bm) - 1;
@@ -685,7 +687,7 @@ __device__ Stage1 half_patch_stage1(const DScene& S, int pidx, const V3& o, cons
                     const int ce = c0 + hl;
                     const unsigned cm =
                         (__ballot_sync(hmask, ce < h * w && cull_box(CB + ((i0 + ce / w) * nc + j0 + ce % w) * 6, cr)) >>
-                         hbase) & 0xFFFFu;
+                         hbase) & kGroupBits;
                     c.cell_tests += min(WH, h * w - c0);
                     c.tri_tests += 6 * __popc(cm);
                     const int total = __popc(cm) * 6;
@@ -848,7 +850,7 @@ __device__ __forceinline__ bool resume_query(const DScene& S, const TraceArgs& A
 // children are tested with it (see the traversal stack tags); HALF: the
 // warp's queued stage 1s are taken two at a time by half-warps (patches of at
 // most 16 blocks of at most 16 cells).
-template <int NT, int MINB, bool CHILD, bool HALF, bool STATS>
+template <int NT, int MINB, bool CHILD, int G, bool STATS>
 __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, WaveArgs W) {
     CountersT<STATS> ctr, cray;
     RayTallyT<STATS> tally;
@@ -1101,20 +1103,23 @@ __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, Wav
         // all 32 lanes: the block, cell and triangle tests of the patch are
         // split over the lanes and the (t, key) minimum is taken over the warp
         // (the same winner as the lane's own ordered loop).
-        // (the HALF instance keeps the whole-warp path too and checks at run
-        // time: measured faster than an instance without it)
-        if (HALF && W.warp_stage1 && W.half_stage1 && S.n_blocks_side * S.n_blocks_side <= 16 &&
+        // With G > 1 (patches of at most 16 blocks of at most 16 cells), G
+        // patches at a time, one per group of 32 / G lanes; the instance keeps
+        // the whole-warp path too and checks at run time (measured faster
+        // than an instance without it).
+        if (G > 1 && W.warp_stage1 && W.half_stage1 && S.n_blocks_side * S.n_blocks_side <= 16 &&
             S.block_cells * S.block_cells <= 16) {
-            // two patches at a time, one per half-warp (the second half
-            // repeats the first patch when only one waits)
+            constexpr int WH = 32 / (G > 1 ? G : 2);
             unsigned pend = __ballot_sync(kFull, mode == M_S1_WARP);
             while (pend) {
-                const int src0 = __ffs(pend) - 1;
-                pend &= pend - 1;
-                const int src1 = pend ? __ffs(pend) - 1 : -1;
-                if (pend) pend &= pend - 1;
-                const int hh = lane >> 4;
-                const int src = (hh == 0 || src1 < 0) ? src0 : src1;
+                // this pass takes the first G waiting lanes; a group without
+                // one repeats the first patch (its result is not used)
+                const unsigned batch = pend;
+#pragma unroll
+                for (int g = 0; g < G; ++g) pend &= pend - 1;
+                const int gg = lane / WH;
+                const unsigned pos = __fns(batch, 0, gg + 1);
+                const int src = pos < 32u ? static_cast<int>(pos) : __ffs(batch) - 1;
                 V3 so, sd;
                 so.x = __shfl_sync(kFull, r.o.x, src);
                 so.y = __shfl_sync(kFull, r.o.y, src);
@@ -1133,12 +1138,12 @@ __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, Wav
                 scr.iz = __shfl_sync(kFull, q.cr.iz, src);
                 scr.delta = __shfl_sync(kFull, q.cr.delta, src);
                 CountersT<STATS> c2;
-                const Stage1 res = half_patch_stage1(S, spidx, so, sd, scull, scr, lane & 15, 0xFFFFu << (16 * hh),
-                                                     16 * hh, c2);
+                const Stage1 res = group_patch_stage1<WH>(S, spidx, so, sd, scull, scr, lane % WH,
+                                                          ((1u << WH) - 1u) << (WH * gg), WH * gg, c2);
                 __syncwarp();
 #pragma unroll
-                for (int hv = 0; hv < 2; ++hv) {
-                    const int leader = 16 * hv;
+                for (int hv = 0; hv < (G > 1 ? G : 2); ++hv) {
+                    const int leader = WH * hv;
                     const int have = __shfl_sync(kFull, res.have ? 1 : 0, leader);
                     const double st = __shfl_sync(kFull, res.t, leader);
                     const int sk = __shfl_sync(kFull, res.key, leader);
@@ -1148,8 +1153,8 @@ __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, Wav
                         ct = __shfl_sync(kFull, c2.cell_tests, leader);
                         tt = __shfl_sync(kFull, c2.tri_tests, leader);
                     }
-                    const int owner = hv == 0 ? src0 : src1;
-                    if (lane == owner) {
+                    const unsigned owner = __fns(batch, 0, hv + 1);
+                    if (owner < 32u && lane == static_cast<int>(owner)) {
                         q.s1.have = have != 0;
                         q.s1.t = st;
                         q.s1.key = sk;
@@ -1752,15 +1757,15 @@ void wave_layout(void* ws, long long n, WaveArgs& W, NewtonRequest*& req_a, Newt
 
 size_t wave_workspace_bytes(long long n) { return wave_bytes_per_ray() * n + 20 * 256; }
 
-template <int NT, int MINB, bool CHILD, bool HALF, bool STATS>
+template <int NT, int MINB, bool CHILD, int G, bool STATS>
 static cudaError_t launch_advance_stats(const DScene& Sl, const TraceArgs& A, const WaveArgs& W, int sm_count,
                                         cudaStream_t stream) {
     const size_t smem = static_cast<size_t>(Sl.smem_nodes) * (6 * sizeof(double) + 4 * sizeof(int));
-    cudaError_t e = cudaFuncSetAttribute(k_advance<NT, MINB, CHILD, HALF, STATS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(k_advance<NT, MINB, CHILD, G, STATS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_advance<NT, MINB, CHILD, HALF, STATS>, NT, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_advance<NT, MINB, CHILD, G, STATS>, NT, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
     // A small round (the late ones) is spread over every SM with smaller
@@ -1772,16 +1777,16 @@ static cudaError_t launch_advance_stats(const DScene& Sl, const TraceArgs& A, co
     long long blocks = static_cast<long long>(per_sm) * sm_count;
     const long long need = (W.n_runnable + threads - 1) / threads;
     if (blocks > need) blocks = need;
-    k_advance<NT, MINB, CHILD, HALF, STATS><<<static_cast<unsigned>(blocks), threads, smem, stream>>>(Sl, A, W);
+    k_advance<NT, MINB, CHILD, G, STATS><<<static_cast<unsigned>(blocks), threads, smem, stream>>>(Sl, A, W);
     return cudaGetLastError();
 }
 
 // The statistics-free instance unless the call collects statistics or a per-ray work profile.
-template <int NT, int MINB, bool CHILD, bool HALF>
+template <int NT, int MINB, bool CHILD, int G>
 static cudaError_t launch_advance_variant(const DScene& Sl, const TraceArgs& A, const WaveArgs& W, int sm_count,
                                           cudaStream_t stream) {
-    if (A.stats || A.ray_work) return launch_advance_stats<NT, MINB, CHILD, HALF, true>(Sl, A, W, sm_count, stream);
-    return launch_advance_stats<NT, MINB, CHILD, HALF, false>(Sl, A, W, sm_count, stream);
+    if (A.stats || A.ray_work) return launch_advance_stats<NT, MINB, CHILD, G, true>(Sl, A, W, sm_count, stream);
+    return launch_advance_stats<NT, MINB, CHILD, G, false>(Sl, A, W, sm_count, stream);
 }
 
 template <int NT, int MINB>
@@ -1793,13 +1798,14 @@ static cudaError_t launch_advance_shape(const DScene& S, const TraceArgs& A, con
     // lanes; else child tests when part of the tree stays in global memory.
     // The two together measured slower than either, and on both measured
     // scenes the half-warp stage 1 beat the child tests.
-    if (W.child_test > 0) return launch_advance_variant<NT, MINB, true, false>(Sl, A, W, sm_count, stream);
+    if (W.child_test > 0) return launch_advance_variant<NT, MINB, true, 1>(Sl, A, W, sm_count, stream);
     const bool half = W.half_stage1 && W.warp_stage1 && S.n_blocks_side * S.n_blocks_side <= 16 &&
                       S.block_cells * S.block_cells <= 16;
-    if (half) return launch_advance_variant<NT, MINB, false, true>(Sl, A, W, sm_count, stream);
+    if (half && W.quarter_stage1) return launch_advance_variant<NT, MINB, false, 4>(Sl, A, W, sm_count, stream);
+    if (half) return launch_advance_variant<NT, MINB, false, 2>(Sl, A, W, sm_count, stream);
     const bool child = W.child_test < 0 && S.n_nodes > Sl.smem_nodes;
-    return child ? launch_advance_variant<NT, MINB, true, false>(Sl, A, W, sm_count, stream)
-                 : launch_advance_variant<NT, MINB, false, false>(Sl, A, W, sm_count, stream);
+    return child ? launch_advance_variant<NT, MINB, true, 1>(Sl, A, W, sm_count, stream)
+                 : launch_advance_variant<NT, MINB, false, 1>(Sl, A, W, sm_count, stream);
 }
 
 // Launch shapes of k_advance: 0 = 128 threads x 3 blocks per SM,
