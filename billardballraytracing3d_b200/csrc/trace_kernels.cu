@@ -977,7 +977,9 @@ __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, Wav
                             }
                             ++q.leaf_k;
                         }
-                    } else if (W.warp_stage1) {
+                    } else if (G > 1 || W.warp_stage1) {
+                        // (instances with G > 1 run only with the warp-cooperative
+                        // stage 1, so they carry no per-lane stage-1 modes)
                         q.obj = obj;
                         q.pidx = S.obj_sub[obj];
                         mode = M_S1_WARP;
@@ -997,7 +999,7 @@ __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, Wav
                     }
                 }
             }
-        } else if (mode == M_BLOCK) {
+        } else if (G == 1 && mode == M_BLOCK) {
             if (q.bi >= NB) {
                 mode = M_S1_DONE;
             } else {
@@ -1015,7 +1017,7 @@ __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, Wav
                     mode = M_CELL;
                 }
             }
-        } else if (mode == M_CELL) {
+        } else if (G == 1 && mode == M_CELL) {
             if (q.ci >= q.i1) {
                 mode = M_BLOCK;
             } else {
@@ -1031,7 +1033,7 @@ __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, Wav
                     mode = M_TRI;
                 }
             }
-        } else if (mode == M_CELL_ALL) {
+        } else if (G == 1 && mode == M_CELL_ALL) {
             if (q.ci >= nc * nc) {
                 mode = M_S1_DONE;
             } else {
@@ -1042,7 +1044,7 @@ __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, Wav
                 q.tri_ret = M_CELL_ALL;
                 mode = M_TRI;
             }
-        } else if (mode == M_TRI) {
+        } else if (G == 1 && mode == M_TRI) {
             ++cray.tri_tests;
             stage1_tri(S.c_xyz + static_cast<long long>(q.pidx) * n * n * 3,
                        S.c_cell + static_cast<long long>(q.pidx) * nc * nc * 4, n, q.tci, q.tcj, q.tri, r.o, r.d, q.s1);
@@ -1165,7 +1167,7 @@ __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, Wav
                     }
                 }
             }
-        } else if (W.warp_stage1) {
+        } else if (G > 1 || W.warp_stage1) {
             unsigned pend = __ballot_sync(kFull, mode == M_S1_WARP);
             while (pend) {
                 const int src = __ffs(pend) - 1;
