@@ -164,6 +164,8 @@ def _hbm_peak():
 
 
 HBM_PEAK_GBS, HBM_PEAK_SOURCE = _hbm_peak()
+# BVH node tests in FP32 with an FP64 re-test of the undecided (the library's default; BBRT_NODE_F32=0: FP64)
+NODE_F32 = os.environ.get("BBRT_NODE_F32", "1") != "0"
 PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "k_advance_traffic.json")
 
 
@@ -172,7 +174,11 @@ def advance_roofline(st, fp64_peak, fp32_peak, l2_peak):
     own device time (CUDA events around each launch inside the library).
 
     Work per unit:
-      BVH node test          12 FP64 FLOP, 64 B (box + links)
+      BVH node test, FP32    16 FP32 FLOP (6 differences, 6 products, 4
+                             margin adds), 40 B (FP32 box + links); the few
+                             it leaves undecided add the FP64 test below
+      BVH node test, FP64    12 FP64 FLOP, 64 B (box + links); 48 B (box)
+                             as the re-test of an undecided FP32 test
       block / cell box test  18 FP32 FLOP, 24 B
       Moller-Trumbore test   28 FP64 FLOP up to the division-free rejection
                              (51 when it passes), 18 FP64 FLOP of corner
@@ -181,14 +187,19 @@ def advance_roofline(st, fp64_peak, fp32_peak, l2_peak):
     nodes = st["node_tests"] - st["tail_node_tests"]
     boxes = st["cell_tests"] - st["tail_cell_tests"]
     mts = st["tri_tests"] - st["tail_tri_tests"]
+    retest = st.get("node_tests_fp64", 0)   # whole step (the tail's few included)
     secs = st["advance_ms"] / 1e3
     if secs <= 0:
         return None
+    if NODE_F32:
+        f64, f32, nbytes = 12 * retest, 16 * nodes, 40 * nodes + 48 * retest
+    else:
+        f64, f32, nbytes = 12 * nodes, 0, 64 * nodes
     pipes = {
-        "fp64": ((12 * nodes + (28 + 18) * mts) / secs / 1e12, fp64_peak, "TFLOP/s"),
-        "fp32": (18 * boxes / secs / 1e12, fp32_peak, "TFLOP/s"),
-        "l2": ((64 * nodes + 24 * boxes + 104 * mts) / secs / 1e9, l2_peak, "GB/s"),
-        "hbm": ((64 * nodes + 24 * boxes + 104 * mts) / secs / 1e9, HBM_PEAK_GBS, "GB/s"),
+        "fp64": ((f64 + (28 + 18) * mts) / secs / 1e12, fp64_peak, "TFLOP/s"),
+        "fp32": ((f32 + 18 * boxes) / secs / 1e12, fp32_peak, "TFLOP/s"),
+        "l2": ((nbytes + 24 * boxes + 104 * mts) / secs / 1e9, l2_peak, "GB/s"),
+        "hbm": ((nbytes + 24 * boxes + 104 * mts) / secs / 1e9, HBM_PEAK_GBS, "GB/s"),
     }
     best = max(pipes, key=lambda k: pipes[k][0] / pipes[k][1])
     a, p, u = pipes[best]

@@ -169,7 +169,7 @@ class TraceStats(ctypes.Structure):
         ("tail_tri_tests", ctypes.c_longlong), ("tail_newton_iters", ctypes.c_longlong),
         ("launches", ctypes.c_longlong),
         ("guess_used", ctypes.c_longlong), ("guess_fallback", ctypes.c_longlong), ("guess_ms", ctypes.c_double),
-        ("off_patch", ctypes.c_longlong),
+        ("off_patch", ctypes.c_longlong), ("node_tests_fp64", ctypes.c_longlong),
     ]
 
     def as_dict(self):
@@ -295,6 +295,7 @@ def _declare(lib):
     lib.bbrt_measure_pipe_peak.argtypes = [I, c_double_p]
     lib.bbrt_umma_check.argtypes = [ctypes.POINTER(ctypes.c_ushort), ctypes.POINTER(ctypes.c_ushort),
                                     ctypes.POINTER(ctypes.c_float)]
+    lib.bbrt_node_test_check.argtypes = [c_double_p, c_double_p, c_double_p, LL, c_double_p, c_int_p]
     lib.bbrt_scene_set_modes.argtypes = [V, I, I]
     lib.bbrt_trace_batch.argtypes = [ctypes.POINTER(V), I, ctypes.POINTER(V), ctypes.POINTER(V), c_ll_p, I,
                                      ctypes.POINTER(TraceOut), ctypes.POINTER(TraceStats), c_double_p]

@@ -17,6 +17,7 @@
 #include <cstring>
 #include <filesystem>
 #include <initializer_list>
+#include <limits>
 #include <memory>
 #include <mutex>
 #include <numeric>
@@ -58,6 +59,8 @@ cudaError_t noalloc_prepare();
 cudaError_t launch_trace_noalloc(const DScene& S, TraceArgs A, bool count_hits, long long* hit_counts_out,
                                  long long* host_stats, cudaStream_t stream, int sm_count);
 int launch_umma_check(const uint16_t* A, const uint16_t* B, float* D, int* err, cudaStream_t st);
+cudaError_t launch_node_check(const DScene& S, const double* o, const double* d, const double* best, long long n,
+                              const double* boxes, int* out, cudaStream_t stream);
 cudaError_t launch_bounce_rays(const double* frames, const double* trig, int theta_n, int phi_n, long long n,
                                double* org, double* dir, cudaStream_t st);
 cudaError_t launch_bounce_reduce(const int* status, const int* bounces, long long points, int dirs_per, int* max_out,
@@ -379,6 +382,44 @@ int device_setup(bbrt_scene* s) {
     return BBRT_OK;
 }
 
+// Per-axis bound on |coordinate| over a scene's node boxes for the FP32
+// node test's error margin (rounded up to FP32, at least 2^-60); the FP32
+// test is off for the scene when a bound exceeds 2^40 or a coordinate is
+// not finite.
+void node_bounds(const double* box, size_t n_values, bbrt::DScene& D) {
+    double bound[3] = { std::ldexp(1.0, -60), std::ldexp(1.0, -60), std::ldexp(1.0, -60) };
+    bool finite = true;
+    for (size_t k = 0; k < n_values; ++k) {
+        finite = finite && std::isfinite(box[k]);
+        bound[k % 3] = std::max(bound[k % 3], std::fabs(box[k]));
+    }
+    D.node_f32_ok = finite ? 1 : 0;
+    for (int a = 0; a < 3; ++a) {
+        if (!(bound[a] <= std::ldexp(1.0, 40))) {
+            D.node_f32_ok = 0;
+            bound[a] = std::ldexp(1.0, 40);
+        }
+        float f = static_cast<float>(bound[a]);
+        if (static_cast<double>(f) < bound[a]) f = std::nextafter(f, std::numeric_limits<float>::infinity());
+        D.node_bound[a] = f;
+    }
+}
+
+// Uploads a scene's BVH node tables: FP64 boxes and links, and the FP32
+// boxes (nearest rounding) of the FP32 node test with their bounds.
+int upload_node_tables(bbrt_scene* s, const std::vector<double>& nbox, const std::vector<int>& nlink) {
+    bbrt::DScene& D = s->dev;
+    int rc;
+    if ((rc = s->upload(nbox, D.node_box))) return rc;
+    if ((rc = s->upload(nlink, D.node_link))) return rc;
+    const std::vector<float> box32(nbox.begin(), nbox.end());
+    node_bounds(nbox.data(), nbox.size(), D);
+    if ((rc = s->upload(box32, D.node_box32))) return rc;
+    if (reinterpret_cast<uintptr_t>(D.node_box32) % 16 != 0)
+        return fail(BBRT_ERR_CUDA, "bbrt_scene_upload: node box array not 16-byte aligned");
+    return BBRT_OK;
+}
+
 int ensure_uploaded(bbrt_scene* s) {
     if (s->uploaded) return BBRT_OK;
     int rc0 = ensure_device(s);
@@ -436,8 +477,7 @@ int ensure_uploaded(bbrt_scene* s) {
     D.smem_nodes = static_cast<int>(std::min<size_t>(nn, 3400));
     for (int q = 0; q < H.n_patches; ++q) D.max_nodes = std::max(D.max_nodes, std::max(H.p_imax[q], H.p_jmax[q]));
     int rc;
-    if ((rc = s->upload(nbox, D.node_box))) return rc;
-    if ((rc = s->upload(nlink, D.node_link))) return rc;
+    if ((rc = upload_node_tables(s, nbox, nlink))) return rc;
     if ((rc = s->upload(H.leaf_objects, D.leaf_objects))) return rc;
     if ((rc = s->upload(H.kind, D.obj_kind))) return rc;
     if ((rc = s->upload(H.sub, D.obj_sub))) return rc;
@@ -577,6 +617,7 @@ void fill_stats(bbrt_scene* s, const long long* st, long long n, float kernel_ms
     out->guess_used = st[bbrt::ST_GUESS_USED];
     out->guess_fallback = st[bbrt::ST_GUESS_FALLBACK];
     out->off_patch = st[bbrt::ST_OFF_PATCH];
+    out->node_tests_fp64 = st[bbrt::ST_NODE_F64];
     double* dst[5] = { &out->order_ms, &out->advance_ms, &out->newton_ms, &out->tail_ms, &out->guess_ms };
     for (const auto& sp : s->kspans) {
         float ms = 0.0f;
@@ -626,6 +667,7 @@ struct Tuning {
     int child_test = -1;              // k_advance child tests: -1 when the BVH exceeds the staged nodes, 0 / 1
     int half_stage1 = 1;              // k_advance stage 1 of two patches at a time by half-warps
     int quarter_stage1 = 0;           // ... four at a time by quarter-warps
+    int node_f32 = 1;                 // BVH nodes tested in FP32, FP64 where FP32 cannot decide (k_advance, tail)
 };
 
 // Launch-shape knobs; defaults tuned on B200, overridable for experiments by
@@ -651,6 +693,7 @@ const Tuning& tuning() {
         if (const char* e = std::getenv("BBRT_CHILD_TEST")) v.child_test = std::atoi(e);
         if (const char* e = std::getenv("BBRT_HALF_S1")) v.half_stage1 = std::atoi(e);
         if (const char* e = std::getenv("BBRT_QUARTER_S1")) v.quarter_stage1 = std::atoi(e);
+        if (const char* e = std::getenv("BBRT_NODE_F32")) v.node_f32 = std::atoi(e);
         return v;
     }();
     return t;
@@ -792,7 +835,8 @@ int build_wave_graph(bbrt_scene* s, const bbrt::TraceArgs& A, const bbrt_tuning&
     W.resume_queries = tuning().resume_queries;
     W.child_test = tuning().child_test;
     W.half_stage1 = tuning().half_stage1;
-        W.quarter_stage1 = tuning().quarter_stage1;
+    W.quarter_stage1 = tuning().quarter_stage1;
+    W.node_f32 = tuning().node_f32;
     W.group_newton = tuning().group_newton;
     W.watchdog_cycles = watchdog_cycles(T);
     W.n_runnable = n;   // sizes the persistent grid; later rounds read their count
@@ -920,7 +964,7 @@ int launch_wave_graph(bbrt_scene* s, const bbrt::TraceArgs& A, const bbrt_tuning
                          static_cast<long long>(T.order_rays), static_cast<long long>(T.warp_tail), T.wave_tail,
                          static_cast<long long>(tuning().resume_queries), static_cast<long long>(tuning().group_newton),
                          static_cast<long long>(tuning().tail_shape), static_cast<long long>(tuning().quarter_stage1),
-                         max_rounds,
+                         static_cast<long long>(tuning().node_f32), max_rounds,
                          static_cast<long long>(sort_round_requests(s)), watchdog_cycles(T), mma_wait_cycles(T),
                          static_cast<long long>(A.off_patch_miss) })
         k.put(x);
@@ -992,6 +1036,7 @@ struct WaveRun {
         W.child_test = tuning().child_test;
         W.half_stage1 = tuning().half_stage1;
         W.quarter_stage1 = tuning().quarter_stage1;
+        W.node_f32 = tuning().node_f32;
         W.group_newton = tuning().group_newton;
         W.watchdog_cycles = watchdog_cycles(T);
         W.runnable = nullptr;
@@ -1930,6 +1975,34 @@ BBRT_API int bbrt_umma_check(const uint16_t* a, const uint16_t* b, float* d) {
     return BBRT_OK;
 }
 
+BBRT_API int bbrt_node_test_check(const double* o, const double* d, const double* best_t, long long n,
+                                  const double* boxes, int* out) {
+    if (n < 0 || (n > 0 && (!o || !d || !best_t || !boxes || !out)))
+        return fail(BBRT_ERR_ARG, "bbrt_node_test_check: NULL argument or negative count");
+    if (n == 0) return BBRT_OK;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0)
+        return fail(BBRT_ERR_CUDA, "bbrt: no CUDA device available (the trace path has no CPU fallback)");
+    bbrt::DScene S;
+    node_bounds(boxes, static_cast<size_t>(6 * n), S);
+    const size_t n3 = sizeof(double) * 3 * n, n1 = sizeof(double) * n, n6 = sizeof(double) * 6 * n,
+                 no = sizeof(int) * 2 * n;
+    DevBuf bo, bd, bb, bx, bout;
+    if (bo.ensure(n3) || bd.ensure(n3) || bb.ensure(n1) || bx.ensure(n6) || bout.ensure(no))
+        return fail(BBRT_ERR_CUDA, "bbrt_node_test_check: cudaMalloc failed");
+    cudaError_t e = cudaMemcpy(bo.p, o, n3, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(bd.p, d, n3, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(bb.p, best_t, n1, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(bx.p, boxes, n6, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = bbrt::launch_node_check(S, static_cast<const double*>(bo.p), static_cast<const double*>(bd.p),
+                                    static_cast<const double*>(bb.p), n, static_cast<const double*>(bx.p),
+                                    static_cast<int*>(bout.p), nullptr);
+    if (e == cudaSuccess) e = cudaMemcpy(out, bout.p, no, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return fail(BBRT_ERR_CUDA, std::string("bbrt_node_test_check: ") + cudaGetErrorString(e));
+    return BBRT_OK;
+}
+
 // ---- arithmetic modes and the learned guess --------------------------------
 
 BBRT_API int bbrt_scene_set_modes(bbrt_scene_t s, int precision, int guess) {
@@ -2512,6 +2585,7 @@ BBRT_API int bbrt_trace_batch(const bbrt_scene_t* scenes, int n_scenes, const do
             stats->guess_used += one.guess_used;
             stats->guess_fallback += one.guess_fallback;
             stats->off_patch += one.off_patch;
+            stats->node_tests_fp64 += one.node_tests_fp64;
         }
         if (batch_ms) stats->kernel_ms = stats->total_ms = *batch_ms;
     }
@@ -2709,8 +2783,7 @@ int build_scene_set(const std::vector<bbrt_scene*>& mem, bbrt_scene_set* set) {
     D.n_blocks_side = cull_blocks;
     D.cull_enabled = 0;   // per member (m_param); a ray without a member never occurs in a set
     D.n_members = M;
-    if ((rc = S.upload(nbox, D.node_box))) return rc;
-    if ((rc = S.upload(nlink, D.node_link))) return rc;
+    if ((rc = upload_node_tables(&S, nbox, nlink))) return rc;
     if ((rc = S.upload(HM.leaf_objects, D.leaf_objects))) return rc;
     if ((rc = S.upload(HM.kind, D.obj_kind))) return rc;
     if ((rc = S.upload(HM.sub, D.obj_sub))) return rc;

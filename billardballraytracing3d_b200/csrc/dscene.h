@@ -31,6 +31,13 @@ struct DScene {
                                            //               leaf:     start, -1, count, 0
     const int* leaf_objects = nullptr;
     int smem_nodes = 0;                    // nodes [0, smem_nodes) staged in shared memory
+    // FP32 copies of the node boxes (nearest rounding) for the FP32 node
+    // test, and per axis a bound on |coordinate| over every node box (FP32,
+    // rounded up, at least 2^-60); node_f32_ok = 0 when a bound exceeds 2^40
+    // (the test then stays FP64).
+    const float* node_box32 = nullptr;     // [n_nodes][6]
+    float node_bound[3] = { 0.0f, 0.0f, 0.0f };
+    int node_f32_ok = 0;
 
     // objects
     const int* obj_kind = nullptr;         // BBRT_OBJ_*
@@ -91,6 +98,8 @@ enum StatSlot {
     ST_GUESS_USED, ST_GUESS_FALLBACK,
     // learned form: patches whose Newton root lay outside the patch, taken as not hit
     ST_OFF_PATCH,
+    // FP32 node test: node tests it left undecided (run in FP64)
+    ST_NODE_F64,
     ST_COUNT
 };
 
@@ -197,6 +206,10 @@ struct WaveArgs {
     NewtonRequest* next_req = nullptr;
     // k_advance stops (counters[3] set) once it has run this many SM cycles.
     long long watchdog_cycles = 1LL << 35;
+    // k_advance and the warp-per-ray tail test BVH nodes in FP32
+    // (node_box_f32), in FP64 only where the FP32 interval does not decide;
+    // the visit sequence is unchanged.
+    int node_f32 = 0;
 };
 
 // Round counters of the wavefront trace in device memory: [0..3] as

@@ -42,11 +42,12 @@ struct CountersT {
     static constexpr bool kOn = true;
     long long node_tests = 0, patch_tests = 0, cell_tests = 0, tri_tests = 0, newton_iters = 0;
     long long off_patch = 0;   // learned form: Newton roots outside their patch taken as misses
+    long long node_f64 = 0;    // node tests the FP32 test left to the FP64 one
 };
 template <>
 struct CountersT<false> {
     static constexpr bool kOn = false;
-    NoCount node_tests, patch_tests, cell_tests, tri_tests, newton_iters, off_patch;
+    NoCount node_tests, patch_tests, cell_tests, tri_tests, newton_iters, off_patch, node_f64;
 };
 using Counters = CountersT<true>;
 
@@ -110,6 +111,59 @@ __device__ __forceinline__ bool cull_box(const float* __restrict__ b, const Cull
     t1 = (b23.x - c.delta - c.oz) * c.iz; t2 = (b45.y + c.delta - c.oz) * c.iz;
     tmin = fmaxf(tmin, fminf(t1, t2)); tmax = fminf(tmax, fmaxf(t1, t2));
     return tmin <= tmax;
+}
+
+// FP32 BVH node test that reproduces ray_box_exact's decision or defers it.
+//
+// ray_box_exact(o, 1/d, box, best_t) passes exactly when, over the three
+// axes, tmin = max(lo_a) <= tmax = min(hi_a), tmin <= best_t and tmax >= 0,
+// where lo_a / hi_a are the FP64 slab times fl(fl(b - o) * fl(1/d)) of the
+// near / far face (its early exit and swap give that; every t is finite for
+// finite o and 1/d).  The same times in FP32 from b32 = fl32(b), o32 =
+// fl32(o) and 1/fl32(d) (the cull ray's values), each face
+// fl32(fl32(b32 - o32) * i32), differ from the FP64 ones by at most
+// (5 * 2^-24 + 2 * 2^-53) (|b| + |o|) |1/d| plus underflow terms below 2^-120
+// (roundings of b and o: 1, of d and the division: 2, of the subtraction and
+// the product: 1 each, in units of 2^-24 (|b| + |o|) |1/d|); e
+// (node_margin) bounds that with 2^-21 (B_a + |o32_a|) |i32_a| for the
+// largest axis, B_a bounding every node coordinate on axis a.  So
+// [tmin32 - e, tmin32 + e] holds the FP64 tmin and likewise tmax, and the
+// test decides wherever the interval decides: 1 = passes, 0 = fails, -1 =
+// undecided (run ray_box_exact).  Boxes are 6 floats (min xyz, max xyz) on a
+// 24-byte stride, read as three 8-byte loads.
+__device__ __forceinline__ int node_box_f32(const float* __restrict__ b, const CullRay& c, float e, double best_t) {
+    const float2 b01 = *reinterpret_cast<const float2*>(b);
+    const float2 b23 = *reinterpret_cast<const float2*>(b + 2);
+    const float2 b45 = *reinterpret_cast<const float2*>(b + 4);
+    float t1 = (b01.x - c.ox) * c.ix, t2 = (b23.y - c.ox) * c.ix;
+    float tmin = fminf(t1, t2), tmax = fmaxf(t1, t2);
+    t1 = (b01.y - c.oy) * c.iy; t2 = (b45.x - c.oy) * c.iy;
+    tmin = fmaxf(tmin, fminf(t1, t2)); tmax = fminf(tmax, fmaxf(t1, t2));
+    t1 = (b23.x - c.oz) * c.iz; t2 = (b45.y - c.oz) * c.iz;
+    tmin = fmaxf(tmin, fminf(t1, t2)); tmax = fminf(tmax, fmaxf(t1, t2));
+    const float lo_dn = __fsub_rd(tmin, e), lo_up = __fadd_ru(tmin, e);
+    const float hi_dn = __fsub_rd(tmax, e), hi_up = __fadd_ru(tmax, e);
+    if (lo_dn > hi_up || hi_up < 0.0f || static_cast<double>(lo_dn) > best_t) return 0;
+    if (lo_up <= hi_dn && hi_dn >= 0.0f && static_cast<double>(lo_up) <= best_t) return 1;
+    return -1;
+}
+
+// The margin e of node_box_f32 for a ray (false: the ray's FP32 values lie
+// outside the range the bound covers, and its node tests stay FP64).  The
+// limits keep every FP32 time below 2^81 and 1/d normal; the 2^-100 floor
+// covers the underflow terms.
+__device__ __forceinline__ bool node_margin(const DScene& S, const CullRay& c, float& e) {
+    const float o[3] = { c.ox, c.oy, c.oz }, iv[3] = { c.ix, c.iy, c.iz };
+    float m = 0x1p-100f;
+    bool ok = S.node_f32_ok != 0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float ai = fabsf(iv[a]), ao = fabsf(o[a]);
+        ok = ok && ai >= 0x1p-40f && ai <= 0x1p40f && ao <= 0x1p40f;
+        m = fmaxf(m, __fmul_ru(__fadd_ru(S.node_bound[a], ao), ai) * 0x1p-21f);
+    }
+    e = m;
+    return ok;
 }
 
 // Stage-1 winner bookkeeping.  key = ((cell * 3 + sign) * 2 + triangle) is
@@ -460,6 +514,7 @@ __device__ __forceinline__ void flush_stats(const TraceArgs& A, const Ctr& ctr, 
     warp_add(A.stats + ST_TRI_TESTS, ctr.tri_tests);
     warp_add(A.stats + ST_NEWTON_ITERS, ctr.newton_iters);
     warp_add(A.stats + ST_OFF_PATCH, ctr.off_patch);
+    warp_add(A.stats + ST_NODE_F64, ctr.node_f64);
 #pragma unroll
     for (int k = 0; k < BBRT_RAY_STATUS_COUNT; ++k) warp_add(A.stats + ST_HIST0 + k, t.hist[k]);
 }
@@ -745,7 +800,9 @@ struct AdvState {
     double inv[3];
     bool neg[3];
     bool use_cull;
-    CullRay cr;
+    bool node32;     // node boxes tested in FP32 (node_box_f32) with margin e32
+    float e32;
+    CullRay cr;      // also the FP32 origin and 1/d of the FP32 node test
     double best_t;
     int best_ver;    // times best_t went down in this query, saturating at kStackAlways
     int best_obj;    // -1: no hit yet
@@ -772,8 +829,8 @@ constexpr unsigned kStackAlways = 0xFFu;
 constexpr unsigned kStackIdx = 0x00FFFFFFu;
 __device__ __forceinline__ int stack_entry(int idx, unsigned ver) { return static_cast<int>((ver << 24) | static_cast<unsigned>(idx)); }
 
-__device__ __forceinline__ void adv_start_query(const DScene& S, const TraceArgs& A, const RayCtx& r, AdvState& q,
-                                                int* stack) {
+__device__ __forceinline__ void adv_start_query(const DScene& S, const TraceArgs& A, const WaveArgs& W,
+                                                const RayCtx& r, AdvState& q, int* stack) {
     q.inv[0] = 1.0 / r.d.x;
     q.inv[1] = 1.0 / r.d.y;
     q.inv[2] = 1.0 / r.d.z;
@@ -781,7 +838,9 @@ __device__ __forceinline__ void adv_start_query(const DScene& S, const TraceArgs
     q.neg[1] = q.inv[1] < 0.0;
     q.neg[2] = q.inv[2] < 0.0;
     q.use_cull = cull_ok(S, r.member, A.cull, r.o, r.d);
-    if (q.use_cull) q.cr = make_cull_ray(S, r.member, r.o, r.d);
+    q.node32 = W.node_f32 && finite3(r.o) && finite3(r.d);
+    if (q.use_cull || q.node32) q.cr = make_cull_ray(S, r.member, r.o, r.d);
+    if (q.node32) q.node32 = node_margin(S, q.cr, q.e32);
     q.best_t = CUDART_INF;
     q.best_ver = 0;
     q.best_obj = -1;
@@ -791,6 +850,22 @@ __device__ __forceinline__ void adv_start_query(const DScene& S, const TraceArgs
     q.ev0 = q.ev1 = 0.0;
     q.sp = 0;
     stack[q.sp++] = stack_entry(root_node(S, r.member), kStackAlways);
+}
+
+// One BVH node test of k_advance: in FP32 where the ray allows it and the
+// FP32 interval decides (node_box_f32), else ray_box_exact, on FP64 boxes
+// from the shared-memory copy when it holds them (n64 nodes; n32 FP32 boxes
+// otherwise), else from global memory.
+template <class Ctr>
+__device__ __forceinline__ bool adv_node_pass(const DScene& S, const RayCtx& r, const AdvState& q, int idx,
+                                              const double* sbox, const float* sbox32, int n64, int n32, Ctr& c) {
+    int dec = -1;
+    if (q.node32) dec = node_box_f32(idx < n32 ? sbox32 + 6 * idx : S.node_box32 + 6LL * idx, q.cr, q.e32, q.best_t);
+    if (dec < 0) {
+        if (q.node32) ++c.node_f64;
+        dec = ray_box_exact(r.o, q.inv, idx < n64 ? sbox + 6 * idx : S.node_box + 6LL * idx, q.best_t);
+    }
+    return dec != 0;
 }
 
 // Keeps the traversal state of a query that suspends for a Newton solve
@@ -825,7 +900,7 @@ __device__ __forceinline__ bool resume_query(const DScene& S, const TraceArgs& A
     const int* qi = W.qs_int + i * kQsInt;
     const int sp = qi[0];
     if (sp < 0) return false;
-    adv_start_query(S, A, r, q, stack);
+    adv_start_query(S, A, W, r, q, stack);
     q.sp = sp;
     q.leaf_start = qi[1];
     q.leaf_count = qi[2];
@@ -865,11 +940,16 @@ __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, Wav
     const int n = S.coarse_n, nc = n - 1, NB = S.n_blocks_side, B = S.block_cells;
     const int lane = threadIdx.x & 31;
     // The first S.smem_nodes BVH nodes (breadth-first order: the top levels)
-    // are staged in shared memory for the whole launch.
+    // are staged in shared memory for the whole launch: their FP64 boxes, or
+    // with the FP32 node test their FP32 boxes (24 instead of 48 bytes a node),
+    // and their links.
     extern __shared__ __align__(16) double smem_bvh[];
+    const int n64 = W.node_f32 ? 0 : S.smem_nodes, n32 = W.node_f32 ? S.smem_nodes : 0;
     double* sbox = smem_bvh;
-    int* slink = reinterpret_cast<int*>(smem_bvh + 6 * S.smem_nodes);
-    for (int k = threadIdx.x; k < 6 * S.smem_nodes; k += blockDim.x) sbox[k] = S.node_box[k];
+    float* sbox32 = reinterpret_cast<float*>(smem_bvh);
+    int* slink = W.node_f32 ? reinterpret_cast<int*>(sbox32 + 6 * n32) : reinterpret_cast<int*>(sbox + 6 * n64);
+    for (int k = threadIdx.x; k < 6 * n64; k += blockDim.x) sbox[k] = S.node_box[k];
+    for (int k = threadIdx.x; k < 6 * n32; k += blockDim.x) sbox32[k] = S.node_box32[k];
     for (int k = threadIdx.x; k < 4 * S.smem_nodes; k += blockDim.x) slink[k] = S.node_link[k];
     __syncthreads();
     // Runnable rays of this round: the host's count, or (graph-launched
@@ -898,8 +978,7 @@ __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, Wav
                 bool pass = true;
                 if (tag == kStackAlways || tag != static_cast<unsigned>(q.best_ver)) {
                     ++cray.node_tests;
-                    pass = ray_box_exact(r.o, q.inv, idx < S.smem_nodes ? sbox + 6 * idx : S.node_box + 6LL * idx,
-                                         q.best_t);
+                    pass = adv_node_pass(S, r, q, idx, sbox, sbox32, n64, n32, ctr);
                 }
                 if (pass) {
                     const int* link = idx < S.smem_nodes ? slink + 4 * idx : S.node_link + 4LL * idx;
@@ -922,10 +1001,8 @@ __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, Wav
                         // both children's boxes now (independent loads); a
                         // child that fails would fail when popped as well
                         const int left = link[0], right = link[1];
-                        const bool pl = ray_box_exact(
-                            r.o, q.inv, left < S.smem_nodes ? sbox + 6 * left : S.node_box + 6LL * left, q.best_t);
-                        const bool pr = ray_box_exact(
-                            r.o, q.inv, right < S.smem_nodes ? sbox + 6 * right : S.node_box + 6LL * right, q.best_t);
+                        const bool pl = adv_node_pass(S, r, q, left, sbox, sbox32, n64, n32, ctr);
+                        const bool pr = adv_node_pass(S, r, q, right, sbox, sbox32, n64, n32, ctr);
                         cray.node_tests += 2;
                         const unsigned v = static_cast<unsigned>(q.best_ver);
                         if (q.neg[link[3]]) {
@@ -1097,7 +1174,7 @@ __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, Wav
                 r.status = BBRT_RAY_MAX_BOUNCES;
                 mode = M_FINISH;
             } else {
-                adv_start_query(S, A, r, q, stack);
+                adv_start_query(S, A, W, r, q, stack);
                 mode = M_NODE;
             }
         }
@@ -1253,7 +1330,7 @@ __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, Wav
                     } else if (r.bounces >= A.max_bounces) {
                         r.status = BBRT_RAY_MAX_BOUNCES;
                     } else {
-                        adv_start_query(S, A, r, q, stack);
+                        adv_start_query(S, A, W, r, q, stack);
                         mode = M_NODE;
                     }
                 }
@@ -1452,7 +1529,8 @@ __global__ void __launch_bounds__(128) k_resume(DScene S, TraceArgs A, WaveArgs 
 // Nodes [0, staged) are read from the shared-memory copy (sbox, slink).
 template <class Ctr>
 __device__ QHit warp_bvh_query(const DScene& S, const V3& o, const V3& d, int cull_flag, int lane, Ctr& ctr,
-                               const double* sbox, const int* slink, int staged, bool off_patch_miss, int member) {
+                               const double* sbox, const float* sbox32, const int* slink, int staged, bool node_f32,
+                               bool off_patch_miss, int member) {
     QHit best;
     best.obj = -1;
     best.err = 0;
@@ -1460,8 +1538,11 @@ __device__ QHit warp_bvh_query(const DScene& S, const V3& o, const V3& d, int cu
     const double inv[3] = { 1.0 / d.x, 1.0 / d.y, 1.0 / d.z };
     const bool neg[3] = { inv[0] < 0.0, inv[1] < 0.0, inv[2] < 0.0 };
     const bool use_cull = cull_ok(S, member, cull_flag, o, d);
+    bool node32 = node_f32 && finite3(o) && finite3(d);
     CullRay cr;
-    if (use_cull) cr = make_cull_ray(S, member, o, d);
+    if (use_cull || node32) cr = make_cull_ray(S, member, o, d);
+    float e32 = 0.0f;
+    if (node32) node32 = node_margin(S, cr, e32);
     double best_t = CUDART_INF;
     int stack[64];
     int sp = 0;
@@ -1470,7 +1551,14 @@ __device__ QHit warp_bvh_query(const DScene& S, const V3& o, const V3& d, int cu
         const int idx = stack[--sp];
         if (lane == 0) ++ctr.node_tests;
         const bool in_smem = idx < staged;
-        if (!ray_box_exact(o, inv, in_smem ? sbox + 6 * idx : S.node_box + 6LL * idx, best_t)) continue;
+        // FP32 node test where it decides (the staged copy then holds FP32 boxes)
+        int dec = -1;
+        if (node32) dec = node_box_f32(in_smem ? sbox32 + 6 * idx : S.node_box32 + 6LL * idx, cr, e32, best_t);
+        if (dec < 0) {
+            if (node32 && lane == 0) ++ctr.node_f64;
+            dec = ray_box_exact(o, inv, in_smem && !node_f32 ? sbox + 6 * idx : S.node_box + 6LL * idx, best_t);
+        }
+        if (!dec) continue;
         const int* link = in_smem ? slink + 4 * idx : S.node_link + 4LL * idx;
         if (link[1] < 0) {
             const int start = link[0], count = link[2];
@@ -1534,9 +1622,17 @@ template <int MINB, bool STATS>
 __global__ void __launch_bounds__(128, MINB) k_resume_warp(DScene S, TraceArgs A, WaveArgs W,
                                                            const NewtonRequest* reqs, const int* rays, long long n) {
     extern __shared__ __align__(16) double smem_tail[];
+    // staged nodes: FP64 boxes, or FP32 boxes with the FP32 node test, then links
+    const bool f32 = W.node_f32 != 0;
     double* sbox = smem_tail;
-    int* slink = reinterpret_cast<int*>(smem_tail + 6 * S.smem_nodes);
-    for (int k = threadIdx.x; k < 6 * S.smem_nodes; k += blockDim.x) sbox[k] = S.node_box[k];
+    float* sbox32 = reinterpret_cast<float*>(smem_tail);
+    int* slink = f32 ? reinterpret_cast<int*>(sbox32 + 6 * S.smem_nodes)
+                     : reinterpret_cast<int*>(smem_tail + 6 * S.smem_nodes);
+    if (f32) {
+        for (int k = threadIdx.x; k < 6 * S.smem_nodes; k += blockDim.x) sbox32[k] = S.node_box32[k];
+    } else {
+        for (int k = threadIdx.x; k < 6 * S.smem_nodes; k += blockDim.x) sbox[k] = S.node_box[k];
+    }
     for (int k = threadIdx.x; k < 4 * S.smem_nodes; k += blockDim.x) slink[k] = S.node_link[k];
     __syncthreads();
     if (W.count_dev) n = *W.count_dev;
@@ -1563,7 +1659,7 @@ __global__ void __launch_bounds__(128, MINB) k_resume_warp(DScene S, TraceArgs A
         while (r.status < 0) {
             if (r.bounces >= A.max_bounces) { r.status = BBRT_RAY_MAX_BOUNCES; break; }
             if (lane == 0) ++tally.queries;
-            const QHit h = warp_bvh_query(S, r.o, r.d, A.cull, lane, c1, sbox, slink, S.smem_nodes,
+            const QHit h = warp_bvh_query(S, r.o, r.d, A.cull, lane, c1, sbox, sbox32, slink, S.smem_nodes, f32,
                                           A.off_patch_miss != 0, r.member);
             if (!step_ray(S, A, i, r, h, lane == 0)) break;
         }
@@ -1579,6 +1675,7 @@ __global__ void __launch_bounds__(128, MINB) k_resume_warp(DScene S, TraceArgs A
         ctr.tri_tests += c1.tri_tests;
         ctr.newton_iters += c1.newton_iters;
         ctr.off_patch += c1.off_patch;
+        ctr.node_f64 += c1.node_f64;
     }
     flush_stats(A, ctr, tally, true);
 }
@@ -1762,7 +1859,8 @@ size_t wave_workspace_bytes(long long n) { return wave_bytes_per_ray() * n + 20 
 template <int NT, int MINB, bool CHILD, int G, bool STATS>
 static cudaError_t launch_advance_stats(const DScene& Sl, const TraceArgs& A, const WaveArgs& W, int sm_count,
                                         cudaStream_t stream) {
-    const size_t smem = static_cast<size_t>(Sl.smem_nodes) * (6 * sizeof(double) + 4 * sizeof(int));
+    const size_t smem = static_cast<size_t>(Sl.smem_nodes) *
+                        ((W.node_f32 ? 6 * sizeof(float) : 6 * sizeof(double)) + 4 * sizeof(int));
     cudaError_t e = cudaFuncSetAttribute(k_advance<NT, MINB, CHILD, G, STATS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess) return e;
@@ -1795,7 +1893,12 @@ template <int NT, int MINB>
 static cudaError_t launch_advance_shape(const DScene& S, const TraceArgs& A, const WaveArgs& W, int sm_count,
                                         int max_smem_nodes, cudaStream_t stream) {
     DScene Sl = S;
-    if (Sl.smem_nodes > max_smem_nodes) Sl.smem_nodes = max_smem_nodes;
+    if (W.node_f32) {
+        // 40 instead of 64 bytes a staged node: the same shared memory holds 1.6 x the nodes
+        Sl.smem_nodes = static_cast<int>(std::min<long long>(S.n_nodes, max_smem_nodes * 64LL / 40));
+    } else if (Sl.smem_nodes > max_smem_nodes) {
+        Sl.smem_nodes = max_smem_nodes;
+    }
     // Half-warp stage 1 where a patch's blocks and a block's cells fit 16
     // lanes; else child tests when part of the tree stays in global memory.
     // The two together measured slower than either, and on both measured
@@ -1885,7 +1988,8 @@ static cudaError_t launch_resume_warp_stats(const DScene& S, const TraceArgs& A,
                                             int max_smem_nodes, cudaStream_t stream) {
     DScene Sl = S;
     if (Sl.smem_nodes > max_smem_nodes) Sl.smem_nodes = max_smem_nodes;
-    const size_t smem = static_cast<size_t>(Sl.smem_nodes) * (6 * sizeof(double) + 4 * sizeof(int));
+    const size_t smem = static_cast<size_t>(Sl.smem_nodes) *
+                        ((W.node_f32 ? 6 * sizeof(float) : 6 * sizeof(double)) + 4 * sizeof(int));
     cudaError_t e = cudaFuncSetAttribute(k_resume_warp<MINB, STATS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess) return e;
@@ -1981,6 +2085,33 @@ cudaError_t launch_bounce_reduce(const int* status, const int* bounces, long lon
     if (points <= 0) return cudaSuccess;
     k_bounce_reduce<<<static_cast<unsigned>((points + 127) / 128), 128, 0, st>>>(status, bounces, points, dirs_per,
                                                                               max_out, err_out, best_out);
+    return cudaGetLastError();
+}
+
+// Check of the FP32 node test (bbrt_node_test_check): ray i against box i
+// with bound t best[i]: out[2i] = ray_box_exact, out[2i + 1] = node_box_f32
+// (-2 when the ray's FP32 values are outside the bound's range).
+__global__ void k_node_check(DScene S, const double* __restrict__ o, const double* __restrict__ d,
+                             const double* __restrict__ best, long long n, const double* __restrict__ boxes,
+                             int* __restrict__ out) {
+    const long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (i >= n) return;
+    const V3 oo = load3(o + 3 * i), dd = load3(d + 3 * i);
+    const double inv[3] = { 1.0 / dd.x, 1.0 / dd.y, 1.0 / dd.z };
+    out[2 * i] = ray_box_exact(oo, inv, boxes + 6 * i, best[i]) ? 1 : 0;
+    const CullRay c = make_cull_ray(S, -1, oo, dd);
+    float e = 0.0f;
+    __align__(8) float b32[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) b32[k] = static_cast<float>(boxes[6 * i + k]);
+    const bool ok = finite3(oo) && finite3(dd) && node_margin(S, c, e);
+    out[2 * i + 1] = ok ? node_box_f32(b32, c, e, best[i]) : -2;
+}
+
+cudaError_t launch_node_check(const DScene& S, const double* o, const double* d, const double* best, long long n,
+                              const double* boxes, int* out, cudaStream_t stream) {
+    if (n <= 0) return cudaSuccess;
+    k_node_check<<<static_cast<unsigned>((n + 255) / 256), 256, 0, stream>>>(S, o, d, best, n, boxes, out);
     return cudaGetLastError();
 }
 

@@ -226,6 +226,7 @@ typedef struct bbrt_trace_stats {
     double guess_ms;          /* learned-guess inference kernels */
     long long off_patch;      /* learned form: patch queries whose Newton root lay outside the patch,
                                  taken as "not hit" instead of a Newton failure of the ray */
+    long long node_tests_fp64;  /* BVH node tests the FP32 test left undecided, re-run in FP64 */
 } bbrt_trace_stats;
 
 /* ---- library ---------------------------------------------------------- */
@@ -516,6 +517,17 @@ BBRT_API int bbrt_measure_pipe_peak(int pipe, double* value);
  * layouts the learned-guess kernels use).  BBRT_ERR_KERNEL when an MMA
  * completion wait timed out. */
 BBRT_API int bbrt_umma_check(const unsigned short* a, const unsigned short* b, float* d);
+
+/* FP32 BVH node test self-check (no reference counterpart; the FP64 test it
+ * stands in for is BVH.hpp:14-37 ray_box): for each i, ray (o[3i..],
+ * d[3i..]) against box i (boxes[6i..]: min xyz, max xyz) with bound
+ * best_t[i], out[2i] = the FP64 test (0 / 1) and out[2i + 1] = the FP32 test
+ * (1 passes, 0 fails, -1 undecided, -2 the ray's FP32 values lie outside the
+ * range its error bound covers), the margin taken from these boxes' own
+ * coordinate bound.  A decided FP32 answer must equal the FP64 one.  Host
+ * arrays. */
+BBRT_API int bbrt_node_test_check(const double* o, const double* d, const double* best_t, long long n,
+                                  const double* boxes, int* out);
 
 /* ---- allocation-free trace ------------------------------------------------
  * No counterpart in the reference (it has no device memory at all).
