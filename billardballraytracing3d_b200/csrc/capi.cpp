@@ -668,6 +668,7 @@ struct Tuning {
     int half_stage1 = 1;              // k_advance stage 1 of two patches at a time by half-warps
     int quarter_stage1 = 0;           // ... four at a time by quarter-warps
     int node_f32 = 1;                 // BVH nodes tested in FP32, FP64 where FP32 cannot decide (k_advance, tail)
+    int adapt_lanes = 1;              // small k_advance rounds: fewer rays per warp, over every warp
 };
 
 // Launch-shape knobs; defaults tuned on B200, overridable for experiments by
@@ -694,6 +695,7 @@ const Tuning& tuning() {
         if (const char* e = std::getenv("BBRT_HALF_S1")) v.half_stage1 = std::atoi(e);
         if (const char* e = std::getenv("BBRT_QUARTER_S1")) v.quarter_stage1 = std::atoi(e);
         if (const char* e = std::getenv("BBRT_NODE_F32")) v.node_f32 = std::atoi(e);
+        if (const char* e = std::getenv("BBRT_ADAPT_LANES")) v.adapt_lanes = std::atoi(e);
         return v;
     }();
     return t;
@@ -837,6 +839,7 @@ int build_wave_graph(bbrt_scene* s, const bbrt::TraceArgs& A, const bbrt_tuning&
     W.half_stage1 = tuning().half_stage1;
     W.quarter_stage1 = tuning().quarter_stage1;
     W.node_f32 = tuning().node_f32;
+    W.adapt_lanes = tuning().adapt_lanes;
     W.group_newton = tuning().group_newton;
     W.watchdog_cycles = watchdog_cycles(T);
     W.n_runnable = n;   // sizes the persistent grid; later rounds read their count
@@ -964,7 +967,8 @@ int launch_wave_graph(bbrt_scene* s, const bbrt::TraceArgs& A, const bbrt_tuning
                          static_cast<long long>(T.order_rays), static_cast<long long>(T.warp_tail), T.wave_tail,
                          static_cast<long long>(tuning().resume_queries), static_cast<long long>(tuning().group_newton),
                          static_cast<long long>(tuning().tail_shape), static_cast<long long>(tuning().quarter_stage1),
-                         static_cast<long long>(tuning().node_f32), max_rounds,
+                         static_cast<long long>(tuning().node_f32), static_cast<long long>(tuning().adapt_lanes),
+                         max_rounds,
                          static_cast<long long>(sort_round_requests(s)), watchdog_cycles(T), mma_wait_cycles(T),
                          static_cast<long long>(A.off_patch_miss) })
         k.put(x);
@@ -1037,6 +1041,7 @@ struct WaveRun {
         W.half_stage1 = tuning().half_stage1;
         W.quarter_stage1 = tuning().quarter_stage1;
         W.node_f32 = tuning().node_f32;
+        W.adapt_lanes = tuning().adapt_lanes;
         W.group_newton = tuning().group_newton;
         W.watchdog_cycles = watchdog_cycles(T);
         W.runnable = nullptr;

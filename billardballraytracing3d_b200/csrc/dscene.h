@@ -210,6 +210,9 @@ struct WaveArgs {
     // (node_box_f32), in FP64 only where the FP32 interval does not decide;
     // the visit sequence is unchanged.
     int node_f32 = 0;
+    // k_advance: in a round with fewer rays than the grid's lanes, fewer
+    // lanes of each warp take rays, spreading the round over every warp.
+    int adapt_lanes = 0;
 };
 
 // Round counters of the wavefront trace in device memory: [0..3] as

@@ -955,6 +955,20 @@ __global__ void __launch_bounds__(NT, MINB) k_advance(DScene S, TraceArgs A, Wav
     // Runnable rays of this round: the host's count, or (graph-launched
     // trace) the count the previous round's control kernel left on the device.
     const long long n_run = W.count_dev ? static_cast<long long>(*W.count_dev) : W.n_runnable;
+    // Rays per warp: a lane owns a ray, and the warp takes its lanes' stage 1s
+    // one (two) at a time, so a warp's share of a round is the sum of its
+    // rays' stage-1 work.  In a round with fewer rays than the grid has lanes
+    // (the late, small rounds) only the first ray_lanes lanes of each warp
+    // take rays (the fewest, a power of two, that still cover the round), so
+    // the round is spread over all the grid's warps instead of packed into a
+    // few full ones; the other lanes only help with the stage 1s.
+    int ray_lanes = 32;
+    if (W.adapt_lanes) {
+        const long long warps = static_cast<long long>(gridDim.x) * (blockDim.x >> 5);
+        const long long per = (n_run + warps - 1) / warps;
+        while (ray_lanes > 1 && ray_lanes / 2 >= per) ray_lanes >>= 1;
+    }
+    if (lane >= ray_lanes) mode = M_DRAINED;
     // Watchdog: a launch that runs far past any real trace (W.watchdog_cycles
     // of SM clock, about 17 s by default) records an error and ends instead
     // of holding the GPU; checked on the first iteration and every 1024th
@@ -1868,15 +1882,21 @@ static cudaError_t launch_advance_stats(const DScene& Sl, const TraceArgs& A, co
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_advance<NT, MINB, CHILD, G, STATS>, NT, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
-    // A small round (the late ones) is spread over every SM with smaller
-    // blocks rather than packed into the first few SMs with full ones.
+    // A small round (the late ones) is spread over every SM: with full blocks
+    // whose warps take fewer rays each (W.adapt_lanes, see k_advance), else
+    // with smaller blocks rather than packed into the first few SMs.
     int threads = NT;
-    const long long per_block = (W.n_runnable + static_cast<long long>(per_sm) * sm_count - 1) /
-                                (static_cast<long long>(per_sm) * sm_count);
-    if (per_block < NT) threads = static_cast<int>(std::max<long long>(32, (per_block + 31) / 32 * 32));
     long long blocks = static_cast<long long>(per_sm) * sm_count;
-    const long long need = (W.n_runnable + threads - 1) / threads;
-    if (blocks > need) blocks = need;
+    if (W.adapt_lanes) {
+        const long long need = (W.n_runnable + NT / 32 - 1) / (NT / 32);   // one ray per warp at least
+        if (blocks > need) blocks = need;
+    } else {
+        const long long per_block = (W.n_runnable + static_cast<long long>(per_sm) * sm_count - 1) /
+                                    (static_cast<long long>(per_sm) * sm_count);
+        if (per_block < NT) threads = static_cast<int>(std::max<long long>(32, (per_block + 31) / 32 * 32));
+        const long long need = (W.n_runnable + threads - 1) / threads;
+        if (blocks > need) blocks = need;
+    }
     k_advance<NT, MINB, CHILD, G, STATS><<<static_cast<unsigned>(blocks), threads, smem, stream>>>(Sl, A, W);
     return cudaGetLastError();
 }

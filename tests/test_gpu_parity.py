@@ -242,12 +242,15 @@ np.savez(sys.argv[2], **{k: g[k] for k in ("status", "bounce_count", "hit_object
                                  {"BBRT_CHILD_TEST": "1"}, {"BBRT_HALF_S1": "0"}, {"BBRT_QUARTER_S1": "1"},
                                  {"BBRT_QUARTER_S1": "1", "BBRT_GRAPH": "0"}, {"BBRT_NODE_F32": "0"},
                                  {"BBRT_NODE_F32": "0", "BBRT_GRAPH": "0"}, {"BBRT_NODE_F32": "0", "BBRT_CHILD_TEST": "1"},
-                                 {"BBRT_NODE_F32": "0", "BBRT_TAIL_SHAPE": "3", "BBRT_WAVE_TAIL": "100000"}])
+                                 {"BBRT_NODE_F32": "0", "BBRT_TAIL_SHAPE": "3", "BBRT_WAVE_TAIL": "100000"},
+                                 {"BBRT_ADAPT_LANES": "0"}, {"BBRT_ADAPT_LANES": "0", "BBRT_GRAPH": "0"},
+                                 {"BBRT_WAVE_TAIL": "0", "BBRT_GRAPH": "0", "BBRT_ADAPT_LANES": "1"}])
 def test_launch_shape_knobs_do_not_change_results(built, workloads, tmp_path, env):
     """Every schedule (all wavefront rounds, per-thread or per-warp tail, fused
     kernel only, unordered rays, host-driven or graph-launched rounds, Newton
     requests grouped by patch or not, BVH nodes tested in FP32 with an FP64
-    re-test or in FP64 only) gives the oracle's results bit for bit."""
+    re-test or in FP64 only, small rounds spread over every warp or not) gives
+    the oracle's results bit for bit."""
     import os
     import subprocess
     import sys
