@@ -651,7 +651,7 @@ cudaError_t timed(bbrt_scene* s, int kind, cudaStream_t st, F&& launch) {
 // to the end.
 struct Tuning {
     long long wave_min_rays = 8192;   // smaller batches: one ray per thread to the end
-    long long wave_tail = 16384;      // last requests finished one ray per thread
+    long long wave_tail = 4096;       // last requests finished one ray per warp
     int order_rays = 1;               // bucket rays by origin / direction before round 0
     int log_rounds = 0;               // print per-round counts and times to stderr
     int warp_tail = 1;                // finish the tail one warp per ray (else one thread per ray)
@@ -669,6 +669,7 @@ struct Tuning {
     int quarter_stage1 = 0;           // ... four at a time by quarter-warps
     int node_f32 = 1;                 // BVH nodes tested in FP32, FP64 where FP32 cannot decide (k_advance, tail)
     int adapt_lanes = 1;              // small k_advance rounds: fewer rays per warp, over every warp
+    long long newton_group_max = 32768;  // smaller Newton rounds: 8 lanes per request
 };
 
 // Launch-shape knobs; defaults tuned on B200, overridable for experiments by
@@ -696,6 +697,7 @@ const Tuning& tuning() {
         if (const char* e = std::getenv("BBRT_QUARTER_S1")) v.quarter_stage1 = std::atoi(e);
         if (const char* e = std::getenv("BBRT_NODE_F32")) v.node_f32 = std::atoi(e);
         if (const char* e = std::getenv("BBRT_ADAPT_LANES")) v.adapt_lanes = std::atoi(e);
+        if (const char* e = std::getenv("BBRT_NEWTON_GROUP_MAX")) v.newton_group_max = std::atoll(e);
         return v;
     }();
     return t;
@@ -840,6 +842,7 @@ int build_wave_graph(bbrt_scene* s, const bbrt::TraceArgs& A, const bbrt_tuning&
     W.quarter_stage1 = tuning().quarter_stage1;
     W.node_f32 = tuning().node_f32;
     W.adapt_lanes = tuning().adapt_lanes;
+    W.newton_group_max = tuning().newton_group_max;
     W.group_newton = tuning().group_newton;
     W.watchdog_cycles = watchdog_cycles(T);
     W.n_runnable = n;   // sizes the persistent grid; later rounds read their count
@@ -968,7 +971,7 @@ int launch_wave_graph(bbrt_scene* s, const bbrt::TraceArgs& A, const bbrt_tuning
                          static_cast<long long>(tuning().resume_queries), static_cast<long long>(tuning().group_newton),
                          static_cast<long long>(tuning().tail_shape), static_cast<long long>(tuning().quarter_stage1),
                          static_cast<long long>(tuning().node_f32), static_cast<long long>(tuning().adapt_lanes),
-                         max_rounds,
+                         tuning().newton_group_max, max_rounds,
                          static_cast<long long>(sort_round_requests(s)), watchdog_cycles(T), mma_wait_cycles(T),
                          static_cast<long long>(A.off_patch_miss) })
         k.put(x);
@@ -1042,6 +1045,7 @@ struct WaveRun {
         W.quarter_stage1 = tuning().quarter_stage1;
         W.node_f32 = tuning().node_f32;
         W.adapt_lanes = tuning().adapt_lanes;
+        W.newton_group_max = tuning().newton_group_max;
         W.group_newton = tuning().group_newton;
         W.watchdog_cycles = watchdog_cycles(T);
         W.runnable = nullptr;
@@ -2447,7 +2451,7 @@ BBRT_API int bbrt_scene_autotune(bbrt_scene_t s, const double* origins, const do
         rc = time_one(c, ms);
         if (!rc && ms < cur_ms) { cur = c; cur_ms = ms; }
     }
-    const long long tails[] = { 4096, 8192, 16384, 32768, 65536 };
+    const long long tails[] = { 0, 1024, 4096, 8192, 16384, 32768, 65536 };
     for (long long tl : tails) {
         if (rc || tl == cur.wave_tail) continue;
         bbrt_tuning c = cur;

@@ -213,6 +213,9 @@ struct WaveArgs {
     // k_advance: in a round with fewer rays than the grid's lanes, fewer
     // lanes of each warp take rays, spreading the round over every warp.
     int adapt_lanes = 0;
+    // Rounds of at most this many Newton requests solve each with 8 lanes
+    // (patches of at most 8 nodes per axis); 0: one request per thread always.
+    long long newton_group_max = 0;
 };
 
 // Round counters of the wavefront trace in device memory: [0..3] as

@@ -1368,8 +1368,8 @@ __device__ __forceinline__ int newton_mode(const DScene& S, int pidx, const V3& 
 // a confident guess is tried first; its root is kept only when it converges
 // inside the patch within guess_t_window patch sizes of the stage-1 t, and
 // otherwise the solve restarts from the stage-1 triangle (the reference's start).
-__global__ void __launch_bounds__(128) k_newton(DScene S, TraceArgs A, WaveArgs W, long long n_req) {
-    if (W.count_dev) n_req = *W.count_dev;
+__device__ __forceinline__ void newton_thread_body(const DScene& S, const TraceArgs& A, const WaveArgs& W,
+                                                   long long n_req) {
     if (blockIdx.x * static_cast<long long>(blockDim.x) >= n_req) return;   // graph launch: spare blocks
     const long long j = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
     long long iters = 0, iters32 = 0, used = 0, fallback = 0, off = 0;
@@ -1438,8 +1438,8 @@ __global__ void __launch_bounds__(128) k_newton(DScene S, TraceArgs A, WaveArgs 
 
 // k_newton with 8 lanes per request (patches of at most 8 nodes per axis):
 // the same starts, fallbacks and results, bit for bit.
-__global__ void __launch_bounds__(128) k_newton_grp(DScene S, TraceArgs A, WaveArgs W, long long n_req) {
-    if (W.count_dev) n_req = *W.count_dev;
+__device__ __forceinline__ void newton_grp_body(const DScene& S, const TraceArgs& A, const WaveArgs& W,
+                                                long long n_req) {
     if (blockIdx.x * static_cast<long long>(blockDim.x) / kGroup >= n_req) return;   // graph launch: spare blocks
     const Grp G = make_grp();
     const long long j = (blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x) / kGroup;
@@ -1502,6 +1502,29 @@ __global__ void __launch_bounds__(128) k_newton_grp(DScene S, TraceArgs A, WaveA
         warp_add(A.stats + ST_GUESS_FALLBACK, fallback);
         warp_add(A.stats + ST_OFF_PATCH, off);
     }
+}
+
+__global__ void __launch_bounds__(128) k_newton(DScene S, TraceArgs A, WaveArgs W, long long n_req) {
+    if (W.count_dev) n_req = *W.count_dev;
+    newton_thread_body(S, A, W, n_req);
+}
+
+__global__ void __launch_bounds__(128) k_newton_grp(DScene S, TraceArgs A, WaveArgs W, long long n_req) {
+    if (W.count_dev) n_req = *W.count_dev;
+    newton_grp_body(S, A, W, n_req);
+}
+
+// A round's Newton solves with the solver picked by the round's size: one
+// request per thread for a big round (throughput), 8 lanes per request for a
+// small one (at most W.newton_group_max requests, and the grid has their
+// lanes), whose time is its slowest solve's latency.  Same results bit for
+// bit either way.
+__global__ void __launch_bounds__(128) k_newton_auto(DScene S, TraceArgs A, WaveArgs W, long long n_req) {
+    if (W.count_dev) n_req = *W.count_dev;
+    if (n_req <= W.newton_group_max && n_req * kGroup <= static_cast<long long>(gridDim.x) * blockDim.x)
+        newton_grp_body(S, A, W, n_req);
+    else
+        newton_thread_body(S, A, W, n_req);
 }
 
 // Finishes rays from their saved state with inline queries (the tail of a
@@ -1989,6 +2012,9 @@ cudaError_t launch_newton(const DScene& S, const TraceArgs& A, const WaveArgs& W
     if (S.max_nodes <= kGroup && W.group_newton) {
         const long long threads = n_req * kGroup;
         k_newton_grp<<<static_cast<unsigned>((threads + 127) / 128), 128, 0, stream>>>(S, A, W, n_req);
+    } else if (S.max_nodes <= kGroup && W.newton_group_max > 0) {
+        const long long threads = std::max(n_req, std::min(n_req, W.newton_group_max) * kGroup);
+        k_newton_auto<<<static_cast<unsigned>((threads + 127) / 128), 128, 0, stream>>>(S, A, W, n_req);
     } else {
         k_newton<<<static_cast<unsigned>((n_req + 127) / 128), 128, 0, stream>>>(S, A, W, n_req);
     }

@@ -427,7 +427,7 @@ typedef struct bbrt_tuning {
     int warp_stage1;          /* 1 (default): each patch's stage 1 by the whole warp */
     int order_rays;           /* 1 (default): bucket rays by direction and origin before round 0 */
     int warp_tail;            /* 1 (default): the tail one warp per ray, else one thread per ray */
-    long long wave_tail;      /* rays still waiting when the tail takes over (16384) */
+    long long wave_tail;      /* rays still waiting when the tail takes over (4096) */
     long long wave_min_rays;  /* smaller batches run the fused per-thread kernel (8192) */
     int graph_rounds;         /* 1 (default): the whole wavefront trace is one CUDA graph launch whose
                                  round loop is a device-side conditional node (no host wait per round;

@@ -178,7 +178,7 @@ def test_bounce_map_rays_equal_oracle(built):
 def test_scene_tuning_roundtrip_and_validation(built):
     sc = api.Scene(scenes.scene_two_spheres(), config=C.default_config(coarse_grid_n=9))
     t = sc.tuning()
-    assert t["advance_shape"] == 3 and t["warp_stage1"] == 1 and t["wave_tail"] == 16384 and t["graph_rounds"] == 1
+    assert t["advance_shape"] == 3 and t["warp_stage1"] == 1 and t["wave_tail"] == 4096 and t["graph_rounds"] == 1
     t2 = sc.tuning(advance_shape=6, wave_tail=8192, graph_rounds=0)
     assert t2["advance_shape"] == 6 and t2["wave_tail"] == 8192 and t2["graph_rounds"] == 0 and sc.tuning() == t2
     with pytest.raises(RuntimeError, match="advance_shape"):

@@ -244,7 +244,9 @@ np.savez(sys.argv[2], **{k: g[k] for k in ("status", "bounce_count", "hit_object
                                  {"BBRT_NODE_F32": "0", "BBRT_GRAPH": "0"}, {"BBRT_NODE_F32": "0", "BBRT_CHILD_TEST": "1"},
                                  {"BBRT_NODE_F32": "0", "BBRT_TAIL_SHAPE": "3", "BBRT_WAVE_TAIL": "100000"},
                                  {"BBRT_ADAPT_LANES": "0"}, {"BBRT_ADAPT_LANES": "0", "BBRT_GRAPH": "0"},
-                                 {"BBRT_WAVE_TAIL": "0", "BBRT_GRAPH": "0", "BBRT_ADAPT_LANES": "1"}])
+                                 {"BBRT_WAVE_TAIL": "0", "BBRT_GRAPH": "0", "BBRT_ADAPT_LANES": "1"},
+                                 {"BBRT_NEWTON_GROUP_MAX": "0"}, {"BBRT_NEWTON_GROUP_MAX": "100000000", "BBRT_GRAPH": "0"},
+                                 {"BBRT_NEWTON_GROUP_MAX": "100000000", "BBRT_WAVE_TAIL": "1024"}])
 def test_launch_shape_knobs_do_not_change_results(built, workloads, tmp_path, env):
     """Every schedule (all wavefront rounds, per-thread or per-warp tail, fused
     kernel only, unordered rays, host-driven or graph-launched rounds, Newton
