@@ -420,7 +420,10 @@ BBRT_API int bbrt_trace_batch(const bbrt_scene_t* scenes, int n_scenes, const do
  * (every schedule gives the same bits; GPU-tested).  A scene starts with the
  * library defaults (environment overrides BBRT_ADV_SHAPE, BBRT_WARP_S1,
  * BBRT_ORDER_RAYS, BBRT_WARP_TAIL, BBRT_WAVE_TAIL, BBRT_WAVE_MIN, BBRT_GRAPH
- * are read once per process). */
+ * are read once per process; so are BBRT_NODE_F32 (0: FP64 BVH node tests
+ * only), BBRT_ADAPT_LANES (0: a small round's warps take 32 rays each) and
+ * BBRT_NEWTON_GROUP_MAX (largest Newton round solved 8 lanes per request,
+ * 32768; 0: never), which are not part of this struct). */
 typedef struct bbrt_tuning {
     int advance_shape;        /* k_advance launch shape, threads x blocks per SM: 0 = 128x3, 1 = 256x2,
                                  2 = 128x4, 3 = 512x1 (default), 4 = 768x1, 5 = 1024x1, 6 = 384x1 */
