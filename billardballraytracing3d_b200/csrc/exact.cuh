@@ -200,6 +200,68 @@ __device__ __forceinline__ void eval_fields9(const double* __restrict__ F, int I
     }
 }
 
+// basis_1d for a compile-time node count N, the values in registers: the
+// same operations in the same order (first node within 1e-12 wins).
+template <int N>
+__device__ __forceinline__ void basis_1d_n(const double* nodes, const double* w, double x, double (&b)[N]) {
+    int hit = -1;
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+        if (hit < 0 && fabs(x - nodes[i]) < 1.0e-12) hit = i;
+    if (hit >= 0) {
+#pragma unroll
+        for (int i = 0; i < N; ++i) b[i] = (i == hit) ? 1.0 : 0.0;
+        return;
+    }
+    double denom = 0.0;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        const double li = w[i] / (x - nodes[i]);
+        b[i] = li;
+        denom += li;
+    }
+#pragma unroll
+    for (int i = 0; i < N; ++i) b[i] /= denom;
+}
+
+// eval_fields9 for rows of JN nodes: the row's basis values in registers and
+// its loop unrolled, so a row's loads issue together instead of one node's
+// at a time; the same sums in the same order.
+template <int JN>
+__device__ __forceinline__ void eval_fields9_n(const double* __restrict__ F, int I, const double* bu,
+                                               const double (&bv)[JN], double* out) {
+#pragma unroll
+    for (int f = 0; f < 9; ++f) out[f] = 0.0;
+    for (int i = 0; i < I; ++i) {
+        const double li = bu[i];
+        if (li == 0.0) continue;
+        double rs[9];
+#pragma unroll
+        for (int f = 0; f < 9; ++f) rs[f] = 0.0;
+        const double* row = F + static_cast<long long>(i) * JN * 12;
+#pragma unroll
+        for (int j = 0; j < JN; ++j) {
+            const double lj = bv[j];
+            const double2 f01 = *reinterpret_cast<const double2*>(row + j * 12);
+            const double2 f23 = *reinterpret_cast<const double2*>(row + j * 12 + 2);
+            const double2 f45 = *reinterpret_cast<const double2*>(row + j * 12 + 4);
+            const double2 f67 = *reinterpret_cast<const double2*>(row + j * 12 + 6);
+            const double f8 = row[j * 12 + 8];
+            rs[0] += lj * f01.x;
+            rs[1] += lj * f01.y;
+            rs[2] += lj * f23.x;
+            rs[3] += lj * f23.y;
+            rs[4] += lj * f45.x;
+            rs[5] += lj * f45.y;
+            rs[6] += lj * f67.x;
+            rs[7] += lj * f67.y;
+            rs[8] += lj * f8;
+        }
+#pragma unroll
+        for (int f = 0; f < 9; ++f) out[f] += li * rs[f];
+    }
+}
+
 // Per-ray outcome of one object intersect: hit, miss, or a Newton failure.
 struct QHit {
     double t;
@@ -212,8 +274,11 @@ struct QHit {
 
 // Newton on F(u,v,t) = X(u,v) - (o + t d) from (u0, v0, t0).  Returns
 // 1 hit, or 0 with h.err set (singular / no convergence / out of domain).
-__device__ __forceinline__ int newton_exact(const DScene& S, int pidx, const V3 o, const V3 d, double u, double v,
-                                         double t, QHit& h, long long& iters) {
+// JN > 0: the patch has JN nodes per row (the v basis in registers, each
+// row's loads together); JN = 0: any count.  The same arithmetic either way.
+template <int JN>
+__device__ __forceinline__ int newton_exact_j(const DScene& S, int pidx, const V3 o, const V3 d, double u, double v,
+                                             double t, QHit& h, long long& iters) {
     const int I = S.p_dims[2 * pidx], J = S.p_dims[2 * pidx + 1];
     const double* un = S.p_nodes + S.p_node_off[pidx];
     const double* vn = un + I;
@@ -225,9 +290,15 @@ __device__ __forceinline__ int newton_exact(const DScene& S, int pidx, const V3 
     for (int it = 0; it < S.newton_max_iters; ++it) {
         ++iters;
         basis_1d(un, uw, I, u, bu);
-        basis_1d(vn, vw, J, v, bv);
         double e[9];
-        eval_fields9(F, I, J, bu, bv, e);
+        if constexpr (JN > 0) {
+            double bvr[JN > 0 ? JN : 1];
+            basis_1d_n<JN>(vn, vw, v, bvr);
+            eval_fields9_n<JN>(F, I, bu, bvr, e);
+        } else {
+            basis_1d(vn, vw, J, v, bv);
+            eval_fields9(F, I, J, bu, bv, e);
+        }
         const V3 R = v3(o.x + t * d.x, o.y + t * d.y, o.z + t * d.z);
         const double Fx = e[0] - R.x, Fy = e[1] - R.y, Fz = e[2] - R.z;
         const double a11 = e[3], a12 = e[6], a13 = -d.x;
@@ -263,6 +334,16 @@ __device__ __forceinline__ int newton_exact(const DScene& S, int pidx, const V3 
     return 1;
 }
 
+// Newton in the reference's arithmetic, with the fixed-row forms for the
+// measured node counts (5 and 7 per row).
+__device__ __forceinline__ int newton_exact(const DScene& S, int pidx, const V3 o, const V3 d, double u, double v,
+                                         double t, QHit& h, long long& iters) {
+    const int J = S.p_dims[2 * pidx + 1];
+    if (J == 7) return newton_exact_j<7>(S, pidx, o, d, u, v, t, h, iters);
+    if (J == 5) return newton_exact_j<5>(S, pidx, o, d, u, v, t, h, iters);
+    return newton_exact_j<0>(S, pidx, o, d, u, v, t, h, iters);
+}
+
 // ---- FP32 Newton phase (precision split) -----------------------------------
 
 constexpr int kFp32Iters = 8;          // FP32 iterations before giving up on the phase
@@ -282,11 +363,38 @@ __device__ __forceinline__ void basis_1d_f(const float* nodes, const float* w, i
     for (int i = 0; i < N; ++i) b[i] *= inv;
 }
 
+// basis_1d_f for a compile-time node count N, the values in registers: the
+// same operations in the same order.
+template <int N>
+__device__ __forceinline__ void basis_1d_f_n(const float* nodes, const float* w, float x, float (&b)[N]) {
+    int hit = -1;
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+        if (hit < 0 && x == nodes[i]) hit = i;
+    if (hit >= 0) {
+#pragma unroll
+        for (int i = 0; i < N; ++i) b[i] = (i == hit) ? 1.0f : 0.0f;
+        return;
+    }
+    float denom = 0.0f;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        const float li = w[i] / (x - nodes[i]);
+        b[i] = li;
+        denom += li;
+    }
+    const float inv = 1.0f / denom;
+#pragma unroll
+    for (int i = 0; i < N; ++i) b[i] *= inv;
+}
+
 // Newton on F(u,v,t) in FP32 until |F| < kFp32Residual.  Returns true with
 // the FP32 iterate in (u, v, t); false when it is singular, leaves the
 // neighbourhood of the patch or does not get there in kFp32Iters steps.
-__device__ __forceinline__ bool newton_fp32(const DScene& S, int pidx, const V3& o, const V3& d, double& u,
-                                            double& v, double& t, long long& iters32) {
+// JN > 0: rows of JN nodes (v basis in registers, a row's loads together).
+template <int JN>
+__device__ __forceinline__ bool newton_fp32_j(const DScene& S, int pidx, const V3& o, const V3& d, double& u,
+                                              double& v, double& t, long long& iters32) {
     const int I = S.p_dims[2 * pidx], J = S.p_dims[2 * pidx + 1];
     const float* un = S.p_nodes32 + S.p_node_off[pidx];
     const float* vn = un + I;
@@ -300,7 +408,9 @@ __device__ __forceinline__ bool newton_fp32(const DScene& S, int pidx, const V3&
     for (int it = 0; it < kFp32Iters; ++it) {
         ++iters32;
         basis_1d_f(un, uw, I, uf, bu);
-        basis_1d_f(vn, vw, J, vf, bv);
+        float bvr[JN > 0 ? JN : 1];
+        if constexpr (JN > 0) basis_1d_f_n<JN>(vn, vw, vf, bvr);
+        else basis_1d_f(vn, vw, J, vf, bv);
         float e[9];
         for (int f = 0; f < 9; ++f) e[f] = 0.0f;
         for (int i = 0; i < I; ++i) {
@@ -308,14 +418,15 @@ __device__ __forceinline__ bool newton_fp32(const DScene& S, int pidx, const V3&
             if (li == 0.0f) continue;
             float rs[9];
             for (int f = 0; f < 9; ++f) rs[f] = 0.0f;
-            const float* row = Fd + static_cast<long long>(i) * J * 12;
-            for (int j = 0; j < J; ++j) {
+            const float* row = Fd + static_cast<long long>(i) * (JN > 0 ? JN : J) * 12;
+#pragma unroll
+            for (int j = 0; j < (JN > 0 ? JN : J); ++j) {
                 // a node's 12 floats start on a 16-byte boundary (checked at
                 // upload): fields 0-7 as two 16-byte loads, field 8 alone
                 const float4 fa = *reinterpret_cast<const float4*>(row + j * 12);
                 const float4 fb = *reinterpret_cast<const float4*>(row + j * 12 + 4);
                 const float f8 = row[j * 12 + 8];
-                const float b = bv[j];
+                const float b = JN > 0 ? bvr[JN > 0 ? j : 0] : bv[j];
                 rs[0] = fmaf(b, fa.x, rs[0]);
                 rs[1] = fmaf(b, fa.y, rs[1]);
                 rs[2] = fmaf(b, fa.z, rs[2]);
@@ -350,6 +461,14 @@ __device__ __forceinline__ bool newton_fp32(const DScene& S, int pidx, const V3&
         if (!(fabsf(uf) < 2.0f && fabsf(vf) < 2.0f) || !isfinite(tf)) return false;
     }
     return false;
+}
+
+__device__ __forceinline__ bool newton_fp32(const DScene& S, int pidx, const V3& o, const V3& d, double& u,
+                                            double& v, double& t, long long& iters32) {
+    const int J = S.p_dims[2 * pidx + 1];
+    if (J == 7) return newton_fp32_j<7>(S, pidx, o, d, u, v, t, iters32);
+    if (J == 5) return newton_fp32_j<5>(S, pidx, o, d, u, v, t, iters32);
+    return newton_fp32_j<0>(S, pidx, o, d, u, v, t, iters32);
 }
 
 // The precision split: FP32 Newton to |F| < 1e-5 from (u, v, t), then the
