@@ -53,15 +53,19 @@ __device__ __forceinline__ double grp_basis(const double* nodes, const double* w
 
 // eval_fields<NF, FIRST>: lane g forms row g's sums over j (j in order),
 // every lane then adds the rows in i order, skipping rows whose basis is 0.
-template <int NF, int FIRST>
+// JN > 0: rows of JN nodes, the row loop unrolled so that its loads issue
+// together (the same sums in the same order); JN = 0: any J.
+template <int NF, int FIRST, int JN = 0>
 __device__ __forceinline__ void grp_eval(const double* __restrict__ F, int I, int J, double bu, double bv,
                                          const Grp& G, double* out) {
     double rs[NF];
 #pragma unroll
     for (int f = 0; f < NF; ++f) rs[f] = 0.0;
     const bool row = G.g < I && bu != 0.0;
-    const double* rp = F + static_cast<long long>(G.g < I ? G.g : 0) * J * 12 + FIRST;
-    for (int j = 0; j < J; ++j) {
+    const int JJ = JN > 0 ? JN : J;
+    const double* rp = F + static_cast<long long>(G.g < I ? G.g : 0) * JJ * 12 + FIRST;
+#pragma unroll
+    for (int j = 0; j < JJ; ++j) {
         const double lj = __shfl_sync(G.mask, bv, G.base + j);
         if (row) {
             if constexpr (NF == 9 && FIRST == 0) {
@@ -97,8 +101,9 @@ __device__ __forceinline__ void grp_eval(const double* __restrict__ F, int I, in
 }
 
 // newton_exact by a group: every lane returns the same result.
-__device__ __forceinline__ int grp_newton_exact(const DScene& S, int pidx, const V3 o, const V3 d, double u, double v,
-                                                double t, QHit& h, long long& iters, const Grp& G) {
+template <int JN>
+__device__ __forceinline__ int grp_newton_exact_j(const DScene& S, int pidx, const V3 o, const V3 d, double u,
+                                                  double v, double t, QHit& h, long long& iters, const Grp& G) {
     const int I = S.p_dims[2 * pidx], J = S.p_dims[2 * pidx + 1];
     const double* un = S.p_nodes + S.p_node_off[pidx];
     const double* vn = un + I;
@@ -111,7 +116,7 @@ __device__ __forceinline__ int grp_newton_exact(const DScene& S, int pidx, const
         const double bu = grp_basis(un, uw, I, u, G);
         const double bv = grp_basis(vn, vw, J, v, G);
         double e[9];
-        grp_eval<9, 0>(F, I, J, bu, bv, G, e);
+        grp_eval<9, 0, JN>(F, I, J, bu, bv, G, e);
         const V3 R = v3(o.x + t * d.x, o.y + t * d.y, o.z + t * d.z);
         const double Fx = e[0] - R.x, Fy = e[1] - R.y, Fz = e[2] - R.z;
         const double a11 = e[3], a12 = e[6], a13 = -d.x;
@@ -147,6 +152,15 @@ __device__ __forceinline__ int grp_newton_exact(const DScene& S, int pidx, const
     return 1;
 }
 
+// Dispatch to the fixed-row forms for 5 and 7 nodes per row.
+__device__ __forceinline__ int grp_newton_exact(const DScene& S, int pidx, const V3 o, const V3 d, double u, double v,
+                                                double t, QHit& h, long long& iters, const Grp& G) {
+    const int J = S.p_dims[2 * pidx + 1];
+    if (J == 7) return grp_newton_exact_j<7>(S, pidx, o, d, u, v, t, h, iters, G);
+    if (J == 5) return grp_newton_exact_j<5>(S, pidx, o, d, u, v, t, h, iters, G);
+    return grp_newton_exact_j<0>(S, pidx, o, d, u, v, t, h, iters, G);
+}
+
 // ---- FP32 phase of the precision split, by a group ---------------------------
 
 __device__ __forceinline__ float grp_basis_f(const float* nodes, const float* w, int N, float x, const Grp& G) {
@@ -161,8 +175,9 @@ __device__ __forceinline__ float grp_basis_f(const float* nodes, const float* w,
 }
 
 // newton_fp32 by a group (same stopping rules); every lane returns the same.
-__device__ __forceinline__ bool grp_newton_fp32(const DScene& S, int pidx, const V3& o, const V3& d, double& u,
-                                                double& v, double& t, long long& iters32, const Grp& G) {
+template <int JN>
+__device__ __forceinline__ bool grp_newton_fp32_j(const DScene& S, int pidx, const V3& o, const V3& d, double& u,
+                                                  double& v, double& t, long long& iters32, const Grp& G) {
     const int I = S.p_dims[2 * pidx], J = S.p_dims[2 * pidx + 1];
     const float* un = S.p_nodes32 + S.p_node_off[pidx];
     const float* vn = un + I;
@@ -179,8 +194,10 @@ __device__ __forceinline__ bool grp_newton_fp32(const DScene& S, int pidx, const
         float rs[9];
         for (int f = 0; f < 9; ++f) rs[f] = 0.0f;
         const bool row = G.g < I && bu != 0.0f;
-        const float* rp = Fd + static_cast<long long>(G.g < I ? G.g : 0) * J * 12;
-        for (int j = 0; j < J; ++j) {
+        const int JJ = JN > 0 ? JN : J;
+        const float* rp = Fd + static_cast<long long>(G.g < I ? G.g : 0) * JJ * 12;
+#pragma unroll
+        for (int j = 0; j < JJ; ++j) {
             const float lj = __shfl_sync(G.mask, bv, G.base + j);
             if (row)
                 for (int f = 0; f < 9; ++f) rs[f] = fmaf(lj, rp[j * 12 + f], rs[f]);
@@ -214,6 +231,14 @@ __device__ __forceinline__ bool grp_newton_fp32(const DScene& S, int pidx, const
         if (!(fabsf(uf) < 2.0f && fabsf(vf) < 2.0f) || !isfinite(tf)) return false;
     }
     return false;
+}
+
+__device__ __forceinline__ bool grp_newton_fp32(const DScene& S, int pidx, const V3& o, const V3& d, double& u,
+                                                double& v, double& t, long long& iters32, const Grp& G) {
+    const int J = S.p_dims[2 * pidx + 1];
+    if (J == 7) return grp_newton_fp32_j<7>(S, pidx, o, d, u, v, t, iters32, G);
+    if (J == 5) return grp_newton_fp32_j<5>(S, pidx, o, d, u, v, t, iters32, G);
+    return grp_newton_fp32_j<0>(S, pidx, o, d, u, v, t, iters32, G);
 }
 
 // Newton in the scene's precision mode, by a group.
