@@ -154,6 +154,24 @@ def test_no_cpu_fallback_without_gpu(built, workloads):
         sc.intersect(o, d)
 
 
+def test_node_test_check_arguments(built):
+    """bbrt_node_test_check: NULL arrays and negative counts are argument
+    errors, an empty call succeeds, and on a machine without a GPU it fails
+    loudly (the FP32 node test has no CPU path)."""
+    lib = C.load_library()
+    out = np.zeros(2, dtype=np.int32)
+    v = np.zeros(3)
+    assert lib.bbrt_node_test_check(None, None, None, 1, None, None) == C.BBRT_ERR_ARG
+    assert lib.bbrt_node_test_check(C.ptr(v), C.ptr(v), C.ptr(v), -1, C.ptr(np.zeros(6)),
+                                    C.ptr(out, ctypes.c_int)) == C.BBRT_ERR_ARG
+    assert lib.bbrt_node_test_check(None, None, None, 0, None, None) == C.BBRT_OK
+    if lib.bbrt_device_count() > 0:
+        return
+    rc = lib.bbrt_node_test_check(C.ptr(v), C.ptr(np.array([0.0, 0.0, -1.0])), C.ptr(np.array([np.inf])), 1,
+                                  C.ptr(np.array([-1.0, -1.0, -1.0, 1.0, 1.0, 1.0])), C.ptr(out, ctypes.c_int))
+    assert rc == C.BBRT_ERR_CUDA and b"no CUDA device" in lib.bbrt_last_error()
+
+
 def test_bounce_map_rays_equal_oracle(built):
     """bbrt_bounce_map_rays is host code: the launch rays of
     BounceMapDriver::run (BounceMapDriver.hpp:119-237), bit for bit."""
