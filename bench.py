@@ -65,6 +65,8 @@ def parse():
     ap.add_argument("--train-rays", type=int, default=32 << 20,
                     help="rays of each scene traced to record training samples")
     ap.add_argument("--train-epochs", type=int, default=6)
+    ap.add_argument("--guess-min-logit", type=float, default=0.0,
+                    help="confidence logit above which Newton starts from the learned guess")
     ap.add_argument("--train-positives", type=int, default=16 << 20, help="converged Newton solves kept for training")
     ap.add_argument("--train-negatives", type=int, default=4 << 20, help="stage-1 misses kept for training")
     ap.add_argument("--accuracy-rays", type=int, default=262144, help="0 skips the accuracy comparison")
@@ -435,7 +437,6 @@ def run_ours(args, rank, world, local_rank):
 
     # launch schedule picked on the workload itself (plain form; results do not depend on it)
     tuned = scene.autotune(o, d, maxb, trials=2) if args.autotune else scene.tuning()
-    # the learned guess: trained on this GPU on a separately seeded ray set of the same source
     # the learned guess: trained on this GPU by the project's own kernels on
     # samples that a plain trace of separately seeded rays records; with a
     # second workload, one network for both scenes (a scene set of the two),
@@ -443,7 +444,8 @@ def run_ours(args, rank, world, local_rank):
     second = None
     train_src = TRAIN_SOURCE.get(args.workload, (5.0, 3.0, 10.0))
     train_o, train_d = scenes.cone_rays(args.train_rays, 99 + rank, *train_src)
-    tcfg = dict(epochs=args.train_epochs, max_positive=args.train_positives, max_negative=args.train_negatives)
+    tcfg = dict(epochs=args.train_epochs, max_positive=args.train_positives, max_negative=args.train_negatives,
+                min_logit=args.guess_min_logit)
     if args.second:
         s_patches, s_o, s_d, s_maxb, s_cn, s_tol = scenes.workload(args.second, args.second_rays)
         s_scene = api.Scene(s_patches, config=C.default_config(coarse_grid_n=s_cn, newton_tol=s_tol, cull=args.cull))
